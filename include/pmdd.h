@@ -1,0 +1,181 @@
+/*
+ * pmdd.h -- C ABI of the B200 Pareto-frontier enumeration engine (libpmdd_gpu.so).
+ *
+ * This is the drop-in boundary for the GPU enumeration seam of rahulptel/PMDD.  The
+ * reference exposes four C++ free functions that take its pointer-based BDD / MDD
+ * objects (src/pmdd/enum/gpu/cuda_wrappers.hpp:11-21):
+ *
+ *   topdown_cuda_enumerate(BDD*, maximization, problem_type, state_dominance,
+ *                          EnumerationStats*, std::string* reason, max_cand)
+ *   topdown_mdd_cuda_enumerate(MDD*, EnumerationStats*, std::string*, max_cand)
+ *   coupled_cuda_enumerate(MDD*, EnumerationStats*, std::string*, max_cand, max_prod)
+ *   coupled_bdd_cuda_enumerate(BDD*, maximization, problem_type, state_dominance,
+ *                              EnumerationStats*, std::string*, max_cand, max_prod)
+ *
+ * All four collapse to pmdd_enumerate() over a flat, layered DD (pmdd_dd below): the
+ * reference's packing step (src/pmdd/enum/gpu/enum.cu:85-158, :438-593) becomes the
+ * caller's job, done once, in plain arrays.  Only POD types cross this boundary.
+ *
+ * Error behaviour mirrors the reference seam: a failed call returns a non-zero status
+ * and writes a one-line reason into `err` (the reference returns NULL and sets
+ * *reason, src/pmdd/enum/gpu/enum_types.cuh:76-81); it never falls back to the CPU.
+ */
+#ifndef PMDD_H_
+#define PMDD_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status codes */
+enum pmdd_status {
+    PMDD_OK = 0,
+    PMDD_ERR_INVALID = 1,        /* malformed DD or options */
+    PMDD_ERR_CUDA = 2,           /* CUDA runtime error (text in err) */
+    PMDD_ERR_OOM = 3,            /* request cannot fit the device / server budget */
+    PMDD_ERR_CAND_OVERFLOW = 4,  /* a single destination exceeds what one pass can hold */
+    PMDD_ERR_TIMEOUT = 5,        /* a bounded device wait gave up */
+    PMDD_ERR_INTERNAL = 6,       /* device-side consistency check failed */
+    PMDD_ERR_CANCELLED = 7,      /* request cancelled before completion */
+    PMDD_ERR_NO_DEVICE = 8,      /* no CUDA device / extension not usable */
+    PMDD_ERR_RANGE = 9           /* objective sums exceed the supported integer range */
+};
+
+/* ------------------------------------------------------------ the flat DD format
+ * Nodes are numbered 0..num_nodes-1 layer by layer; layer l holds nodes
+ * [layer_offsets[l], layer_offsets[l+1]).  Layer 0 holds exactly one node (the root)
+ * and the last layer exactly one node (the terminal).
+ *
+ * Arcs are stored once, grouped by their HEAD (destination) node: the incoming arcs
+ * of node v are [in_arc_offsets[v], in_arc_offsets[v+1]); arc a runs from node
+ * arc_src[a] (which must lie in the layer just above v) to v and carries the weight
+ * vector weights[arc_weight[a]*nobjs .. +nobjs).  A BDD uses weight row 0 for every
+ * 0-arc (the zero vector) and one further row per layer for its 1-arcs, so an arc's
+ * type is (arc_weight[a] != 0); a TSP MDD uses row 0 for the arc into the fixed first
+ * city and row 1 + i*n + j for the move from city i to city j.  The bottom-up
+ * direction (outgoing arcs) is derived by the engine.
+ *
+ * min_weight (optional, may be NULL): knapsack used-capacity lower bound per node,
+ * required only for state_dominance > 0 with problem_type 1 (the reference's
+ * Node::min_weight, src/pmdd/bdd/knapsack_bdd.cpp:123-150).
+ */
+typedef struct pmdd_dd {
+    int32_t nobjs;        /* objectives per point, 1..8 */
+    int32_t num_layers;   /* >= 2 */
+    int32_t num_nodes;
+    int32_t num_arcs;
+    int32_t num_weights;  /* rows in `weights` */
+    const int32_t *layer_offsets;   /* [num_layers+1] */
+    const int32_t *in_arc_offsets;  /* [num_nodes+1] */
+    const int32_t *arc_src;         /* [num_arcs] */
+    const int32_t *arc_weight;      /* [num_arcs] row index into weights */
+    const int32_t *weights;         /* [num_weights*nobjs] */
+    const int32_t *min_weight;      /* [num_nodes] or NULL */
+} pmdd_dd;
+
+/* ------------------------------------------------------------------- options */
+typedef struct pmdd_options {
+    int32_t method;           /* 1 = top-down, 3 = dynamic layer cutset (coupled) */
+    int32_t problem_type;     /* 1 knapsack, 2 set packing, 3 TSP */
+    int32_t state_dominance;  /* > 0: knapsack label pruning (method 1, problem 1) */
+    int32_t maximization;     /* must be 1 (the reference's main always maximises) */
+    int64_t max_cand;         /* candidate points per expansion pass (--max-cand, 20M) */
+    int64_t max_prod;         /* pair products per coupling pass (--max-prod, 625K) */
+    int32_t device;           /* CUDA device ordinal (the reference always uses 0) */
+    int32_t reserved;
+} pmdd_options;
+
+/* Fills `o` with the reference CLI defaults (method 1, max_cand 20M, max_prod 625K). */
+void pmdd_options_default(pmdd_options *o);
+
+/* -------------------------------------------------------------------- output */
+typedef struct pmdd_frontier {
+    int32_t nobjs;
+    int32_t elem_bytes;   /* 4: int32 points, 8: int64 points (wide objective bound) */
+    int64_t num_points;
+    void *points;         /* num_points*nobjs values, unsorted; free with pmdd_frontier_free */
+} pmdd_frontier;
+
+void pmdd_frontier_free(pmdd_frontier *f);
+
+/* Run statistics: the GPU-side subset of the reference's EnumerationStats
+ * (src/pmdd/util/stats.hpp:18-85), same names and meaning. */
+typedef struct pmdd_stats {
+    double wall_pack_transfer_s;
+    double wall_join_s;
+    double kernel_expand_td_s;
+    double kernel_dominance_s;
+    double kernel_total_s;
+    int64_t gpu_mem_peak_used_bytes;
+    int64_t gpu_mem_peak_reserved_bytes;
+    int64_t work_candidates_total;
+    int64_t work_candidates_peak;
+    int64_t work_frontier_survivors_total;
+    int64_t work_frontier_peak_points;
+    int64_t work_join_products_total;
+    int64_t dominance_filtered_total;
+    int32_t layer_coupling;
+    int32_t layers_td;
+    int32_t layers_bu;
+    int32_t cutset_size;
+    int64_t gpu_launches;   /* kernels this call launched */
+} pmdd_stats;
+
+/* ------------------------------------------------------------ one-shot entry
+ * Replaces all four reference seam functions.  Synchronous; blocks until the
+ * frontier is on the host.  Thread-safe across different devices. */
+int pmdd_enumerate(const pmdd_dd *dd, const pmdd_options *opts, pmdd_frontier *out,
+                   pmdd_stats *stats, char *err, size_t errlen);
+
+/* Batched entry: enumerates `count` independent DDs in shared launches (one launch
+ * per phase per step covers every instance still running).  outs[i] / status[i]
+ * receive each instance's frontier and status; stats (optional) aggregates. */
+int pmdd_enumerate_batch(const pmdd_dd *dds, int32_t count, const pmdd_options *opts,
+                         pmdd_frontier *outs, int32_t *status, pmdd_stats *stats,
+                         char *err, size_t errlen);
+
+/* ---------------------------------------------------------------- serving
+ * A device-resident request loop with continuous batching: submitted requests are
+ * admitted as slots and HBM budget free up; every admitted request advances one
+ * layer per engine step, sharing each launch with the others. */
+typedef struct pmdd_server pmdd_server;
+
+typedef struct pmdd_result {
+    uint64_t req_id;
+    int32_t status;
+    int32_t reserved;
+    pmdd_frontier frontier;   /* owned by the caller after poll; pmdd_frontier_free */
+    double submit_s;          /* host monotonic clock, seconds */
+    double admit_s;
+    double finish_s;
+    char error[160];
+} pmdd_result;
+
+pmdd_server *pmdd_server_create(int32_t device, int64_t budget_bytes, int32_t max_slots,
+                                char *err, size_t errlen);
+/* Copies the DD; the caller's buffers may be reused immediately. */
+int pmdd_server_submit(pmdd_server *srv, const pmdd_dd *dd, const pmdd_options *opts,
+                       uint64_t req_id);
+/* Runs engine steps until at least one request completes or nothing is pending;
+ * returns the number of results now waiting. */
+int pmdd_server_run(pmdd_server *srv, int32_t max_steps);
+/* Non-blocking: 1 and fills *out if a finished result is available, else 0. */
+int pmdd_server_poll(pmdd_server *srv, pmdd_result *out);
+int pmdd_server_cancel(pmdd_server *srv, uint64_t req_id);
+/* Requests submitted but not yet finished (queued + running). */
+int pmdd_server_pending(const pmdd_server *srv);
+void pmdd_server_destroy(pmdd_server *srv);
+
+/* --------------------------------------------------------------- utilities */
+const char *pmdd_version(void);
+/* Number of kernels this library has launched in this process (all calls). */
+int64_t pmdd_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PMDD_H_ */

@@ -1,0 +1,91 @@
+// Shared device-side definitions of the enumeration engine.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace pmdd {
+namespace dev {
+
+// Fused expand+filter tiles: a tile owns every destination whose candidate range
+// starts inside its window of kTileWindow candidates; destinations of at most
+// kSmallMax candidates are filtered in shared memory, larger ones take the
+// global-memory ("big") path.  A tile therefore holds < 2*kTileWindow candidates.
+constexpr int kTileThreads = 256;
+constexpr int kTileWindow = 1024;
+constexpr int kSmallMax = 1024;
+constexpr int kTileCap = 2 * kTileWindow;
+constexpr int kTileItemCap = 1024;   // destinations staged per pass inside one tile
+
+constexpr int kCountThreads = 1024;
+constexpr int kBigThreads = 256;
+constexpr int kBigJTile = 1024;       // candidates per shared-memory comparison tile
+
+// Device error word bits (written with atomicOr; read back once per step).
+constexpr uint32_t kErrBounds = 1u;        // an index check failed (work skipped)
+constexpr uint32_t kErrCoupleOverflow = 2u;
+
+// One layer expansion of one instance in one direction.  "Items" are the destination
+// nodes of the layer; each has a contiguous range of arcs whose neighbour (the arc's
+// other end, in the previous layer of this direction) carries a frontier.
+struct ExpandJob {
+    const int32_t *item_arc_off;   // [global node id] -> first arc; range end at v+1
+    const int32_t *arc_nbr;        // neighbour node (global id)
+    const int32_t *arc_wrow;       // weight row per arc
+    const int32_t *weights;        // [rows * D]
+    const int64_t *arc_cand_off;   // [arc - arc_base] -> first candidate of the arc; A+1 entries
+    int32_t arc_base;
+    int32_t item_base;             // global id of the first destination node
+    int32_t num_items;
+    int32_t prev_base;             // global id of the first neighbour-layer node
+    const void *prev_pts;          // neighbour frontiers (slot layout, D values per point)
+    const int64_t *prev_off;       // [local neighbour] -> slot start (points)
+    const int32_t *prev_size;      // [local neighbour] -> live points in slot
+    void *out_pts;                 // destination slots: total_cand points
+    int64_t *out_off;              // [local item] -> slot start
+    int32_t *out_size;             // [local item] -> survivors
+    int64_t total_cand;
+    int64_t tile_base;             // first global tile index of this job
+    int64_t num_tiles;
+    const int64_t *big_list;       // (local item, scratch offset) pairs
+    int32_t num_big;
+    int32_t pad0;
+    void *big_pts;                 // scratch for oversized destinations (points)
+    int32_t *big_tag;              // arc of each scratch point
+    uint8_t *big_keep;             // keep flag of each scratch point
+    uint32_t *err;
+};
+
+// Counting pass for the next layer of one direction.
+struct CountJob {
+    const int32_t *item_arc_off;
+    const int32_t *arc_nbr;
+    int32_t arc_base;
+    int32_t num_arcs;
+    int32_t item_base;
+    int32_t num_items;
+    int32_t cur_base;              // global id of the first node of the current layer
+    int32_t cur_nodes;             // nodes in the current layer
+    const int32_t *cur_size;       // [local current node] -> frontier size
+    int64_t *arc_cand_off;         // out: num_arcs + 1 entries
+    int64_t *big_list;             // out: (local item, scratch offset) pairs, capacity num_items
+    struct CountResult *result;    // out
+};
+
+struct CountResult {
+    int64_t total;       // candidates of the next layer
+    int64_t max_item;    // largest destination
+    int64_t big_total;   // candidates in destinations above kSmallMax
+    int64_t cur_total;   // points of the current layer's frontiers (survivor statistics)
+    int32_t num_big;
+    int32_t pad;
+};
+
+// Big-path work entry: one oversized destination of one job.
+struct BigWork {
+    int32_t job;
+    int32_t big;       // index into the job's big_list
+};
+
+}  // namespace dev
+}  // namespace pmdd

@@ -1,0 +1,52 @@
+// Method-3 coupling and DD-preparation launchers (couple.cu).
+#pragma once
+
+#include <algorithm>
+
+#include "common.cuh"
+
+namespace pmdd {
+namespace dev {
+
+constexpr int kCoupleThreads = 256;
+constexpr int kCoupleFS = 2048;  // running-frontier points staged in shared memory for pruning
+
+// Per-job device counters (int64 each).
+enum CoupleCtr {
+    kCtrF = 0,          // points of the running frontier at the front of U
+    kCtrB = 1,          // survivors appended this round (may exceed room; clamped)
+    kCtrResume = 2,     // first cutset node whose survivors did not fit (num_nodes: none)
+    kCtrCursor = 3,     // next cutset node to hand out this round
+    kCtrEvaluated = 4,  // products compared one by one (statistics)
+    kCtrDone = 5,       // 1 once a round finished every node
+    kCtrValidEnd = 6,   // U slots below this index hold written points (set on overflow)
+    kCtrProducts = 7,   // sum over cutset nodes of |TD_v| * |BU_v| (statistics)
+    kCtrCount = 8
+};
+
+struct CoupleJob {
+    const void *td_pts;
+    const int64_t *td_off;
+    const int32_t *td_size;
+    const void *bu_pts;
+    const int64_t *bu_off;
+    const int32_t *bu_size;
+    int32_t num_nodes;
+    int32_t pad0;
+    void *U;            // running frontier followed by this round's survivors
+    int64_t ucap;       // points U can hold
+    uint8_t *keep;      // ucap flags
+    int64_t *ctr;       // kCtrCount counters
+};
+
+cudaError_t launch_build_out_csr(const int32_t *in_off, const int32_t *arc_src, const int32_t *arc_w,
+                                 int32_t num_nodes, int32_t num_arcs, int32_t *out_off, int32_t *cursor,
+                                 int32_t *out_head, int32_t *out_w, cudaStream_t stream);
+
+cudaError_t launch_couple_round(int d, bool wide, const CoupleJob *jobs, int num_jobs, int blocks_per_job,
+                                cudaStream_t stream);
+// Once per job at the start of coupling: kCtrProducts = sum of |TD_v| * |BU_v|.
+cudaError_t launch_couple_products(const CoupleJob *jobs, int num_jobs, cudaStream_t stream);
+
+}  // namespace dev
+}  // namespace pmdd

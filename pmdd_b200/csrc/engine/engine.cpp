@@ -1,0 +1,946 @@
+// Host side of the enumeration engine: arena, admission, and the step scheduler.
+//
+// One engine step advances every admitted request by one layer in one direction:
+//   H2D of this step's descriptors
+//   -> out-arc CSR for newly admitted method-3 requests
+//   -> fused expand+filter tiles for all expanding requests (+ the oversized-destination path)
+//   -> next-layer counting for every side that moved (and for new requests)
+//   -> one coupling round for every request at its cutset
+//   -> D2H of a small summary, one stream synchronisation.
+// The layer-choice rule of method 3 is the reference GPU driver's
+// (src/pmdd/enum/gpu/enum.cu:331-428, :661-738): expand top-down while
+// top-down score <= bottom-up score, where the top-down score is the next top-down
+// layer's candidate count and the bottom-up score is 1.5x (truncated) the next
+// bottom-up layer's candidate count; both start at 0.
+#include "engine.hpp"
+
+#include <algorithm>
+#include <atomic>
+#include <climits>
+#include <cstring>
+
+namespace pmdd {
+
+double now_s() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+static size_t align256(size_t x) { return (x + 255) & ~static_cast<size_t>(255); }
+
+// ------------------------------------------------------------------- Arena
+Arena::~Arena() {
+    if (base_) cudaFree(base_);
+}
+
+bool Arena::init(size_t bytes, std::string *err) {
+    bytes &= ~static_cast<size_t>(255);
+    cudaError_t e = cudaMalloc(reinterpret_cast<void **>(&base_), bytes);
+    if (e != cudaSuccess) {
+        if (err) *err = std::string("cudaMalloc of the engine arena failed: ") + cudaGetErrorString(e);
+        base_ = nullptr;
+        return false;
+    }
+    cap_ = bytes;
+    free_.clear();
+    free_[0] = bytes;
+    return true;
+}
+
+void *Arena::alloc(size_t bytes) {
+    bytes = align256(bytes == 0 ? 1 : bytes);
+    for (auto it = free_.begin(); it != free_.end(); ++it) {
+        if (it->second < bytes) continue;
+        const size_t off = it->first, rem = it->second - bytes;
+        free_.erase(it);
+        if (rem) free_[off + bytes] = rem;
+        live_[off] = bytes;
+        used_ += bytes;
+        peak_ = std::max(peak_, used_);
+        return base_ + off;
+    }
+    return nullptr;
+}
+
+void Arena::release(void *p) {
+    if (p == nullptr) return;
+    const size_t off = static_cast<size_t>(static_cast<char *>(p) - base_);
+    auto lv = live_.find(off);
+    if (lv == live_.end()) return;
+    size_t start = off, bytes = lv->second;
+    live_.erase(lv);
+    used_ -= bytes;
+    auto next = free_.lower_bound(start);
+    if (next != free_.end() && next->first == start + bytes) {
+        bytes += next->second;
+        next = free_.erase(next);
+    }
+    if (next != free_.begin()) {
+        auto prev = std::prev(next);
+        if (prev->first + prev->second == start) {
+            start = prev->first;
+            bytes += prev->second;
+            free_.erase(prev);
+        }
+    }
+    free_[start] = bytes;
+}
+
+bool Engine::Pinned::reserve(size_t bytes) {
+    if (bytes <= cap) return true;
+    size_t c = std::max<size_t>(bytes, cap * 2);
+    c = std::max<size_t>(c, 1 << 16);
+    void *np = nullptr;
+    if (cudaMallocHost(&np, c) != cudaSuccess) return false;
+    if (p) cudaFreeHost(p);
+    p = np;
+    cap = c;
+    return true;
+}
+
+Engine::Pinned::~Pinned() {
+    if (p) cudaFreeHost(p);
+}
+
+// ------------------------------------------------------ request preparation
+int prepare_instance(const pmdd_dd &dd, const pmdd_options &o, uint64_t id, Instance *I, std::string *err) {
+    auto bad = [&](const std::string &m) {
+        if (err) *err = m;
+        return static_cast<int>(PMDD_ERR_INVALID);
+    };
+    if (o.method != 1 && o.method != 3) return bad("method must be 1 (top-down) or 3 (coupled) on the GPU backend");
+    if (o.maximization == 0) return bad("only maximisation is supported (the reference's main always maximises)");
+    if (dd.nobjs < 1 || dd.nobjs > 8) return bad("nobjs must be in 1..8");
+    if (dd.num_layers < 2) return bad("DD needs at least a root and a terminal layer");
+    if (dd.num_nodes < 2 || dd.num_arcs < 0 || dd.num_weights < 1) return bad("DD sizes out of range");
+    if (!dd.layer_offsets || !dd.in_arc_offsets || !dd.weights || (dd.num_arcs > 0 && (!dd.arc_src || !dd.arc_weight)))
+        return bad("DD array pointer is NULL");
+    const int32_t L = dd.num_layers, N = dd.num_nodes, A = dd.num_arcs, K = dd.num_weights, d = dd.nobjs;
+    if (dd.layer_offsets[0] != 0 || dd.layer_offsets[L] != N) return bad("layer_offsets must run from 0 to num_nodes");
+    for (int l = 0; l < L; ++l)
+        if (dd.layer_offsets[l + 1] <= dd.layer_offsets[l]) return bad("every layer needs at least one node");
+    if (dd.layer_offsets[1] != 1) return bad("layer 0 must hold exactly the root");
+    if (dd.layer_offsets[L] - dd.layer_offsets[L - 1] != 1) return bad("the last layer must hold exactly the terminal");
+    if (dd.in_arc_offsets[0] != 0 || dd.in_arc_offsets[1] != 0) return bad("the root has no incoming arcs");
+    if (dd.in_arc_offsets[N] != A) return bad("in_arc_offsets must end at num_arcs");
+    for (int32_t v = 0; v < N; ++v)
+        if (dd.in_arc_offsets[v + 1] < dd.in_arc_offsets[v]) return bad("in_arc_offsets must be non-decreasing");
+    // every arc runs from the layer right above its head; bound on |path sums|
+    int64_t bound = 0;
+    for (int l = 1; l < L; ++l) {
+        int64_t layer_max = 0;
+        const int32_t lo = dd.layer_offsets[l - 1], hi = dd.layer_offsets[l];
+        for (int32_t v = dd.layer_offsets[l]; v < dd.layer_offsets[l + 1]; ++v) {
+            for (int32_t a = dd.in_arc_offsets[v]; a < dd.in_arc_offsets[v + 1]; ++a) {
+                const int32_t s = dd.arc_src[a], w = dd.arc_weight[a];
+                if (s < lo || s >= hi) return bad("arc tail is not in the layer above its head");
+                if (w < 0 || w >= K) return bad("arc weight row out of range");
+                for (int k = 0; k < d; ++k)
+                    layer_max = std::max<int64_t>(layer_max, std::llabs(static_cast<int64_t>(dd.weights[static_cast<int64_t>(w) * d + k])));
+            }
+        }
+        bound += layer_max;
+    }
+    I->id = id;
+    I->opts = o;
+    I->d = d;
+    I->wide = bound > static_cast<int64_t>(INT32_MAX);
+    I->L = L;
+    I->N = N;
+    I->A = A;
+    I->K = K;
+    I->layer_off.assign(dd.layer_offsets, dd.layer_offsets + L + 1);
+    I->arc_at_layer.resize(L + 1);
+    for (int l = 0; l <= L; ++l) I->arc_at_layer[l] = dd.in_arc_offsets[dd.layer_offsets[l]];
+    // pack the DD arrays
+    size_t off = 0;
+    I->off_layer = off;
+    off = align256(off + sizeof(int32_t) * (L + 1));
+    I->off_in = off;
+    off = align256(off + sizeof(int32_t) * (static_cast<size_t>(N) + 1));
+    I->off_src = off;
+    off = align256(off + sizeof(int32_t) * static_cast<size_t>(A));
+    I->off_w = off;
+    off = align256(off + sizeof(int32_t) * static_cast<size_t>(A));
+    I->off_weights = off;
+    off = align256(off + sizeof(int32_t) * static_cast<size_t>(K) * d);
+    const bool has_minw = dd.min_weight != nullptr;
+    I->off_minw = has_minw ? off : 0;
+    if (has_minw) off = align256(off + sizeof(int32_t) * static_cast<size_t>(N));
+    I->blob_bytes = off;
+    I->blob.assign(off, 0);
+    std::memcpy(I->blob.data() + I->off_layer, dd.layer_offsets, sizeof(int32_t) * (L + 1));
+    std::memcpy(I->blob.data() + I->off_in, dd.in_arc_offsets, sizeof(int32_t) * (static_cast<size_t>(N) + 1));
+    if (A > 0) {
+        std::memcpy(I->blob.data() + I->off_src, dd.arc_src, sizeof(int32_t) * static_cast<size_t>(A));
+        std::memcpy(I->blob.data() + I->off_w, dd.arc_weight, sizeof(int32_t) * static_cast<size_t>(A));
+    }
+    std::memcpy(I->blob.data() + I->off_weights, dd.weights, sizeof(int32_t) * static_cast<size_t>(K) * d);
+    if (has_minw) std::memcpy(I->blob.data() + I->off_minw, dd.min_weight, sizeof(int32_t) * static_cast<size_t>(N));
+    size_t dev = off;
+    if (o.method == 3) {
+        dev = align256(dev + sizeof(int32_t) * (static_cast<size_t>(N) + 1));  // out_off
+        dev = align256(dev + sizeof(int32_t) * static_cast<size_t>(A));       // out_head
+        dev = align256(dev + sizeof(int32_t) * static_cast<size_t>(A));       // out_w
+        dev = align256(dev + sizeof(int32_t) * static_cast<size_t>(N));       // cursor
+    }
+    I->dev_bytes = dev;
+    // admission estimate: the DD, plus a few layers' worth of frontier slots
+    int64_t widest_arcs = 0;
+    for (int l = 0; l < L; ++l) widest_arcs = std::max<int64_t>(widest_arcs, I->arc_at_layer[l + 1] - I->arc_at_layer[l]);
+    I->est_bytes = static_cast<int64_t>(dev) + 8 * widest_arcs * static_cast<int64_t>(d * I->elem() + 16);
+    I->submit_s = now_s();
+    return PMDD_OK;
+}
+
+// ------------------------------------------------------------------ Engine
+Engine::Engine(int device, int64_t budget_bytes, int max_slots) : device_(device), max_slots_(max_slots) {
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count <= 0) {
+        error_ = e != cudaSuccess ? std::string("cudaGetDeviceCount failed: ") + cudaGetErrorString(e)
+                                  : std::string("No CUDA device found");
+        return;
+    }
+    if (device < 0 || device >= count) {
+        error_ = "CUDA device ordinal out of range";
+        return;
+    }
+    if (!cuda_ok(cudaSetDevice(device), "cudaSetDevice")) return;
+    cudaDeviceProp prop;
+    if (!cuda_ok(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties")) return;
+    if (prop.major < 10) {
+        error_ = "this engine is built for sm_100a (B200); device reports compute capability " +
+                 std::to_string(prop.major) + "." + std::to_string(prop.minor);
+        return;
+    }
+    sms_ = prop.multiProcessorCount;
+    if (!cuda_ok(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate")) return;
+    size_t free_b = 0, total_b = 0;
+    if (!cuda_ok(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo")) return;
+    int64_t budget = budget_bytes;
+    const int64_t cap = static_cast<int64_t>(free_b) - (static_cast<int64_t>(1) << 30);
+    if (budget <= 0 || budget > cap) budget = static_cast<int64_t>(cap * 0.9);
+    if (budget < (static_cast<int64_t>(64) << 20)) {
+        error_ = "not enough free device memory for the engine arena";
+        return;
+    }
+    if (!arena_.init(static_cast<size_t>(budget), &error_)) return;
+    d_err_ = static_cast<uint32_t *>(arena_.alloc(sizeof(uint32_t)));
+    if (!cuda_ok(cudaMemsetAsync(d_err_, 0, sizeof(uint32_t), stream_), "cudaMemsetAsync")) return;
+    if (max_slots_ <= 0) max_slots_ = 1 << 20;
+    // constant initial frontier: one zero point (up to 8 int64 values), offset 0, size 1
+    if (!h_init_.reserve(256)) {
+        error_ = "cudaMallocHost failed";
+        return;
+    }
+    std::memset(h_init_.p, 0, 256);
+    *reinterpret_cast<int32_t *>(static_cast<char *>(h_init_.p) + 128) = 1;
+    ok_ = true;
+}
+
+Engine::~Engine() {
+    if (stream_) {
+        cudaStreamSynchronize(stream_);
+        cudaStreamDestroy(stream_);
+    }
+}
+
+bool Engine::cuda_ok(cudaError_t e, const char *what) {
+    if (e == cudaSuccess) return true;
+    error_ = std::string(what) + " failed: " + cudaGetErrorString(e);
+    ok_ = false;
+    return false;
+}
+
+void *Engine::scratch(size_t bytes) {
+    void *p = arena_.alloc(bytes);
+    if (p) step_scratch_.push_back(p);
+    return p;
+}
+
+void Engine::submit(std::unique_ptr<Instance> inst) { queued_.push_back(std::move(inst)); }
+
+void Engine::release_side(Side &s) {
+    arena_.release(s.pts);
+    arena_.release(s.off);
+    arena_.release(s.size);
+    arena_.release(s.arc_off);
+    arena_.release(s.big_list);
+    s.pts = nullptr;
+    s.off = nullptr;
+    s.size = nullptr;
+    s.arc_off = nullptr;
+    s.big_list = nullptr;
+    s.counted = false;
+}
+
+void Engine::release_instance(Instance &I) {
+    release_side(I.td);
+    release_side(I.bu);
+    arena_.release(I.dd);
+    arena_.release(I.cu_U);
+    arena_.release(I.cu_keep);
+    arena_.release(I.cu_ctr);
+    I.dd = nullptr;
+    I.cu_U = nullptr;
+    I.cu_keep = nullptr;
+    I.cu_ctr = nullptr;
+    I.blob.clear();
+    I.blob.shrink_to_fit();
+}
+
+void Engine::fail(Instance &I, int status, const std::string &msg) {
+    I.status = status;
+    I.error = msg;
+    I.phase = Instance::DONE;
+}
+
+bool Engine::cancel(uint64_t id) {
+    for (auto it = queued_.begin(); it != queued_.end(); ++it) {
+        if ((*it)->id == id) {
+            fail(**it, PMDD_ERR_CANCELLED, "request cancelled");
+            (*it)->finish_s = now_s();
+            finished_.push_back(std::move(*it));
+            queued_.erase(it);
+            return true;
+        }
+    }
+    for (auto &p : active_) {
+        if (p && p->id == id && p->phase != Instance::DONE) {
+            fail(*p, PMDD_ERR_CANCELLED, "request cancelled");
+            return true;  // collected at the end of the next step
+        }
+    }
+    return false;
+}
+
+// Uploads the DD, builds the bottom-up CSR (method 3) and seeds the frontiers.
+bool Engine::admit(Instance &I) {
+    I.dd = static_cast<unsigned char *>(arena_.alloc(I.dev_bytes));
+    if (!I.dd) return false;
+    auto seed = [&](Side &s, int layer) -> bool {
+        s.layer = layer;
+        s.pts = arena_.alloc(8 * 8);
+        s.off = static_cast<int64_t *>(arena_.alloc(sizeof(int64_t)));
+        s.size = static_cast<int32_t *>(arena_.alloc(sizeof(int32_t)));
+        if (!s.pts || !s.off || !s.size) return false;
+        const char *h = static_cast<const char *>(h_init_.p);
+        cudaMemcpyAsync(s.pts, h, 64, cudaMemcpyHostToDevice, stream_);
+        cudaMemcpyAsync(s.off, h + 64, sizeof(int64_t), cudaMemcpyHostToDevice, stream_);
+        cudaMemcpyAsync(s.size, h + 128, sizeof(int32_t), cudaMemcpyHostToDevice, stream_);
+        s.counted = false;
+        s.score = 0;
+        return true;
+    };
+    if (!seed(I.td, 0) || (I.opts.method == 3 && !seed(I.bu, I.L - 1))) {
+        release_instance(I);
+        return false;
+    }
+    if (!cuda_ok(cudaMemcpyAsync(I.dd, I.blob.data(), I.blob_bytes, cudaMemcpyHostToDevice, stream_), "DD upload"))
+        return false;
+    I.d_in_off = reinterpret_cast<const int32_t *>(I.dd + I.off_in);
+    I.d_arc_src = reinterpret_cast<const int32_t *>(I.dd + I.off_src);
+    I.d_arc_w = reinterpret_cast<const int32_t *>(I.dd + I.off_w);
+    I.d_weights = reinterpret_cast<const int32_t *>(I.dd + I.off_weights);
+    if (I.opts.method == 3) {
+        size_t off = I.blob_bytes;
+        I.d_out_off = reinterpret_cast<int32_t *>(I.dd + off);
+        off = align256(off + sizeof(int32_t) * (static_cast<size_t>(I.N) + 1));
+        I.d_out_head = reinterpret_cast<int32_t *>(I.dd + off);
+        off = align256(off + sizeof(int32_t) * static_cast<size_t>(I.A));
+        I.d_out_w = reinterpret_cast<int32_t *>(I.dd + off);
+        off = align256(off + sizeof(int32_t) * static_cast<size_t>(I.A));
+        I.d_cursor = reinterpret_cast<int32_t *>(I.dd + off);
+        if (!cuda_ok(dev::launch_build_out_csr(I.d_in_off, I.d_arc_src, I.d_arc_w, I.N, I.A, I.d_out_off, I.d_cursor,
+                                               I.d_out_head, I.d_out_w, stream_),
+                     "out-arc CSR"))
+            return false;
+        launches_ += 3;
+    }
+    I.blob.clear();
+    I.blob.shrink_to_fit();
+    I.phase = Instance::RUNNING;
+    I.admit_s = now_s();
+    return true;
+}
+
+namespace {
+
+struct ExpPlan {
+    Instance *I;
+    bool td;
+    int nl;
+    void *out_pts;
+    int64_t *out_off;
+    int32_t *out_size;
+    void *big_pts;
+    int32_t *big_tag;
+    uint8_t *big_keep;
+};
+
+struct CountPlan {
+    Instance *I;
+    bool td;
+    bool after_expand;  // score update (false for the initial counts at admission)
+};
+
+}  // namespace
+
+std::atomic<int64_t> g_total_launches{0};
+
+int Engine::step() {
+    if (!ok_) return -1;
+    struct LaunchTally {
+        const int64_t &n;
+        int64_t start;
+        ~LaunchTally() { g_total_launches += n - start; }
+    } tally{launches_, launches_};
+    // ---------------------------------------------------------------- admission
+    std::vector<CountPlan> counts;
+    while (!queued_.empty() && static_cast<int>(active_.size()) < max_slots_) {
+        Instance &I = *queued_.front();
+        const bool room = static_cast<int64_t>(arena_.used()) + I.est_bytes <= static_cast<int64_t>(arena_.capacity());
+        if (!room && !active_.empty()) break;
+        if (!admit(I)) {
+            if (!ok_) return -1;
+            if (!active_.empty()) break;  // wait for memory to free up
+            fail(I, PMDD_ERR_OOM, "request does not fit the device memory budget");
+            I.finish_s = now_s();
+            finished_.push_back(std::move(queued_.front()));
+            queued_.pop_front();
+            continue;
+        }
+        counts.push_back({&I, true, false});
+        if (I.opts.method == 3) counts.push_back({&I, false, false});
+        active_.push_back(std::move(queued_.front()));
+        queued_.pop_front();
+    }
+
+    // ------------------------------------------------------------ expansions
+    std::vector<ExpPlan> exps;
+    int64_t blocked_need = -1;
+    Instance *blocked = nullptr;
+    for (auto &p : active_) {
+        Instance &I = *p;
+        if (I.phase != Instance::RUNNING) continue;
+        bool is_td = true;
+        if (I.opts.method == 3) is_td = I.td.score <= I.bu.score;
+        Side &s = is_td ? I.td : I.bu;
+        if (!s.counted) continue;
+        const int nl = is_td ? s.layer + 1 : s.layer - 1;
+        const int64_t C = s.res.total;
+        const int32_t V = I.nodes_in(nl);
+        ExpPlan e{&I, is_td, nl, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+        const size_t pts_bytes = static_cast<size_t>(std::max<int64_t>(C, 1)) * I.d * I.elem();
+        e.out_pts = arena_.alloc(pts_bytes);
+        e.out_off = static_cast<int64_t *>(arena_.alloc(sizeof(int64_t) * V));
+        e.out_size = static_cast<int32_t *>(arena_.alloc(sizeof(int32_t) * V));
+        bool okay = e.out_pts && e.out_off && e.out_size;
+        if (okay && s.res.num_big > 0) {
+            const int64_t bt = s.res.big_total;
+            e.big_pts = arena_.alloc(static_cast<size_t>(bt) * I.d * I.elem());
+            e.big_tag = static_cast<int32_t *>(arena_.alloc(sizeof(int32_t) * bt));
+            e.big_keep = static_cast<uint8_t *>(arena_.alloc(static_cast<size_t>(bt)));
+            okay = e.big_pts && e.big_tag && e.big_keep;
+        }
+        if (!okay) {
+            for (void *q : {e.out_pts, static_cast<void *>(e.out_off), static_cast<void *>(e.out_size), e.big_pts,
+                            static_cast<void *>(e.big_tag), static_cast<void *>(e.big_keep)})
+                arena_.release(q);
+            const int64_t need = static_cast<int64_t>(pts_bytes);
+            if (need > blocked_need) {
+                blocked_need = need;
+                blocked = &I;
+            }
+            continue;
+        }
+        exps.push_back(e);
+    }
+
+    // group by (d, wide) and build descriptors
+    std::map<std::pair<int, bool>, std::vector<size_t>> groups;
+    for (size_t i = 0; i < exps.size(); ++i) groups[{exps[i].I->d, exps[i].I->wide}].push_back(i);
+
+    // staging of every H2D payload of this step
+    size_t stage_bytes = 0;
+    stage_bytes += align256(sizeof(dev::ExpandJob) * exps.size());
+    stage_bytes += align256(sizeof(dev::BigWork) * 1);  // sized below per group
+    std::vector<dev::ExpandJob> xjobs(exps.size());
+    std::vector<dev::BigWork> bigwork;
+    struct GroupLaunch {
+        int d;
+        bool wide;
+        size_t first, count;       // into xjobs
+        int64_t tiles;
+        size_t big_first, big_count;
+        int64_t max_big;
+    };
+    std::vector<GroupLaunch> glaunch;
+    {
+        size_t pos = 0;
+        std::vector<ExpPlan> ordered;
+        ordered.reserve(exps.size());
+        for (auto &g : groups) {
+            GroupLaunch gl{g.first.first, g.first.second, pos, g.second.size(), 0, bigwork.size(), 0, 0};
+            for (size_t idx : g.second) {
+                const ExpPlan &e = exps[idx];
+                Instance &I = *e.I;
+                Side &s = e.td ? I.td : I.bu;
+                dev::ExpandJob &J = xjobs[pos];
+                std::memset(&J, 0, sizeof(J));
+                if (e.td) {
+                    J.item_arc_off = I.d_in_off;
+                    J.arc_nbr = I.d_arc_src;
+                    J.arc_wrow = I.d_arc_w;
+                    J.arc_base = I.arc_at_layer[e.nl];
+                } else {
+                    J.item_arc_off = I.d_out_off;
+                    J.arc_nbr = I.d_out_head;
+                    J.arc_wrow = I.d_out_w;
+                    J.arc_base = I.arc_at_layer[e.nl + 1];
+                }
+                J.weights = I.d_weights;
+                J.arc_cand_off = s.arc_off;
+                J.item_base = I.layer_off[e.nl];
+                J.num_items = I.nodes_in(e.nl);
+                J.prev_base = I.layer_off[s.layer];
+                J.prev_pts = s.pts;
+                J.prev_off = s.off;
+                J.prev_size = s.size;
+                J.out_pts = e.out_pts;
+                J.out_off = e.out_off;
+                J.out_size = e.out_size;
+                J.total_cand = s.res.total;
+                J.num_tiles = std::max<int64_t>(1, (s.res.total + dev::kTileWindow - 1) / dev::kTileWindow);
+                J.tile_base = gl.tiles;
+                gl.tiles += J.num_tiles;
+                J.big_list = s.big_list;
+                J.num_big = s.res.num_big;
+                J.big_pts = e.big_pts;
+                J.big_tag = e.big_tag;
+                J.big_keep = e.big_keep;
+                J.err = d_err_;
+                for (int b = 0; b < s.res.num_big; ++b) bigwork.push_back({static_cast<int32_t>(pos - gl.first), b});
+                if (s.res.num_big > 0) gl.max_big = std::max(gl.max_big, s.res.max_item);
+                ordered.push_back(e);
+                ++pos;
+            }
+            gl.big_count = bigwork.size() - gl.big_first;
+            glaunch.push_back(gl);
+        }
+        exps.swap(ordered);
+    }
+
+    // count plans for sides that move this step
+    for (const ExpPlan &e : exps) {
+        Instance &I = *e.I;
+        if (I.opts.method == 1) {
+            if (e.nl < I.L - 1) counts.push_back({&I, true, true});
+        } else {
+            const int td_layer = e.td ? e.nl : I.td.layer;
+            const int bu_layer = e.td ? I.bu.layer : e.nl;
+            if (td_layer != bu_layer) counts.push_back({&I, e.td, true});
+        }
+    }
+    std::vector<dev::CountJob> cjobs(counts.size());
+    std::vector<int64_t *> new_arc_off(counts.size(), nullptr);
+    std::vector<int64_t *> new_big(counts.size(), nullptr);
+    dev::CountResult *d_results = nullptr;
+    if (!counts.empty()) d_results = static_cast<dev::CountResult *>(scratch(sizeof(dev::CountResult) * counts.size()));
+    bool count_alloc_ok = counts.empty() || d_results != nullptr;
+    // the expansion's new frontier is what the count reads; resolve per plan below
+
+    // ------------------------------------------------------------- staging
+    const size_t off_x = 0;
+    const size_t off_b = align256(off_x + sizeof(dev::ExpandJob) * xjobs.size());
+    const size_t off_c = align256(off_b + sizeof(dev::BigWork) * bigwork.size());
+    size_t off_k = align256(off_c + sizeof(dev::CountJob) * cjobs.size());
+    // coupling: requests at their cutset
+    std::vector<Instance *> couplers;
+    for (auto &p : active_)
+        if (p->phase == Instance::COUPLING) couplers.push_back(p.get());
+    // (requests entering coupling this step are appended after the expansion bookkeeping)
+
+    // --------------------------------------------------- finish planning of counts
+    // Counts read the frontier a side will have after this step's expansions.
+    auto side_after = [&](Instance &I, bool td) -> std::pair<int, int32_t *> {
+        for (const ExpPlan &e : exps)
+            if (e.I == &I && e.td == td) return {e.nl, e.out_size};
+        Side &s = td ? I.td : I.bu;
+        return {s.layer, s.size};
+    };
+    for (size_t k = 0; k < counts.size() && count_alloc_ok; ++k) {
+        Instance &I = *counts[k].I;
+        const bool td = counts[k].td;
+        auto cur = side_after(I, td);
+        const int l = cur.first;
+        const int nl = td ? l + 1 : l - 1;
+        dev::CountJob &J = cjobs[k];
+        std::memset(&J, 0, sizeof(J));
+        if (td) {
+            J.item_arc_off = I.d_in_off;
+            J.arc_nbr = I.d_arc_src;
+            J.arc_base = I.arc_at_layer[nl];
+            J.num_arcs = I.arc_at_layer[nl + 1] - I.arc_at_layer[nl];
+        } else {
+            J.item_arc_off = I.d_out_off;
+            J.arc_nbr = I.d_out_head;
+            J.arc_base = I.arc_at_layer[nl + 1];
+            J.num_arcs = I.arc_at_layer[nl + 2] - I.arc_at_layer[nl + 1];
+        }
+        J.item_base = I.layer_off[nl];
+        J.num_items = I.nodes_in(nl);
+        J.cur_base = I.layer_off[l];
+        J.cur_nodes = I.nodes_in(l);
+        J.cur_size = cur.second;
+        new_arc_off[k] = static_cast<int64_t *>(arena_.alloc(sizeof(int64_t) * (static_cast<size_t>(J.num_arcs) + 1)));
+        new_big[k] = static_cast<int64_t *>(arena_.alloc(sizeof(int64_t) * 2 * std::max(1, J.num_items)));
+        if (!new_arc_off[k] || !new_big[k]) {
+            count_alloc_ok = false;
+            break;
+        }
+        J.arc_cand_off = new_arc_off[k];
+        J.big_list = new_big[k];
+        J.result = d_results + k;
+    }
+    if (!count_alloc_ok) {
+        // Out of device memory for bookkeeping: give everything back and fail the
+        // largest blocked request so the others can progress next step.
+        for (size_t k = 0; k < counts.size(); ++k) {
+            arena_.release(new_arc_off[k]);
+            arena_.release(new_big[k]);
+        }
+        for (const ExpPlan &e : exps) {
+            for (void *q : {e.out_pts, static_cast<void *>(e.out_off), static_cast<void *>(e.out_size), e.big_pts,
+                            static_cast<void *>(e.big_tag), static_cast<void *>(e.big_keep)})
+                arena_.release(q);
+        }
+        for (void *q : step_scratch_) arena_.release(q);
+        step_scratch_.clear();
+        Instance *victim = exps.empty() ? (counts.empty() ? nullptr : counts.back().I) : exps.back().I;
+        if (victim) fail(*victim, PMDD_ERR_OOM, "device memory budget exhausted");
+        int done = 0;
+        for (auto it = active_.begin(); it != active_.end();) {
+            if ((*it)->phase == Instance::DONE) {
+                release_instance(**it);
+                (*it)->finish_s = now_s();
+                finished_.push_back(std::move(*it));
+                it = active_.erase(it);
+                ++done;
+            } else {
+                ++it;
+            }
+        }
+        return done;
+    }
+
+    // requests whose sides meet this step enter coupling now
+    std::vector<Instance *> entering;
+    for (const ExpPlan &e : exps) {
+        Instance &I = *e.I;
+        if (I.opts.method != 3) continue;
+        const int td_layer = e.td ? e.nl : I.td.layer;
+        const int bu_layer = e.td ? I.bu.layer : e.nl;
+        if (td_layer == bu_layer) entering.push_back(&I);
+    }
+
+    // coupling descriptors (built after the expansion bookkeeping below swaps sides)
+    const size_t n_couple_max = couplers.size() + entering.size();
+    const size_t off_u = off_k;  // CoupleJob array
+    const size_t off_ctrinit = align256(off_u + sizeof(dev::CoupleJob) * n_couple_max);
+    stage_bytes = align256(off_ctrinit + sizeof(int64_t) * dev::kCtrCount * n_couple_max);
+    if (!h_desc_.reserve(stage_bytes)) {
+        error_ = "cudaMallocHost failed";
+        ok_ = false;
+        return -1;
+    }
+    char *hs = static_cast<char *>(h_desc_.p);
+    if (!xjobs.empty()) std::memcpy(hs + off_x, xjobs.data(), sizeof(dev::ExpandJob) * xjobs.size());
+    if (!bigwork.empty()) std::memcpy(hs + off_b, bigwork.data(), sizeof(dev::BigWork) * bigwork.size());
+    if (!cjobs.empty()) std::memcpy(hs + off_c, cjobs.data(), sizeof(dev::CountJob) * cjobs.size());
+
+    // ------------------------------------------------- expansion bookkeeping
+    // Sides move to their new layer now (host view); device work is stream-ordered.
+    std::vector<Instance *> finishing;  // method 1 reached the terminal
+    std::vector<void *> to_release;
+    for (const ExpPlan &e : exps) {
+        Instance &I = *e.I;
+        Side &s = e.td ? I.td : I.bu;
+        to_release.push_back(s.pts);
+        to_release.push_back(s.off);
+        to_release.push_back(s.size);
+        to_release.push_back(s.arc_off);
+        to_release.push_back(s.big_list);
+        to_release.push_back(e.big_pts);
+        to_release.push_back(e.big_tag);
+        to_release.push_back(e.big_keep);
+        I.stats.work_candidates_total += s.res.total;
+        I.stats.work_candidates_peak = std::max(I.stats.work_candidates_peak, s.res.total);
+        s.pts = e.out_pts;
+        s.off = e.out_off;
+        s.size = e.out_size;
+        s.arc_off = nullptr;
+        s.big_list = nullptr;
+        s.counted = false;
+        s.layer = e.nl;
+        if (e.td) I.stats.layers_td++;
+        else I.stats.layers_bu++;
+        if (I.opts.method == 1 && e.nl == I.L - 1) finishing.push_back(&I);
+    }
+    for (Instance *I : entering) {
+        I->phase = Instance::COUPLING;
+        I->stats.layer_coupling = I->td.layer;
+        I->stats.cutset_size = I->nodes_in(I->td.layer);
+        // running frontier + one round of survivors
+        const int64_t ucap = std::max<int64_t>(std::max<int64_t>(I->opts.max_prod, 1 << 16), 1 << 18);
+        I->cu_ucap = ucap;
+        I->cu_U = arena_.alloc(static_cast<size_t>(ucap) * I->d * I->elem());
+        I->cu_keep = static_cast<uint8_t *>(arena_.alloc(static_cast<size_t>(ucap)));
+        I->cu_ctr = static_cast<int64_t *>(arena_.alloc(sizeof(int64_t) * dev::kCtrCount));
+        if (!I->cu_U || !I->cu_keep || !I->cu_ctr) {
+            fail(*I, PMDD_ERR_OOM, "device memory budget exhausted at the cutset join");
+            continue;
+        }
+        couplers.push_back(I);
+    }
+    std::vector<dev::CoupleJob> ujobs;
+    std::vector<Instance *> ujob_inst;
+    std::vector<int> ujob_new;
+    for (Instance *I : couplers) {
+        if (I->phase != Instance::COUPLING) continue;
+        dev::CoupleJob J;
+        std::memset(&J, 0, sizeof(J));
+        J.td_pts = I->td.pts;
+        J.td_off = I->td.off;
+        J.td_size = I->td.size;
+        J.bu_pts = I->bu.pts;
+        J.bu_off = I->bu.off;
+        J.bu_size = I->bu.size;
+        J.num_nodes = I->nodes_in(I->td.layer);
+        J.U = I->cu_U;
+        J.ucap = I->cu_ucap;
+        J.keep = I->cu_keep;
+        J.ctr = I->cu_ctr;
+        const bool is_new = std::find(entering.begin(), entering.end(), I) != entering.end();
+        int64_t *ci = reinterpret_cast<int64_t *>(hs + off_ctrinit) + dev::kCtrCount * ujobs.size();
+        std::memset(ci, 0, sizeof(int64_t) * dev::kCtrCount);
+        ci[dev::kCtrResume] = J.num_nodes;
+        ci[dev::kCtrValidEnd] = J.ucap;
+        ujobs.push_back(J);
+        ujob_inst.push_back(I);
+        ujob_new.push_back(is_new ? 1 : 0);
+    }
+    if (!ujobs.empty()) std::memcpy(hs + off_u, ujobs.data(), sizeof(dev::CoupleJob) * ujobs.size());
+
+    // ----------------------------------------------------------- device work
+    char *d_stage = stage_bytes ? static_cast<char *>(scratch(stage_bytes)) : nullptr;
+    // summary layout (D2H): count results | coupling ctrs | finishing sizes | error word
+    const size_t s_counts = 0;
+    const size_t s_ctr = align256(s_counts + sizeof(dev::CountResult) * counts.size());
+    const size_t s_fin = align256(s_ctr + sizeof(int64_t) * dev::kCtrCount * ujobs.size());
+    const size_t s_err = align256(s_fin + sizeof(int32_t) * finishing.size());
+    const size_t s_total = s_err + sizeof(uint32_t);
+    if ((stage_bytes && !d_stage) || !h_summary_.reserve(s_total)) {
+        error_ = "engine bookkeeping allocation failed";
+        ok_ = false;
+        return -1;
+    }
+    cudaEvent_t ev0, ev1, ev2, ev3;
+    cudaEventCreate(&ev0);
+    cudaEventCreate(&ev1);
+    cudaEventCreate(&ev2);
+    cudaEventCreate(&ev3);
+    if (stage_bytes && !cuda_ok(cudaMemcpyAsync(d_stage, hs, stage_bytes, cudaMemcpyHostToDevice, stream_), "H2D"))
+        return -1;
+    // coupling counters of requests that just reached their cutset start from the staged init values
+    for (size_t k = 0; k < ujobs.size(); ++k) {
+        if (!ujob_new[k]) continue;
+        cudaMemcpyAsync(ujobs[k].ctr, d_stage + off_ctrinit + sizeof(int64_t) * dev::kCtrCount * k,
+                        sizeof(int64_t) * dev::kCtrCount, cudaMemcpyDeviceToDevice, stream_);
+    }
+    cudaEventRecord(ev0, stream_);
+    for (const GroupLaunch &gl : glaunch) {
+        const dev::ExpandJob *dj = reinterpret_cast<const dev::ExpandJob *>(d_stage + off_x) + gl.first;
+        const int grid = sms_ * 4;
+        if (!cuda_ok(dev::launch_expand_tiles(gl.d, gl.wide, dj, static_cast<int>(gl.count), gl.tiles, grid, stream_),
+                     "expand_tile_kernel"))
+            return -1;
+        launches_ += 1;
+    }
+    cudaEventRecord(ev1, stream_);
+    for (const GroupLaunch &gl : glaunch) {
+        if (gl.big_count == 0) continue;
+        const dev::ExpandJob *dj = reinterpret_cast<const dev::ExpandJob *>(d_stage + off_x) + gl.first;
+        const dev::BigWork *bw = reinterpret_cast<const dev::BigWork *>(d_stage + off_b) + gl.big_first;
+        if (!cuda_ok(dev::launch_big(gl.d, gl.wide, dj, bw, static_cast<int>(gl.big_count), gl.max_big, sms_, stream_),
+                     "oversized-destination kernels"))
+            return -1;
+        launches_ += 3;
+    }
+    cudaEventRecord(ev2, stream_);
+    if (!cjobs.empty()) {
+        if (!cuda_ok(dev::launch_count_scan(reinterpret_cast<const dev::CountJob *>(d_stage + off_c),
+                                            static_cast<int>(cjobs.size()), stream_),
+                     "count_scan_kernel"))
+            return -1;
+        launches_ += 1;
+    }
+    // coupling rounds, grouped by (d, wide)
+    {
+        std::map<std::pair<int, bool>, std::vector<size_t>> ug;
+        for (size_t k = 0; k < ujobs.size(); ++k) ug[{ujob_inst[k]->d, ujob_inst[k]->wide}].push_back(k);
+        const dev::CoupleJob *du = reinterpret_cast<const dev::CoupleJob *>(d_stage + off_u);
+        // new requests: product statistics once
+        for (size_t k = 0; k < ujobs.size(); ++k) {
+            if (!ujob_new[k]) continue;
+            dev::launch_couple_products(du + k, 1, stream_);
+            launches_ += 1;
+        }
+        for (auto &g : ug) {
+            // jobs of one group are contiguous only if sorted; launch per job run
+            size_t i = 0;
+            while (i < g.second.size()) {
+                size_t j = i;
+                while (j + 1 < g.second.size() && g.second[j + 1] == g.second[j] + 1) ++j;
+                const int n = static_cast<int>(j - i + 1);
+                const int per = std::max(1, (sms_ * 2) / n);
+                if (!cuda_ok(dev::launch_couple_round(g.first.first, g.first.second, du + g.second[i], n, per, stream_),
+                             "coupling round"))
+                    return -1;
+                launches_ += 3;
+                i = j + 1;
+            }
+        }
+    }
+    cudaEventRecord(ev3, stream_);
+    char *hsum = static_cast<char *>(h_summary_.p);
+    if (!counts.empty())
+        cudaMemcpyAsync(hsum + s_counts, d_results, sizeof(dev::CountResult) * counts.size(), cudaMemcpyDeviceToHost,
+                        stream_);
+    for (size_t k = 0; k < ujobs.size(); ++k)
+        cudaMemcpyAsync(hsum + s_ctr + sizeof(int64_t) * dev::kCtrCount * k, ujobs[k].ctr,
+                        sizeof(int64_t) * dev::kCtrCount, cudaMemcpyDeviceToHost, stream_);
+    for (size_t k = 0; k < finishing.size(); ++k)
+        cudaMemcpyAsync(hsum + s_fin + sizeof(int32_t) * k, finishing[k]->td.size, sizeof(int32_t),
+                        cudaMemcpyDeviceToHost, stream_);
+    cudaMemcpyAsync(hsum + s_err, d_err_, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream_);
+    for (void *q : to_release) arena_.release(q);
+    const cudaError_t se = cudaStreamSynchronize(stream_);
+    if (!cuda_ok(se, "engine step")) {
+        for (auto &p : active_) fail(*p, PMDD_ERR_CUDA, error_);
+        return -1;
+    }
+    float ms_expand = 0, ms_big = 0, ms_rest = 0;
+    cudaEventElapsedTime(&ms_expand, ev0, ev1);
+    cudaEventElapsedTime(&ms_big, ev1, ev2);
+    cudaEventElapsedTime(&ms_rest, ev2, ev3);
+    cudaEventDestroy(ev0);
+    cudaEventDestroy(ev1);
+    cudaEventDestroy(ev2);
+    cudaEventDestroy(ev3);
+    for (void *q : step_scratch_) arena_.release(q);
+    step_scratch_.clear();
+
+    // ----------------------------------------------------------- host updates
+    const uint32_t errw = *reinterpret_cast<uint32_t *>(hsum + s_err);
+    if (errw != 0) {
+        cudaMemsetAsync(d_err_, 0, sizeof(uint32_t), stream_);
+        for (auto &p : active_)
+            if (p->phase != Instance::DONE) fail(*p, PMDD_ERR_INTERNAL, "device-side index check failed");
+    }
+    for (const ExpPlan &e : exps) {
+        e.I->stats.kernel_expand_td_s += ms_expand * 1e-3;
+        e.I->stats.kernel_dominance_s += ms_big * 1e-3;
+        e.I->stats.kernel_total_s += (ms_expand + ms_big + ms_rest) * 1e-3;
+    }
+    const dev::CountResult *hres = reinterpret_cast<const dev::CountResult *>(hsum + s_counts);
+    for (size_t k = 0; k < counts.size(); ++k) {
+        Instance &I = *counts[k].I;
+        Side &s = counts[k].td ? I.td : I.bu;
+        s.arc_off = new_arc_off[k];
+        s.big_list = new_big[k];
+        s.res = hres[k];
+        s.counted = true;
+        if (counts[k].after_expand) {
+            s.score = counts[k].td ? s.res.total : static_cast<int64_t>(1.5 * static_cast<double>(s.res.total));
+            I.stats.work_frontier_survivors_total += s.res.cur_total;
+            I.stats.work_frontier_peak_points = std::max(I.stats.work_frontier_peak_points, s.res.cur_total);
+        }
+    }
+    for (size_t k = 0; k < finishing.size(); ++k) {
+        Instance &I = *finishing[k];
+        if (I.phase == Instance::DONE) continue;
+        const int32_t n = *reinterpret_cast<const int32_t *>(hsum + s_fin + sizeof(int32_t) * k);
+        I.result_n = n;
+        I.result.resize(static_cast<size_t>(n) * I.d * I.elem());
+        if (n > 0 && !cuda_ok(cudaMemcpy(I.result.data(), I.td.pts, I.result.size(), cudaMemcpyDeviceToHost), "D2H"))
+            return -1;
+        I.stats.work_frontier_survivors_total += n;
+        I.stats.work_frontier_peak_points = std::max<int64_t>(I.stats.work_frontier_peak_points, n);
+        I.phase = Instance::DONE;
+    }
+    for (size_t k = 0; k < ujobs.size(); ++k) {
+        Instance &I = *ujob_inst[k];
+        if (I.phase == Instance::DONE) continue;
+        const int64_t *c = reinterpret_cast<const int64_t *>(hsum + s_ctr + sizeof(int64_t) * dev::kCtrCount * k);
+        I.couple_rounds++;
+        if (ujob_new[k]) I.stats.work_join_products_total = c[dev::kCtrProducts];
+        if (c[dev::kCtrDone]) {
+            const int64_t n = c[dev::kCtrF];
+            I.result_n = n;
+            I.result.resize(static_cast<size_t>(n) * I.d * I.elem());
+            if (n > 0 && !cuda_ok(cudaMemcpy(I.result.data(), I.cu_U, I.result.size(), cudaMemcpyDeviceToHost), "D2H"))
+                return -1;
+            I.stats.work_frontier_survivors_total += n;
+            I.stats.work_frontier_peak_points = std::max<int64_t>(I.stats.work_frontier_peak_points, n);
+            I.phase = Instance::DONE;
+        } else if (c[dev::kCtrF] > I.cu_ucap / 2) {
+            // the running frontier crowds out the survivors of a round: grow U
+            const int64_t ncap = I.cu_ucap * 2;
+            void *nU = arena_.alloc(static_cast<size_t>(ncap) * I.d * I.elem());
+            uint8_t *nk = static_cast<uint8_t *>(arena_.alloc(static_cast<size_t>(ncap)));
+            if (!nU || !nk) {
+                arena_.release(nU);
+                arena_.release(nk);
+                fail(I, PMDD_ERR_OOM, "device memory budget exhausted growing the cutset frontier");
+                continue;
+            }
+            cudaMemcpyAsync(nU, I.cu_U, static_cast<size_t>(c[dev::kCtrF]) * I.d * I.elem(), cudaMemcpyDeviceToDevice,
+                            stream_);
+            int64_t upd[2] = {ncap, 0};
+            (void)upd;
+            arena_.release(I.cu_U);
+            arena_.release(I.cu_keep);
+            I.cu_U = nU;
+            I.cu_keep = nk;
+            I.cu_ucap = ncap;
+            // ValidEnd must follow the capacity
+            int64_t *hv = reinterpret_cast<int64_t *>(h_init_.p) + 24;  // scratch slot in the init block
+            *hv = ncap;
+            cudaMemcpyAsync(I.cu_ctr + dev::kCtrValidEnd, hv, sizeof(int64_t), cudaMemcpyHostToDevice, stream_);
+            cudaStreamSynchronize(stream_);
+        }
+    }
+    if (blocked && exps.empty() && ujobs.empty() && counts.empty()) {
+        // nothing could move: the largest blocked request cannot fit next to the others
+        fail(*blocked, PMDD_ERR_OOM, "device memory budget exhausted (layer does not fit)");
+    }
+    int done = 0;
+    for (auto it = active_.begin(); it != active_.end();) {
+        if ((*it)->phase == Instance::DONE) {
+            Instance &I = **it;
+            I.stats.gpu_mem_peak_used_bytes = static_cast<int64_t>(arena_.peak());
+            I.stats.gpu_mem_peak_reserved_bytes = static_cast<int64_t>(arena_.capacity());
+            release_instance(I);
+            I.finish_s = now_s();
+            finished_.push_back(std::move(*it));
+            it = active_.erase(it);
+            ++done;
+        } else {
+            ++it;
+        }
+    }
+    return done;
+}
+
+}  // namespace pmdd

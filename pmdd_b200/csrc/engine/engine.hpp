@@ -1,0 +1,157 @@
+// Host side of the B200 enumeration engine: a device-memory arena, per-request device
+// state, and the step scheduler that advances every admitted request by one layer per
+// step in shared launches (continuous batching).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <chrono>
+#include <cstdint>
+#include <deque>
+#include <map>
+#include <memory>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "common.cuh"
+#include "couple.cuh"
+#include "kernels.cuh"
+#include "pmdd.h"
+
+namespace pmdd {
+
+double now_s();
+
+// Kernels launched by every engine of this process.
+extern std::atomic<int64_t> g_total_launches;
+
+// First-fit allocator over one device allocation.  Bookkeeping is host-side; every
+// kernel of the engine runs on one stream, so memory released on the host may be
+// handed out again immediately (later work on the stream runs after earlier work).
+class Arena {
+  public:
+    ~Arena();
+    bool init(size_t bytes, std::string *err);
+    void *alloc(size_t bytes);
+    void release(void *p);
+    size_t capacity() const { return cap_; }
+    size_t used() const { return used_; }
+    size_t peak() const { return peak_; }
+    void reset_peak() { peak_ = used_; }
+
+  private:
+    char *base_ = nullptr;
+    size_t cap_ = 0, used_ = 0, peak_ = 0;
+    std::map<size_t, size_t> free_;             // offset -> bytes
+    std::unordered_map<size_t, size_t> live_;   // offset -> bytes
+};
+
+// Frontiers of one direction at its current layer, in slot layout: node i's points
+// live at pts[off[i] .. off[i]+size[i]) (D values each).
+struct Side {
+    int layer = -1;
+    void *pts = nullptr;
+    int64_t *off = nullptr;
+    int32_t *size = nullptr;
+    // counts for the next layer in this direction
+    bool counted = false;
+    int64_t *arc_off = nullptr;
+    int64_t *big_list = nullptr;
+    dev::CountResult res{};
+    int64_t score = 0;
+};
+
+struct Instance {
+    enum Phase { QUEUED, RUNNING, COUPLING, DONE };
+    uint64_t id = 0;
+    pmdd_options opts{};
+    int d = 0;
+    bool wide = false;
+    int32_t L = 0, N = 0, A = 0, K = 0;
+    std::vector<int32_t> layer_off;     // L+1
+    std::vector<int32_t> arc_at_layer;  // L+1: in-arcs of layers < l
+    std::vector<unsigned char> blob;    // packed DD arrays, uploaded at admission
+    size_t off_layer = 0, off_in = 0, off_src = 0, off_w = 0, off_weights = 0, off_minw = 0, blob_bytes = 0;
+    size_t dev_bytes = 0;               // blob + out-arc CSR
+    // device DD
+    unsigned char *dd = nullptr;
+    const int32_t *d_in_off = nullptr, *d_arc_src = nullptr, *d_arc_w = nullptr, *d_weights = nullptr;
+    int32_t *d_out_off = nullptr, *d_out_head = nullptr, *d_out_w = nullptr, *d_cursor = nullptr;
+    Side td, bu;
+    Phase phase = QUEUED;
+    // coupling state
+    void *cu_U = nullptr;
+    uint8_t *cu_keep = nullptr;
+    int64_t *cu_ctr = nullptr;
+    int64_t cu_ucap = 0;
+    int couple_rounds = 0;
+    // outcome
+    int status = PMDD_OK;
+    std::string error;
+    std::vector<unsigned char> result;  // num_points * d * elem
+    int64_t result_n = 0;
+    pmdd_stats stats{};
+    double submit_s = 0, admit_s = 0, finish_s = 0;
+    int64_t est_bytes = 0;              // admission estimate
+
+    size_t elem() const { return wide ? 8 : 4; }
+    int32_t nodes_in(int l) const { return layer_off[l + 1] - layer_off[l]; }
+};
+
+// Validates a flat DD and packs it into an Instance (host side only).
+int prepare_instance(const pmdd_dd &dd, const pmdd_options &opts, uint64_t id, Instance *inst, std::string *err);
+
+class Engine {
+  public:
+    Engine(int device, int64_t budget_bytes, int max_slots);
+    ~Engine();
+    bool ok() const { return ok_; }
+    const std::string &error() const { return error_; }
+
+    // Takes ownership; the instance waits in the queue until it fits.
+    void submit(std::unique_ptr<Instance> inst);
+    // One engine step; returns the number of requests that finished during it, or -1
+    // on an engine-wide CUDA failure.
+    int step();
+    bool idle() const { return queued_.empty() && active_.empty(); }
+    size_t queued() const { return queued_.size(); }
+    size_t running() const { return active_.size(); }
+    std::deque<std::unique_ptr<Instance>> &finished() { return finished_; }
+    bool cancel(uint64_t id);
+    int64_t launches() const { return launches_; }
+    const Arena &arena() const { return arena_; }
+    int device() const { return device_; }
+
+  private:
+    struct Pinned {
+        void *p = nullptr;
+        size_t cap = 0;
+        bool reserve(size_t bytes);
+        ~Pinned();
+    };
+    bool admit(Instance &I);
+    void fail(Instance &I, int status, const std::string &msg);
+    void release_instance(Instance &I);
+    void release_side(Side &s);
+    bool cuda_ok(cudaError_t e, const char *what);
+    void *scratch(size_t bytes);  // step-lifetime device memory
+
+    bool ok_ = false;
+    std::string error_;
+    int device_ = 0;
+    int sms_ = 148;
+    int max_slots_ = 0;
+    cudaStream_t stream_ = nullptr;
+    Arena arena_;
+    std::deque<std::unique_ptr<Instance>> queued_;
+    std::vector<std::unique_ptr<Instance>> active_;
+    std::deque<std::unique_ptr<Instance>> finished_;
+    std::vector<void *> step_scratch_;
+    Pinned h_desc_, h_summary_, h_init_;
+    uint32_t *d_err_ = nullptr;
+    int64_t launches_ = 0;
+};
+
+}  // namespace pmdd

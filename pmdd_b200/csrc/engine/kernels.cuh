@@ -1,0 +1,17 @@
+// Launchers of the enumeration kernels (kernels.cu, couple.cu).  `d` selects the
+// objective count (1..8), `wide` the int64 point type.
+#pragma once
+
+#include "common.cuh"
+
+namespace pmdd {
+namespace dev {
+
+cudaError_t launch_count_scan(const CountJob *jobs, int num_jobs, cudaStream_t stream);
+cudaError_t launch_expand_tiles(int d, bool wide, const ExpandJob *jobs, int num_jobs, int64_t total_tiles, int grid,
+                                cudaStream_t stream);
+cudaError_t launch_big(int d, bool wide, const ExpandJob *jobs, const BigWork *work, int num_work, int64_t max_item,
+                       int sms, cudaStream_t stream);
+
+}  // namespace dev
+}  // namespace pmdd

@@ -1,0 +1,132 @@
+"""Python mirror of the reference's GPU enumeration seam.
+
+The reference (src/pmdd/enum/gpu/cuda_wrappers.hpp:11-21) exposes four functions; each
+returns a new ParetoFrontier or NULL with *reason set.  Here each returns the frontier
+as an (F, nobjs) integer array and raises `CudaEnumerationError` (carrying the reason)
+on failure.  `stats`, when given, is a dict updated in place with the GPU fields of
+the reference's EnumerationStats.  The frontier comes back unsorted; the reference's
+main sorts it afterwards (`sort_lexicographic_ascending`).
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Iterable, Optional
+
+import numpy as np
+
+from . import _native
+from .dd import DecisionDiagram
+
+DEFAULT_MAX_CAND = 20_000_000   # --max-cand default (src/pmdd/util/cli_parser.hpp:10)
+DEFAULT_MAX_PROD = 625_000      # --max-prod default (src/pmdd/util/cli_parser.hpp:11)
+
+
+class CudaEnumerationError(RuntimeError):
+    def __init__(self, status: int, reason: str):
+        super().__init__(f"GPU enumeration failed ({_native.STATUS_NAMES.get(status, status)}): {reason}")
+        self.status = status
+        self.reason = reason
+
+
+def _options(method, problem_type, state_dominance, maximization, max_cand, max_prod, device):
+    o = _native.PmddOptions()
+    _native.gpu_lib().pmdd_options_default(ctypes.byref(o))
+    o.method = method
+    o.problem_type = problem_type
+    o.state_dominance = state_dominance
+    o.maximization = 1 if maximization else 0
+    o.max_cand = int(max_cand)
+    o.max_prod = int(max_prod)
+    o.device = device
+    return o
+
+
+def _to_array(fr: _native.PmddFrontier) -> np.ndarray:
+    n, d = fr.num_points, fr.nobjs
+    dtype = np.int64 if fr.elem_bytes == 8 else np.int32
+    if n == 0 or not fr.points:
+        return np.zeros((0, d), dtype=dtype)
+    buf = (ctypes.c_char * (n * d * fr.elem_bytes)).from_address(fr.points)
+    return np.frombuffer(buf, dtype=dtype).reshape(n, d).copy()
+
+
+def enumerate_dd(dd: DecisionDiagram, method: int = 1, problem_type: Optional[int] = None,
+                 state_dominance: int = 0, maximization: bool = True, max_cand: int = DEFAULT_MAX_CAND,
+                 max_prod: int = DEFAULT_MAX_PROD, device: int = 0, stats: Optional[dict] = None) -> np.ndarray:
+    """One frontier through pmdd_enumerate (the C ABI)."""
+    lib = _native.gpu_lib()
+    o = _options(method, problem_type or dd.problem_type, state_dominance, maximization, max_cand, max_prod, device)
+    fr = _native.PmddFrontier()
+    st = _native.PmddStats()
+    err = ctypes.create_string_buffer(512)
+    view = dd.view
+    rc = lib.pmdd_enumerate(ctypes.byref(view), ctypes.byref(o), ctypes.byref(fr), ctypes.byref(st), err, len(err))
+    if rc != _native.PMDD_OK:
+        raise CudaEnumerationError(rc, err.value.decode(errors="replace"))
+    try:
+        out = _to_array(fr)
+    finally:
+        lib.pmdd_frontier_free(ctypes.byref(fr))
+    if stats is not None:
+        stats.update(st.as_dict())
+    return out
+
+
+def enumerate_batch(dds: Iterable[DecisionDiagram], method: int = 1, state_dominance: int = 0,
+                    max_cand: int = DEFAULT_MAX_CAND, max_prod: int = DEFAULT_MAX_PROD, device: int = 0,
+                    stats: Optional[dict] = None) -> list:
+    """Frontiers of many DDs, advanced together in shared launches."""
+    dds = list(dds)
+    lib = _native.gpu_lib()
+    n = len(dds)
+    views = (_native.PmddDD * max(n, 1))()
+    for i, dd in enumerate(dds):
+        views[i] = dd.view
+    ptype = dds[0].problem_type if dds else 1
+    o = _options(method, ptype, state_dominance, True, max_cand, max_prod, device)
+    outs = (_native.PmddFrontier * max(n, 1))()
+    status = (ctypes.c_int32 * max(n, 1))()
+    st = _native.PmddStats()
+    err = ctypes.create_string_buffer(512)
+    rc = lib.pmdd_enumerate_batch(views, n, ctypes.byref(o), outs, status, ctypes.byref(st), err, len(err))
+    try:
+        if rc != _native.PMDD_OK:
+            raise CudaEnumerationError(rc, err.value.decode(errors="replace"))
+        res = [_to_array(outs[i]) for i in range(n)]
+    finally:
+        for i in range(n):
+            lib.pmdd_frontier_free(ctypes.byref(outs[i]))
+    if stats is not None:
+        stats.update(st.as_dict())
+    return res
+
+
+# ---------------------------------------------------------------- the seam mirror
+def topdown_cuda_enumerate(bdd: DecisionDiagram, maximization: bool = True, problem_type: int = 1,
+                           state_dominance: int = 0, stats: Optional[dict] = None,
+                           gpu_batch_size: int = DEFAULT_MAX_CAND) -> np.ndarray:
+    """Method 1 on a BDD (reference: topdown_cuda_enumerate, src/pmdd/enum/gpu/enum.cu:55-63)."""
+    return enumerate_dd(bdd, 1, problem_type, state_dominance, maximization, gpu_batch_size, DEFAULT_MAX_PROD,
+                        stats=stats)
+
+
+def topdown_mdd_cuda_enumerate(mdd: DecisionDiagram, stats: Optional[dict] = None,
+                               gpu_batch_size: int = DEFAULT_MAX_CAND) -> np.ndarray:
+    """Method 1 on an MDD (reference: topdown_mdd_cuda_enumerate, src/pmdd/enum/gpu/enum.cu:65-71)."""
+    return enumerate_dd(mdd, 1, 3, 0, True, gpu_batch_size, DEFAULT_MAX_PROD, stats=stats)
+
+
+def coupled_cuda_enumerate(mdd: DecisionDiagram, stats: Optional[dict] = None,
+                           gpu_batch_size: int = DEFAULT_MAX_CAND,
+                           gpu_max_prod: int = DEFAULT_MAX_PROD) -> np.ndarray:
+    """Method 3 on an MDD (reference: coupled_cuda_enumerate, src/pmdd/enum/gpu/enum.cu:73-79)."""
+    return enumerate_dd(mdd, 3, 3, 0, True, gpu_batch_size, gpu_max_prod, stats=stats)
+
+
+def coupled_bdd_cuda_enumerate(bdd: DecisionDiagram, maximization: bool = True, problem_type: int = 1,
+                               state_dominance: int = 0, stats: Optional[dict] = None,
+                               gpu_batch_size: int = DEFAULT_MAX_CAND,
+                               gpu_max_prod: int = DEFAULT_MAX_PROD) -> np.ndarray:
+    """Method 3 on a BDD (reference: coupled_bdd_cuda_enumerate, src/pmdd/enum/gpu/enum.cu:595-756).
+    Like the reference, the coupled path applies no state dominance."""
+    return enumerate_dd(bdd, 3, problem_type, 0, maximization, gpu_batch_size, gpu_max_prod, stats=stats)

@@ -1,0 +1,64 @@
+"""Seeded synthetic instances in the reference's text formats.
+
+One fixed generator (numpy PCG64 via `default_rng(seed)`) per problem type, written
+so that the reference's parsers and this package's read the same files:
+
+* knapsack (knapsack_instance.cpp:17-47): profits ~ U[1,1000] per objective and item,
+  one weight row ~ U[1,1000], capacity = floor(sum of weights / 2);
+* set packing (setpacking_instance.hpp:49-80): objective coefficients ~ U[1,100];
+  m constraints, each a uniform random subset of size U{2..20} (1-based indices);
+* TSP (tsp_instance.cpp:11-32): per objective an n x n cost matrix ~ U[1,1000] with a
+  zero diagonal.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def knapsack_text(n: int, nobjs: int, seed: int) -> str:
+    rng = np.random.default_rng(seed)
+    profits = rng.integers(1, 1001, size=(nobjs, n))
+    weights = rng.integers(1, 1001, size=n)
+    cap = int(weights.sum()) // 2
+    lines = [f"{n} 1 {nobjs}"]
+    lines += [" ".join(str(int(x)) for x in row) for row in profits]
+    lines.append(" ".join(str(int(x)) for x in weights) + f" {cap}")
+    return "\n".join(lines) + "\n"
+
+
+def setpacking_text(n: int, m: int, nobjs: int, seed: int) -> str:
+    rng = np.random.default_rng(seed)
+    objs = rng.integers(1, 101, size=(nobjs, n))
+    lines = [f"{n} {m} {nobjs}"]
+    lines += [" ".join(str(int(x)) for x in row) for row in objs]
+    for _ in range(m):
+        k = int(rng.integers(2, 21))
+        k = min(k, n)
+        vars_ = rng.choice(n, size=k, replace=False) + 1
+        lines.append(f"{k} " + " ".join(str(int(v)) for v in vars_))
+    return "\n".join(lines) + "\n"
+
+
+def tsp_text(n: int, nobjs: int, seed: int) -> str:
+    rng = np.random.default_rng(seed)
+    lines = [f"{nobjs}", f"{n}"]
+    for _ in range(nobjs):
+        mat = rng.integers(1, 1001, size=(n, n))
+        np.fill_diagonal(mat, 0)
+        lines += [" ".join(str(int(x)) for x in row) for row in mat]
+    return "\n".join(lines) + "\n"
+
+
+def stream_mix(num_knapsack: int = 512, num_setpacking: int = 256, nobjs: int = 3, seed0: int = 0):
+    """The batched-stream workload: knapsack n ~ U{20..60} and set packing n ~ U{60..100}
+    (m = 20), one seed per instance.  Returns (problem_type, text, tag) triples."""
+    out = []
+    rng = np.random.default_rng(10_000 + seed0)
+    for i in range(num_knapsack):
+        n = int(rng.integers(20, 61))
+        out.append((1, knapsack_text(n, nobjs, seed0 + i), f"kp{nobjs}_n{n}_s{seed0 + i}"))
+    for j in range(num_setpacking):
+        n = int(rng.integers(60, 101))
+        s = seed0 + num_knapsack + j
+        out.append((2, setpacking_text(n, 20, nobjs, s), f"sp{nobjs}_n{n}_s{s}"))
+    return out

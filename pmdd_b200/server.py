@@ -1,0 +1,84 @@
+"""Served request loop over libpmdd_gpu.so's pmdd_server_* entry points.
+
+Requests are admitted as slots and HBM budget free up; every admitted request
+advances one DD layer per engine step, sharing each launch with the others
+(continuous batching).  Timestamps are host monotonic seconds.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+
+from . import _native
+from .dd import DecisionDiagram
+from .enumerate import DEFAULT_MAX_CAND, DEFAULT_MAX_PROD, CudaEnumerationError, _options, _to_array
+
+
+@dataclass
+class ServedResult:
+    req_id: int
+    status: int
+    frontier: np.ndarray
+    submit_s: float
+    admit_s: float
+    finish_s: float
+    error: str = ""
+    extra: dict = field(default_factory=dict)
+
+    @property
+    def latency_s(self) -> float:
+        return self.finish_s - self.submit_s
+
+
+class Server:
+    def __init__(self, device: int = 0, budget_bytes: int = 0, max_slots: int = 0):
+        lib = _native.gpu_lib()
+        err = ctypes.create_string_buffer(512)
+        self._h = lib.pmdd_server_create(device, int(budget_bytes), int(max_slots), err, len(err))
+        if not self._h:
+            raise CudaEnumerationError(8, err.value.decode(errors="replace"))
+        self._lib = lib
+        self._keep = {}   # req_id -> DecisionDiagram kept alive until submitted (the server copies it)
+
+    def submit(self, dd: DecisionDiagram, req_id: int, method: int = 1, state_dominance: int = 0,
+               max_cand: int = DEFAULT_MAX_CAND, max_prod: int = DEFAULT_MAX_PROD) -> int:
+        o = _options(method, dd.problem_type, state_dominance, True, max_cand, max_prod, 0)
+        view = dd.view
+        return self._lib.pmdd_server_submit(self._h, ctypes.byref(view), ctypes.byref(o), ctypes.c_uint64(req_id))
+
+    def run(self, max_steps: int = 0) -> int:
+        r = self._lib.pmdd_server_run(self._h, max_steps)
+        if r < 0:
+            raise CudaEnumerationError(2, "engine step failed")
+        return r
+
+    def poll(self) -> Optional[ServedResult]:
+        res = _native.PmddResult()
+        if not self._lib.pmdd_server_poll(self._h, ctypes.byref(res)):
+            return None
+        try:
+            pts = _to_array(res.frontier)
+        finally:
+            self._lib.pmdd_frontier_free(ctypes.byref(res.frontier))
+        return ServedResult(int(res.req_id), int(res.status), pts, res.submit_s, res.admit_s, res.finish_s,
+                            res.error.decode(errors="replace"))
+
+    def cancel(self, req_id: int) -> bool:
+        return self._lib.pmdd_server_cancel(self._h, ctypes.c_uint64(req_id)) == 0
+
+    def pending(self) -> int:
+        return self._lib.pmdd_server_pending(self._h)
+
+    def close(self):
+        if self._h:
+            self._lib.pmdd_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

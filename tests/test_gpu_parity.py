@@ -1,0 +1,124 @@
+"""Parity of the CUDA engine (through the C ABI) with the reference's frontiers:
+the committed golden fixtures (made by the reference's own binary) and the oracle on
+seeded instances.  Bar: bit-exact equality of the frontier as a set of integer
+vectors (no floating point on this path)."""
+import itertools
+
+import numpy as np
+import pytest
+
+import oracle
+import pmdd_b200 as P
+from conftest import golden_cases, golden_frontier
+from pmdd_b200 import instances
+
+pytestmark = pytest.mark.gpu
+
+CASES = golden_cases()
+
+
+def same_set(a, b):
+    return np.array_equal(oracle.sorted_set(np.asarray(a, dtype=np.int64)), oracle.sorted_set(np.asarray(b, dtype=np.int64)))
+
+
+@pytest.mark.parametrize("rec", CASES, ids=[c["name"] for c in CASES])
+def test_golden_fixtures(rec):
+    dd = P.DecisionDiagram.from_file(rec["dat"], rec["problem_type"], rec["nobjs"])
+    for m in rec["methods"]:
+        st = {}
+        got = P.enumerate_dd(dd, method=int(m), stats=st)
+        assert same_set(got, golden_frontier(rec, int(m))), f"method {m}"
+        if int(m) == 1:
+            assert st["work_candidates_total"] == rec["methods"]["1"]["work_candidates_total"]
+        elif st["layer_coupling"] == rec["methods"]["3"]["layer_coupling"]:
+            # same cutset layer as the reference CPU run -> same join volume
+            assert st["work_join_products_total"] == rec["methods"]["3"]["work_join_products_total"]
+
+
+SEEDED = (
+    [(1, d, instances.knapsack_text(n, d, 100 + 7 * n + d), f"kp{d}_n{n}") for d, n in
+     itertools.product((1, 2, 3, 4, 6, 8), (1, 2, 7, 16, 22))]
+    + [(2, d, instances.setpacking_text(n, m, d, 200 + n), f"sp{d}_n{n}_m{m}") for d, n, m in
+       ((3, 12, 4), (3, 50, 15), (2, 80, 20), (5, 35, 10), (1, 20, 5))]
+    + [(3, d, instances.tsp_text(n, d, 300 + n), f"tsp{d}_n{n}") for d, n in
+       ((3, 2), (3, 3), (3, 5), (2, 9), (4, 8), (6, 7), (5, 9))]
+)
+
+
+@pytest.mark.parametrize("case", SEEDED, ids=[c[3] for c in SEEDED])
+@pytest.mark.parametrize("method", (1, 3))
+def test_seeded_against_oracle(case, method):
+    ptype, d, text, _ = case
+    dd = P.DecisionDiagram.from_text(text, ptype, d)
+    got = P.enumerate_dd(dd, method=method)
+    want = oracle.enumerate(dd, method)
+    assert same_set(got, want)
+    # a frontier is an antichain without duplicates
+    assert len(np.unique(got, axis=0)) == len(got)
+
+
+def test_seam_mirror_functions():
+    bdd = P.DecisionDiagram.from_text(instances.knapsack_text(20, 3, 5), 1, 3)
+    mdd = P.DecisionDiagram.from_text(instances.tsp_text(7, 3, 5), 3, 3)
+    want_b = oracle.enumerate(bdd, 1)
+    want_m = oracle.enumerate(mdd, 1)
+    assert same_set(P.topdown_cuda_enumerate(bdd, True, 1, 0), want_b)
+    assert same_set(P.coupled_bdd_cuda_enumerate(bdd, True, 1, 0), want_b)
+    assert same_set(P.topdown_mdd_cuda_enumerate(mdd), want_m)
+    assert same_set(P.coupled_cuda_enumerate(mdd), want_m)
+
+
+def test_batch_equals_one_at_a_time():
+    texts = [(1, instances.knapsack_text(15 + (i % 10), 3, 1000 + i)) for i in range(24)]
+    texts += [(2, instances.setpacking_text(40 + i, 12, 3, 2000 + i)) for i in range(8)]
+    dds = [P.DecisionDiagram.from_text(t, p, 3) for p, t in texts]
+    for method in (1, 3):
+        batch = P.enumerate_batch(dds, method=method)
+        for dd, got in zip(dds, batch):
+            assert same_set(got, P.enumerate_dd(dd, method=method))
+            assert same_set(got, oracle.enumerate(dd, method))
+
+
+def brute_force_knapsack(profits, weights, cap):
+    """All feasible subsets (int64 sums) -> their Pareto-maximal distinct vectors."""
+    d, n = profits.shape
+    vals = []
+    for mask in range(1 << n):
+        sel = np.array([(mask >> i) & 1 for i in range(n)], dtype=np.int64)
+        if int(sel @ weights) <= cap:
+            vals.append(profits.astype(np.int64) @ sel)
+    pts = np.unique(np.array(vals, dtype=np.int64), axis=0)
+    keep = [not any(np.all(q >= p) and np.any(q != p) for q in pts) for p in pts]
+    return pts[np.array(keep)]
+
+
+def test_wide_objectives_use_int64():
+    """Profits near 2^30 push path sums past int32: the engine switches to int64 points."""
+    rng = np.random.default_rng(42)
+    n, d = 9, 3
+    profits = rng.integers(1, 1 << 30, size=(d, n))
+    weights = rng.integers(1, 100, size=n)
+    cap = int(weights.sum()) // 2
+    text = f"{n} 1 {d}\n" + "\n".join(" ".join(map(str, r)) for r in profits) + "\n" + \
+        " ".join(map(str, weights)) + f" {cap}\n"
+    dd = P.DecisionDiagram.from_text(text, 1, d)
+    want = brute_force_knapsack(profits, weights, cap)
+    for method in (1, 3):
+        got = P.enumerate_dd(dd, method=method)
+        assert got.dtype == np.int64
+        assert same_set(got, want)
+
+
+def test_oversized_destinations_path():
+    """A 5-objective TSP drives destinations past one tile into the global-memory path."""
+    dd = P.DecisionDiagram.from_text(instances.tsp_text(10, 5, 77), 3, 5)
+    st = {}
+    got = P.enumerate_dd(dd, method=1, stats=st)
+    assert st["work_candidates_peak"] > 1024
+    assert same_set(got, oracle.enumerate(dd, 1))
+
+
+def test_invalid_dd_is_rejected_not_run():
+    dd = P.DecisionDiagram.from_text(instances.knapsack_text(5, 3, 1), 1, 3)
+    with pytest.raises(P.CudaEnumerationError):
+        P.enumerate_dd(dd, method=2)
