@@ -1,0 +1,436 @@
+#!/usr/bin/env python
+"""Throughput of exact Pareto-frontier enumeration on B200.
+
+Workload (one "step"): the batched stream -- 512 knapsack BDDs (3 objectives,
+n ~ U{20..60}) + 256 set-packing independent-set BDDs (3 objectives, n ~ U{60..100},
+20 constraints), seeds 0..767, all enumerated top-down (method 1) through one engine
+run whose every launch covers every instance still running.
+
+  value   solves/s with the DDs already resident in HBM (pmdd_resident_*), device time
+          from CUDA events on the engine stream, summed over the K timed steps;
+          L2 flushed (256 MiB write) between timed steps.
+  e2e     solves/s through pmdd_enumerate_batch with host DD buffers: DD upload and
+          frontier download inside the timed region (host clock around the call).
+Extra keys: one-at-a-time solves/s of the same stream through pmdd_enumerate, the
+served loop (Poisson arrivals at 50/200/800 req/s, KP/SP method 1 + TSP method 3),
+the config-1 filter roofline (1024 x KP d=3 n=40), the reference CPU baseline.
+
+Multi-GPU: one process per GPU (torchrun); every rank enumerates its own stream
+(seeds offset by rank), no data-path collective ("replicas", weak scaling); the
+timed region is bracketed by barriers and the max over ranks is reported.
+"""
+from __future__ import annotations
+
+import argparse
+import concurrent.futures as cf
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "solves/s + p50/p99 latency, batched vs one-at-a-time on B200; filter % HBM"
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ------------------------------------------------------------------ helpers
+def build_dds(specs, threads=16):
+    """specs: list of (problem_type, text, tag) -> DecisionDiagrams (built in parallel;
+    ctypes releases the GIL inside the C++ constructors)."""
+    from pmdd_b200 import DecisionDiagram
+
+    def one(s):
+        return DecisionDiagram.from_text(s[1], s[0], 3)
+
+    with cf.ThreadPoolExecutor(threads) as ex:
+        return list(ex.map(one, specs))
+
+
+def dd_bytes(dd):
+    v = dd.view
+    n = (v.num_layers + 1) + (v.num_nodes + 1) + 2 * v.num_arcs + v.num_weights * v.nobjs
+    if v.min_weight:
+        n += v.num_nodes
+    return 4 * n
+
+
+def read_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.idx = device_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            for line in open(self.path):
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    mx = float(parts[2])
+                except ValueError:
+                    continue
+                for name, val in zip(names, parts[5:9]):
+                    if val.lower() in ("active", "1", "yes"):
+                        reasons.add(name)
+        except Exception:
+            pass
+        finally:
+            try:
+                os.unlink(self.path)
+            except Exception:
+                pass
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ----------------------------------------------------------- reference CPU arm
+def cpu_reference_sample(specs, workers, budget_s=25.0, max_items=96):
+    """Reference binary (oracle/_ref) on a bounded sample of the stream, `workers`
+    concurrent single-threaded processes; returns (solves/s, sample size, kind)."""
+    import oracle
+
+    sample = specs[:: max(1, len(specs) // max_items)][:max_items]
+    if not oracle.have_ref(3):
+        return None
+    tmp = tempfile.mkdtemp()
+    paths = []
+    for i, (ptype, text, tag) in enumerate(sample):
+        p = os.path.join(tmp, f"{i}.dat")
+        with open(p, "w") as f:
+            f.write(text)
+        paths.append((ptype, p))
+    lock = threading.Lock()
+    per_worker = [0.0] * workers
+    done = [0]
+    t_start = time.time()
+
+    def work(w):
+        for k in range(w, len(paths), workers):
+            if time.time() - t_start > budget_s * 4:
+                break
+            ptype, p = paths[k]
+            r = oracle.run_ref(p, ptype, 1, 3, threads=1)
+            with lock:
+                per_worker[w] += float(r["stats"]["timing"]["wall"]["wall_enumeration_s"])
+                done[0] += 1
+
+    with cf.ThreadPoolExecutor(workers) as ex:
+        list(ex.map(work, range(workers)))
+    makespan = max(per_worker) if per_worker else 0.0
+    return (done[0] / makespan if makespan > 0 else None), done[0]
+
+
+# --------------------------------------------------------------- served loop
+def served_loop(rate, n_req, seed, P, instances):
+    """Poisson arrivals at `rate` req/s; KP (n~U{20..60}) / SP (n~U{60..100}) method 1 and
+    TSP (n~U{9..13}, method 3); latency = finish - arrival on the host clock."""
+    rng = np.random.default_rng(seed)
+    specs = []
+    for i in range(n_req):
+        kind = rng.integers(0, 3)
+        s = 50_000 + seed * 10_000 + i
+        if kind == 0:
+            specs.append((1, instances.knapsack_text(int(rng.integers(20, 61)), 3, s), 1))
+        elif kind == 1:
+            specs.append((2, instances.setpacking_text(int(rng.integers(60, 101)), 20, 3, s), 1))
+        else:
+            specs.append((3, instances.tsp_text(int(rng.integers(9, 14)), 3, s), 3))
+    dds = build_dds([(p, t, "") for p, t, _ in specs])
+    gaps = rng.exponential(1.0 / rate, size=n_req)
+    arrivals = np.cumsum(gaps)
+    srv = P.Server()
+    t0 = time.perf_counter()
+    t0_mono = time.monotonic()
+    nxt = 0
+    lat = []
+    finished = 0
+    while finished < n_req:
+        now = time.perf_counter() - t0
+        while nxt < n_req and arrivals[nxt] <= now:
+            srv.submit(dds[nxt], nxt, method=specs[nxt][2])
+            nxt += 1
+        if srv.pending() == 0:
+            if nxt < n_req:
+                time.sleep(max(0.0, min(0.002, arrivals[nxt] - now)))
+            continue
+        srv.run(1)
+        while True:
+            r = srv.poll()
+            if r is None:
+                break
+            if r.status != 0:
+                raise RuntimeError(f"served request {r.req_id} failed: {r.error}")
+            # finish_s is the engine's steady clock; arrival is relative to t0
+            lat.append((r.finish_s - (t0_mono + arrivals[r.req_id])) * 1e3)
+            finished += 1
+    wall = time.perf_counter() - t0
+    srv.close()
+    lat = np.array(lat)
+    return {"rate_rps": rate, "requests": n_req, "p50_ms": float(np.percentile(lat, 50)),
+            "p99_ms": float(np.percentile(lat, 99)), "solves_per_s": n_req / wall}
+
+
+# ------------------------------------------------------------------- main
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("native", "reference"), default="native")
+    ap.add_argument("--quick", action="store_true", help="smaller side measurements (development)")
+    ap.add_argument("--no-extras", action="store_true", help="skip one-at-a-time, served, config-1 and CPU legs")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    from pmdd_b200 import instances
+
+    n_kp, n_sp = 512, 256
+    specs = instances.stream_mix(n_kp, n_sp, 3, seed0=rank * (n_kp + n_sp))
+    config = {"workload": "batched stream: 512 knapsack BDDs (d=3, n~U{20..60}) + 256 set-packing BDDs "
+                          "(d=3, n~U{60..100}, m=20), seeds 0..767, method 1",
+              "instances_per_gpu": n_kp + n_sp, "nobjs": 3, "method": 1,
+              "l2": "256 MiB buffer written between timed steps",
+              "parallelism": f"replicas x{args.gpus} (independent instances per GPU, no collective)"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        cores = os.cpu_count() or 1
+        vals = []
+        n_done = 0
+        for s in range(args.warmup + args.steps):
+            r = cpu_reference_sample(specs, cores, budget_s=10.0, max_items=48)
+            if r is None:
+                print(json.dumps({"impl": "reference", "unavailable": "reference CPU binary oracle/_ref/multiobj_nobjs3 "
+                                                                      "not built (make -C oracle REF=...)"}))
+                return
+            if s >= args.warmup:
+                vals.append(r[0])
+                n_done = r[1]
+        v = float(np.median(vals))
+        sample = f"{n_done} stream instances per step, {cores} concurrent single-threaded reference processes"
+        print(json.dumps({"impl": "reference", "metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": args.gpus,
+                          "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * n_done / v,
+                          "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+                          "data": "synthetic", "config": config,
+                          "cpu_baseline": {"value": v, "unit": "solves/s", "cores": cores, "kind": "reference",
+                                           "sample": sample},
+                          "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        return
+
+    import torch
+
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+        from datetime import timedelta
+
+        dist = dist_mod
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    device = local
+    torch.cuda.set_device(device)
+
+    import pmdd_b200 as P
+
+    lib = P._native.gpu_lib()
+    t = time.time()
+    dds = build_dds(specs)
+    log(f"[rank {rank}] built {len(dds)} DDs in {time.time() - t:.1f}s")
+    h2d_bytes = sum(dd_bytes(d) for d in dds)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{device}")
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        tt = torch.tensor([x], dtype=torch.float64, device=f"cuda:{device}")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        return float(tt.item())
+
+    # ---------------------------------------------- device-resident (value)
+    res = P.ResidentSet(dds, device=device)
+    sizes = None
+    for _ in range(args.warmup):
+        sizes = res.enumerate(method=1, keep=False)
+    barrier()
+    dev_time = 0.0
+    k_expand = 0.0
+    launches = 0
+    cand = surv = 0
+    stats_last = {}
+    with ClockSampler(device) as clk:
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            st = {}
+            res.enumerate(method=1, stats=st, keep=False)
+            dev_time += st["device_elapsed_s"]
+            k_expand += st["kernel_expand_td_s"]
+            launches += st["gpu_launches"]
+            cand += st["work_candidates_total"]
+            surv += st["work_frontier_survivors_total"]
+            stats_last = st
+    barrier()
+    clocks = clk.summary()
+    t_max = max_over_ranks(dev_time)
+    n_inst = len(dds)
+    value = n_inst * args.steps * world / t_max
+    ms_per_step = 1e3 * t_max / args.steps
+    res.close()
+
+    # roofline of the fused expand+filter kernel: algorithmic bytes = candidates read
+    # (parent points) + survivors written, D int32 each
+    peak, peak_kind = read_peaks()
+    alg_bytes = (cand + surv) * 3 * 4
+    achieved = alg_bytes / k_expand / 1e9 if k_expand > 0 else 0.0
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "expand_tile_kernel_stream_traffic.json")
+    if os.path.exists(tpath):
+        try:
+            tj = json.load(open(tpath))
+            traffic = tj.get("dram_bytes_per_algorithmic_byte")
+            if traffic is not None:
+                traffic = traffic * alg_bytes / max(1, stats_last.get("layers_td", 0) or 1)
+        except Exception:
+            traffic = None
+    tile_launches_per_step = None
+
+    # ---------------------------------------------------------------- e2e
+    barrier()
+    e2e_wall = 0.0
+    d2h = 0
+    for s in range(args.warmup + args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        outs = P.enumerate_batch(dds, method=1)
+        t1 = time.perf_counter()
+        if s >= args.warmup:
+            e2e_wall += t1 - t0
+            d2h = sum(o.nbytes for o in outs)
+    e2e_max = max_over_ranks(e2e_wall)
+    e2e_value = n_inst * args.steps * world / e2e_max
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded generators, reference text formats)",
+        "config": config,
+        "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": int(h2d_bytes),
+                "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak if peak else None, "traffic": traffic,
+                     "kernel": "expand_tile_kernel<3,int32> (fused expand + dominance filter)",
+                     "peak_kind": peak_kind,
+                     "algorithmic_bytes_per_step": int(alg_bytes / max(1, args.steps)),
+                     "kernel_s_per_step": k_expand / max(1, args.steps)},
+    }
+
+    if rank == 0 and not args.no_extras:
+        # one-at-a-time through the C ABI (same stream, e2e style)
+        sub = dds if not args.quick else dds[::8]
+        t0 = time.perf_counter()
+        for d in sub:
+            P.enumerate_dd(d, method=1)
+        oat = len(sub) / (time.perf_counter() - t0)
+        line["one_at_a_time"] = {"value": oat, "unit": "solves/s", "instances": len(sub),
+                                 "batched_e2e_over_one_at_a_time": e2e_value / world / oat}
+        # served loop
+        served = []
+        for rate in (50, 200, 800):
+            n_req = {50: 100, 200: 200, 800: 400}[rate] // (4 if args.quick else 1)
+            served.append(served_loop(rate, n_req, rate, P, instances))
+        line["served"] = served
+        # config-1 filter roofline: 1024 x KP d=3 n=40
+        n1 = 256 if args.quick else 1024
+        dd1 = build_dds([(1, instances.knapsack_text(40, 3, s), "") for s in range(n1)])
+        r1 = P.ResidentSet(dd1, device=device)
+        r1.enumerate(method=1, keep=False)
+        st1 = {}
+        flush.zero_()
+        torch.cuda.synchronize()
+        r1.enumerate(method=1, stats=st1, keep=False)
+        b1 = (st1["work_candidates_total"] + st1["work_frontier_survivors_total"]) * 3 * 4
+        a1 = b1 / st1["kernel_expand_td_s"] / 1e9
+        line["config1_filter"] = {"instances": n1, "solves_per_s": n1 / st1["device_elapsed_s"],
+                                  "achieved_gbs": a1, "frac_of_peak": a1 / peak,
+                                  "kernel_s": st1["kernel_expand_td_s"], "algorithmic_bytes": int(b1)}
+        r1.close()
+        # reference CPU baseline on the box's cores
+        if world == 1:
+            cores = os.cpu_count() or 1
+            r = cpu_reference_sample(specs, cores, budget_s=12.0, max_items=48)
+            if r is not None and r[0]:
+                line["cpu_baseline"] = {"value": r[0], "unit": "solves/s", "cores": cores, "kind": "reference",
+                                        "sample": f"{r[1]} stream instances, {cores} concurrent single-threaded "
+                                                  f"reference processes (wall_enumeration_s, DD build excluded)"}
+    if rank == 0:
+        print(json.dumps(line))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -122,6 +122,7 @@ typedef struct pmdd_stats {
     int32_t layers_bu;
     int32_t cutset_size;
     int64_t gpu_launches;   /* kernels this call launched */
+    double device_elapsed_s;  /* CUDA-event time on the engine stream, first to last op of the call */
 } pmdd_stats;
 
 /* ------------------------------------------------------------ one-shot entry
@@ -136,6 +137,17 @@ int pmdd_enumerate(const pmdd_dd *dd, const pmdd_options *opts, pmdd_frontier *o
 int pmdd_enumerate_batch(const pmdd_dd *dds, int32_t count, const pmdd_options *opts,
                          pmdd_frontier *outs, int32_t *status, pmdd_stats *stats,
                          char *err, size_t errlen);
+
+/* Device-resident DD set: uploads `count` DDs once (with both arc directions) into
+ * the device engine's memory; pmdd_resident_enumerate then runs a batch over them
+ * with no host->device DD traffic.  Frees with pmdd_resident_free. */
+typedef struct pmdd_resident pmdd_resident;
+pmdd_resident *pmdd_resident_upload(const pmdd_dd *dds, int32_t count, int32_t device, char *err, size_t errlen);
+int pmdd_resident_enumerate(pmdd_resident *res, const pmdd_options *opts, pmdd_frontier *outs, int32_t *status,
+                            pmdd_stats *stats, char *err, size_t errlen);
+/* Sum of the uploaded DDs' device bytes. */
+int64_t pmdd_resident_bytes(const pmdd_resident *res);
+void pmdd_resident_free(pmdd_resident *res);
 
 /* ---------------------------------------------------------------- serving
  * A device-resident request loop with continuous batching: submitted requests are

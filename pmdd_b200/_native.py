@@ -78,6 +78,7 @@ class PmddStats(ctypes.Structure):
         ("layers_bu", c_i32),
         ("cutset_size", c_i32),
         ("gpu_launches", c_i64),
+        ("device_elapsed_s", ctypes.c_double),
     ]
 
     def as_dict(self) -> dict:
@@ -148,6 +149,15 @@ GPU_SYMBOLS = {
         [ctypes.POINTER(PmddDD), c_i32, ctypes.POINTER(PmddOptions), ctypes.POINTER(PmddFrontier),
          P_i32, ctypes.POINTER(PmddStats), ctypes.c_char_p, ctypes.c_size_t],
     ),
+    "pmdd_resident_upload": (ctypes.c_void_p, [ctypes.POINTER(PmddDD), c_i32, c_i32, ctypes.c_char_p,
+                                                ctypes.c_size_t]),
+    "pmdd_resident_enumerate": (
+        ctypes.c_int,
+        [ctypes.c_void_p, ctypes.POINTER(PmddOptions), ctypes.POINTER(PmddFrontier), P_i32,
+         ctypes.POINTER(PmddStats), ctypes.c_char_p, ctypes.c_size_t],
+    ),
+    "pmdd_resident_bytes": (c_i64, [ctypes.c_void_p]),
+    "pmdd_resident_free": (None, [ctypes.c_void_p]),
     "pmdd_server_create": (ctypes.c_void_p, [c_i32, c_i64, c_i32, ctypes.c_char_p, ctypes.c_size_t]),
     "pmdd_server_submit": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(PmddDD), ctypes.POINTER(PmddOptions),
                                           ctypes.c_uint64]),

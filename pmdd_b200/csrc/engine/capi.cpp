@@ -18,12 +18,15 @@ void write_err(char *err, size_t errlen, const std::string &msg) {
     err[n] = '\0';
 }
 
-// One engine per device for the one-shot and batch entries, created on first use and
-// kept for the life of the process (its arena is sized by PMDD_ARENA_BYTES, default a
-// quarter of the device's free memory).
+// One engine per device for the one-shot, batch and resident entries, created on
+// first use and kept for the life of the process (its arena is sized by
+// PMDD_ARENA_BYTES, default a quarter of the device's free memory).  `generation`
+// changes whenever the engine is rebuilt after a CUDA failure, which invalidates
+// resident DD sets made on the old one.
 struct DeviceSlot {
     std::mutex mu;
     std::unique_ptr<pmdd::Engine> engine;
+    uint64_t generation = 0;
 };
 std::mutex g_slots_mu;
 std::unordered_map<int, std::unique_ptr<DeviceSlot>> g_slots;
@@ -46,6 +49,19 @@ int64_t default_arena_bytes(int device) {
     return static_cast<int64_t>(free_b / 4);
 }
 
+// Caller holds slot.mu.
+int ensure_engine(int device, DeviceSlot &slot, std::string *err) {
+    if (slot.engine && slot.engine->ok()) return PMDD_OK;
+    slot.engine.reset(new pmdd::Engine(device, default_arena_bytes(device), 0));
+    slot.generation++;
+    if (!slot.engine->ok()) {
+        *err = slot.engine->error();
+        slot.engine.reset();
+        return PMDD_ERR_NO_DEVICE;
+    }
+    return PMDD_OK;
+}
+
 int export_result(pmdd::Instance &I, pmdd_frontier *out, pmdd_stats *stats) {
     if (stats) *stats = I.stats;
     if (out) {
@@ -65,19 +81,23 @@ int export_result(pmdd::Instance &I, pmdd_frontier *out, pmdd_stats *stats) {
     return I.status;
 }
 
-// Runs `n` prepared requests to completion on the device's shared engine.
-int run_on_device(int device, std::vector<std::unique_ptr<pmdd::Instance>> &reqs, std::string *err) {
-    DeviceSlot &slot = slot_for(device);
-    std::lock_guard<std::mutex> lk(slot.mu);
-    if (!slot.engine || !slot.engine->ok()) {
-        slot.engine.reset(new pmdd::Engine(device, default_arena_bytes(device), 0));
-        if (!slot.engine->ok()) {
-            *err = slot.engine->error();
-            slot.engine.reset();
-            return PMDD_ERR_NO_DEVICE;
-        }
-    }
+struct RunInfo {
+    double device_elapsed_s = 0;
+    int64_t launches = 0;
+    double t_expand = 0, t_big = 0, t_rest = 0;  // kernel time of this call on the engine stream
+};
+
+// Runs prepared requests to completion on the device's shared engine.  Caller holds
+// slot.mu and has called ensure_engine.
+int run_locked(DeviceSlot &slot, std::vector<std::unique_ptr<pmdd::Instance>> &reqs, RunInfo *info,
+               std::string *err) {
     pmdd::Engine &E = *slot.engine;
+    const int64_t l0 = E.launches();
+    const pmdd::KernelTimes k0 = E.kernel_times();
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, E.stream());
     std::unordered_map<uint64_t, size_t> index;
     for (size_t i = 0; i < reqs.size(); ++i) {
         reqs[i]->id = i;
@@ -85,28 +105,84 @@ int run_on_device(int device, std::vector<std::unique_ptr<pmdd::Instance>> &reqs
         E.submit(std::move(reqs[i]));
     }
     size_t got = 0;
+    int rc = PMDD_OK;
     while (got < index.size()) {
         const int r = E.step();
-        if (r < 0) {
-            *err = E.error();
-            // the engine is unusable: drop it so the next call starts clean
-            for (auto &q : E.finished()) {
-                const size_t k = index[q->id];
-                reqs[k] = std::move(q);
-            }
-            E.finished().clear();
-            slot.engine.reset();
-            return PMDD_ERR_CUDA;
-        }
         while (!E.finished().empty()) {
             std::unique_ptr<pmdd::Instance> q = std::move(E.finished().front());
             E.finished().pop_front();
-            const size_t k = index[q->id];
-            reqs[k] = std::move(q);
+            reqs[index[q->id]] = std::move(q);
             ++got;
         }
+        if (r < 0) {
+            *err = E.error();
+            rc = PMDD_ERR_CUDA;
+            break;
+        }
     }
-    return PMDD_OK;
+    if (rc == PMDD_OK) {
+        cudaEventRecord(e1, E.stream());
+        cudaEventSynchronize(e1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (info) {
+            const pmdd::KernelTimes k1 = E.kernel_times();
+            info->device_elapsed_s = ms * 1e-3;
+            info->launches = E.launches() - l0;
+            info->t_expand = k1.expand - k0.expand;
+            info->t_big = k1.big - k0.big;
+            info->t_rest = k1.rest - k0.rest;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc != PMDD_OK) {
+        // the engine is unusable: drop it so the next call starts clean
+        for (auto &r : reqs)
+            if (!r) r.reset(new pmdd::Instance);
+        slot.engine.reset();
+    }
+    return rc;
+}
+
+int run_on_device(int device, std::vector<std::unique_ptr<pmdd::Instance>> &reqs, RunInfo *info, std::string *err) {
+    DeviceSlot &slot = slot_for(device);
+    std::lock_guard<std::mutex> lk(slot.mu);
+    const int rc = ensure_engine(device, slot, err);
+    if (rc != PMDD_OK) return rc;
+    return run_locked(slot, reqs, info, err);
+}
+
+int collect_batch(std::vector<std::unique_ptr<pmdd::Instance>> &reqs, pmdd_frontier *outs, int32_t *status,
+                  pmdd_stats *stats, const RunInfo &info, char *err, size_t errlen) {
+    const int32_t count = static_cast<int32_t>(reqs.size());
+    if (stats) {
+        stats->device_elapsed_s = info.device_elapsed_s;
+        stats->gpu_launches = info.launches;
+        stats->kernel_expand_td_s = info.t_expand;
+        stats->kernel_dominance_s = info.t_big;
+        stats->kernel_total_s = info.t_expand + info.t_big + info.t_rest;
+    }
+    int first_bad = PMDD_OK;
+    for (int32_t i = 0; i < count; ++i) {
+        pmdd_stats st;
+        const int r = export_result(*reqs[i], outs ? &outs[i] : nullptr, &st);
+        if (status) status[i] = r;
+        if (r != PMDD_OK && first_bad == PMDD_OK) {
+            first_bad = r;
+            write_err(err, errlen, "instance " + std::to_string(i) + ": " + reqs[i]->error);
+        }
+        if (stats) {
+            stats->work_candidates_total += st.work_candidates_total;
+            stats->work_candidates_peak = std::max(stats->work_candidates_peak, st.work_candidates_peak);
+            stats->work_frontier_survivors_total += st.work_frontier_survivors_total;
+            stats->work_frontier_peak_points = std::max(stats->work_frontier_peak_points, st.work_frontier_peak_points);
+            stats->work_join_products_total += st.work_join_products_total;
+            stats->gpu_mem_peak_used_bytes = std::max(stats->gpu_mem_peak_used_bytes, st.gpu_mem_peak_used_bytes);
+            stats->gpu_mem_peak_reserved_bytes = st.gpu_mem_peak_reserved_bytes;
+        }
+    }
+    return first_bad;
 }
 
 }  // namespace
@@ -152,13 +228,16 @@ int pmdd_enumerate(const pmdd_dd *dd, const pmdd_options *opts, pmdd_frontier *o
         write_err(err, errlen, msg);
         return rc;
     }
-    rc = run_on_device(o.device, reqs, &msg);
+    RunInfo info;
+    rc = run_on_device(o.device, reqs, &info, &msg);
     if (rc != PMDD_OK) {
         write_err(err, errlen, msg);
         return rc;
     }
     pmdd::Instance &I = *reqs[0];
     I.stats.wall_pack_transfer_s = I.admit_s - t0;
+    I.stats.device_elapsed_s = info.device_elapsed_s;
+    I.stats.gpu_launches = info.launches;
     rc = export_result(I, out, stats);
     if (rc != PMDD_OK) write_err(err, errlen, I.error);
     return rc;
@@ -186,32 +265,149 @@ int pmdd_enumerate_batch(const pmdd_dd *dds, int32_t count, const pmdd_options *
             return rc;
         }
     }
-    int rc = run_on_device(o.device, reqs, &msg);
+    RunInfo info;
+    int rc = run_on_device(o.device, reqs, &info, &msg);
     if (rc != PMDD_OK) {
         write_err(err, errlen, msg);
         return rc;
     }
-    int first_bad = PMDD_OK;
-    for (int32_t i = 0; i < count; ++i) {
-        pmdd_stats st;
-        const int r = export_result(*reqs[i], outs ? &outs[i] : nullptr, &st);
-        if (status) status[i] = r;
-        if (r != PMDD_OK && first_bad == PMDD_OK) {
-            first_bad = r;
-            write_err(err, errlen, "instance " + std::to_string(i) + ": " + reqs[i]->error);
-        }
-        if (stats) {
-            stats->kernel_total_s = std::max(stats->kernel_total_s, st.kernel_total_s);
-            stats->work_candidates_total += st.work_candidates_total;
-            stats->work_candidates_peak = std::max(stats->work_candidates_peak, st.work_candidates_peak);
-            stats->work_frontier_survivors_total += st.work_frontier_survivors_total;
-            stats->work_frontier_peak_points = std::max(stats->work_frontier_peak_points, st.work_frontier_peak_points);
-            stats->work_join_products_total += st.work_join_products_total;
-            stats->gpu_mem_peak_used_bytes = std::max(stats->gpu_mem_peak_used_bytes, st.gpu_mem_peak_used_bytes);
-            stats->gpu_mem_peak_reserved_bytes = st.gpu_mem_peak_reserved_bytes;
-        }
+    return collect_batch(reqs, outs, status, stats, info, err, errlen);
+}
+
+// --------------------------------------------------------- resident DD sets
+struct pmdd_resident {
+    int device = 0;
+    uint64_t generation = 0;
+    int64_t bytes = 0;
+    std::vector<std::unique_ptr<pmdd::Instance>> tmpl;  // prepared requests whose DD stays on the device
+};
+
+pmdd_resident *pmdd_resident_upload(const pmdd_dd *dds, int32_t count, int32_t device, char *err, size_t errlen) {
+    if (count < 0 || (count > 0 && !dds)) {
+        write_err(err, errlen, "invalid DD set");
+        return nullptr;
     }
-    return first_bad;
+    std::unique_ptr<pmdd_resident> R(new pmdd_resident);
+    R->device = device;
+    pmdd_options o;
+    pmdd_options_default(&o);
+    std::string msg;
+    for (int32_t i = 0; i < count; ++i) {
+        std::unique_ptr<pmdd::Instance> I(new pmdd::Instance);
+        if (pmdd::prepare_instance(dds[i], o, static_cast<uint64_t>(i), I.get(), &msg, true) != PMDD_OK) {
+            write_err(err, errlen, "instance " + std::to_string(i) + ": " + msg);
+            return nullptr;
+        }
+        R->tmpl.push_back(std::move(I));
+    }
+    DeviceSlot &slot = slot_for(device);
+    std::lock_guard<std::mutex> lk(slot.mu);
+    if (ensure_engine(device, slot, &msg) != PMDD_OK) {
+        write_err(err, errlen, msg);
+        return nullptr;
+    }
+    R->generation = slot.generation;
+    for (size_t i = 0; i < R->tmpl.size(); ++i) {
+        pmdd::Instance &I = *R->tmpl[i];
+        if (!slot.engine->upload_dd(I)) {
+            for (size_t k = 0; k <= i; ++k) slot.engine->release_dd(*R->tmpl[k]);
+            write_err(err, errlen, slot.engine->ok() ? "DD set does not fit the device memory budget"
+                                                     : slot.engine->error());
+            return nullptr;
+        }
+        R->bytes += static_cast<int64_t>(I.dev_bytes);
+    }
+    if (cudaStreamSynchronize(slot.engine->stream()) != cudaSuccess) {
+        write_err(err, errlen, "DD upload failed");
+        return nullptr;
+    }
+    for (auto &I : R->tmpl) {
+        I->blob.clear();
+        I->blob.shrink_to_fit();
+    }
+    return R.release();
+}
+
+int pmdd_resident_enumerate(pmdd_resident *R, const pmdd_options *opts, pmdd_frontier *outs, int32_t *status,
+                            pmdd_stats *stats, char *err, size_t errlen) {
+    if (stats) std::memset(stats, 0, sizeof(*stats));
+    if (!R) {
+        write_err(err, errlen, "resident set is NULL");
+        return PMDD_ERR_INVALID;
+    }
+    pmdd_options o;
+    if (opts) o = *opts;
+    else pmdd_options_default(&o);
+    if (o.method != 1 && o.method != 3) {
+        write_err(err, errlen, "method must be 1 (top-down) or 3 (coupled) on the GPU backend");
+        return PMDD_ERR_INVALID;
+    }
+    DeviceSlot &slot = slot_for(R->device);
+    std::lock_guard<std::mutex> lk(slot.mu);
+    if (!slot.engine || !slot.engine->ok() || slot.generation != R->generation) {
+        write_err(err, errlen, "resident DD set was invalidated by an engine restart");
+        return PMDD_ERR_CUDA;
+    }
+    std::vector<std::unique_ptr<pmdd::Instance>> reqs;
+    reqs.reserve(R->tmpl.size());
+    for (size_t i = 0; i < R->tmpl.size(); ++i) {
+        const pmdd::Instance &T = *R->tmpl[i];
+        std::unique_ptr<pmdd::Instance> I(new pmdd::Instance);
+        I->opts = o;
+        I->d = T.d;
+        I->wide = T.wide;
+        I->L = T.L;
+        I->N = T.N;
+        I->A = T.A;
+        I->K = T.K;
+        I->layer_off = T.layer_off;
+        I->arc_at_layer = T.arc_at_layer;
+        I->off_layer = T.off_layer;
+        I->off_in = T.off_in;
+        I->off_src = T.off_src;
+        I->off_w = T.off_w;
+        I->off_weights = T.off_weights;
+        I->off_minw = T.off_minw;
+        I->blob_bytes = T.blob_bytes;
+        I->dev_bytes = T.dev_bytes;
+        I->dd = T.dd;
+        I->d_in_off = T.d_in_off;
+        I->d_arc_src = T.d_arc_src;
+        I->d_arc_w = T.d_arc_w;
+        I->d_weights = T.d_weights;
+        I->d_out_off = T.d_out_off;
+        I->d_out_head = T.d_out_head;
+        I->d_out_w = T.d_out_w;
+        I->d_cursor = T.d_cursor;
+        I->external_dd = true;
+        I->with_out_csr = T.with_out_csr;
+        I->est_bytes = std::max<int64_t>(0, T.est_bytes - static_cast<int64_t>(T.dev_bytes));
+        I->submit_s = pmdd::now_s();
+        reqs.push_back(std::move(I));
+    }
+    RunInfo info;
+    std::string msg;
+    const int rc = run_locked(slot, reqs, &info, &msg);
+    if (rc != PMDD_OK) {
+        write_err(err, errlen, msg);
+        return rc;
+    }
+    for (int32_t i = 0; i < static_cast<int32_t>(reqs.size()); ++i)
+        if (outs) std::memset(&outs[i], 0, sizeof(outs[i]));
+    return collect_batch(reqs, outs, status, stats, info, err, errlen);
+}
+
+int64_t pmdd_resident_bytes(const pmdd_resident *R) { return R ? R->bytes : 0; }
+
+void pmdd_resident_free(pmdd_resident *R) {
+    if (!R) return;
+    DeviceSlot &slot = slot_for(R->device);
+    {
+        std::lock_guard<std::mutex> lk(slot.mu);
+        if (slot.engine && slot.generation == R->generation)
+            for (auto &I : R->tmpl) slot.engine->release_dd(*I);
+    }
+    delete R;
 }
 
 // ------------------------------------------------------------------ serving

@@ -102,7 +102,8 @@ Engine::Pinned::~Pinned() {
 }
 
 // ------------------------------------------------------ request preparation
-int prepare_instance(const pmdd_dd &dd, const pmdd_options &o, uint64_t id, Instance *I, std::string *err) {
+int prepare_instance(const pmdd_dd &dd, const pmdd_options &o, uint64_t id, Instance *I, std::string *err,
+                     bool with_out_csr) {
     auto bad = [&](const std::string &m) {
         if (err) *err = m;
         return static_cast<int>(PMDD_ERR_INVALID);
@@ -177,7 +178,8 @@ int prepare_instance(const pmdd_dd &dd, const pmdd_options &o, uint64_t id, Inst
     std::memcpy(I->blob.data() + I->off_weights, dd.weights, sizeof(int32_t) * static_cast<size_t>(K) * d);
     if (has_minw) std::memcpy(I->blob.data() + I->off_minw, dd.min_weight, sizeof(int32_t) * static_cast<size_t>(N));
     size_t dev = off;
-    if (o.method == 3) {
+    I->with_out_csr = with_out_csr || o.method == 3;
+    if (I->with_out_csr) {
         dev = align256(dev + sizeof(int32_t) * (static_cast<size_t>(N) + 1));  // out_off
         dev = align256(dev + sizeof(int32_t) * static_cast<size_t>(A));       // out_head
         dev = align256(dev + sizeof(int32_t) * static_cast<size_t>(A));       // out_w
@@ -277,7 +279,7 @@ void Engine::release_side(Side &s) {
 void Engine::release_instance(Instance &I) {
     release_side(I.td);
     release_side(I.bu);
-    arena_.release(I.dd);
+    if (!I.external_dd) arena_.release(I.dd);
     arena_.release(I.cu_U);
     arena_.release(I.cu_keep);
     arena_.release(I.cu_ctr);
@@ -314,10 +316,48 @@ bool Engine::cancel(uint64_t id) {
     return false;
 }
 
-// Uploads the DD, builds the bottom-up CSR (method 3) and seeds the frontiers.
-bool Engine::admit(Instance &I) {
+bool Engine::upload_dd(Instance &I) {
     I.dd = static_cast<unsigned char *>(arena_.alloc(I.dev_bytes));
     if (!I.dd) return false;
+    if (!cuda_ok(cudaMemcpyAsync(I.dd, I.blob.data(), I.blob_bytes, cudaMemcpyHostToDevice, stream_), "DD upload"))
+        return false;
+    I.d_in_off = reinterpret_cast<const int32_t *>(I.dd + I.off_in);
+    I.d_arc_src = reinterpret_cast<const int32_t *>(I.dd + I.off_src);
+    I.d_arc_w = reinterpret_cast<const int32_t *>(I.dd + I.off_w);
+    I.d_weights = reinterpret_cast<const int32_t *>(I.dd + I.off_weights);
+    if (I.with_out_csr) {
+        size_t off = I.blob_bytes;
+        I.d_out_off = reinterpret_cast<int32_t *>(I.dd + off);
+        off = align256(off + sizeof(int32_t) * (static_cast<size_t>(I.N) + 1));
+        I.d_out_head = reinterpret_cast<int32_t *>(I.dd + off);
+        off = align256(off + sizeof(int32_t) * static_cast<size_t>(I.A));
+        I.d_out_w = reinterpret_cast<int32_t *>(I.dd + off);
+        off = align256(off + sizeof(int32_t) * static_cast<size_t>(I.A));
+        I.d_cursor = reinterpret_cast<int32_t *>(I.dd + off);
+        if (!cuda_ok(dev::launch_build_out_csr(I.d_in_off, I.d_arc_src, I.d_arc_w, I.N, I.A, I.d_out_off, I.d_cursor,
+                                               I.d_out_head, I.d_out_w, stream_),
+                     "out-arc CSR"))
+            return false;
+        launches_ += 3;
+        g_total_launches += 3;
+    }
+    return true;
+}
+
+void Engine::release_dd(Instance &I) {
+    arena_.release(I.dd);
+    I.dd = nullptr;
+}
+
+// Uploads the DD (unless resident), builds the bottom-up CSR and seeds the frontiers.
+bool Engine::admit(Instance &I) {
+    if (!I.external_dd) {
+        if (!upload_dd(I)) {
+            arena_.release(I.dd);
+            I.dd = nullptr;
+            return false;
+        }
+    }
     auto seed = [&](Side &s, int layer) -> bool {
         s.layer = layer;
         s.pts = arena_.alloc(8 * 8);
@@ -336,26 +376,9 @@ bool Engine::admit(Instance &I) {
         release_instance(I);
         return false;
     }
-    if (!cuda_ok(cudaMemcpyAsync(I.dd, I.blob.data(), I.blob_bytes, cudaMemcpyHostToDevice, stream_), "DD upload"))
-        return false;
-    I.d_in_off = reinterpret_cast<const int32_t *>(I.dd + I.off_in);
-    I.d_arc_src = reinterpret_cast<const int32_t *>(I.dd + I.off_src);
-    I.d_arc_w = reinterpret_cast<const int32_t *>(I.dd + I.off_w);
-    I.d_weights = reinterpret_cast<const int32_t *>(I.dd + I.off_weights);
-    if (I.opts.method == 3) {
-        size_t off = I.blob_bytes;
-        I.d_out_off = reinterpret_cast<int32_t *>(I.dd + off);
-        off = align256(off + sizeof(int32_t) * (static_cast<size_t>(I.N) + 1));
-        I.d_out_head = reinterpret_cast<int32_t *>(I.dd + off);
-        off = align256(off + sizeof(int32_t) * static_cast<size_t>(I.A));
-        I.d_out_w = reinterpret_cast<int32_t *>(I.dd + off);
-        off = align256(off + sizeof(int32_t) * static_cast<size_t>(I.A));
-        I.d_cursor = reinterpret_cast<int32_t *>(I.dd + off);
-        if (!cuda_ok(dev::launch_build_out_csr(I.d_in_off, I.d_arc_src, I.d_arc_w, I.N, I.A, I.d_out_off, I.d_cursor,
-                                               I.d_out_head, I.d_out_w, stream_),
-                     "out-arc CSR"))
-            return false;
-        launches_ += 3;
+    if (I.opts.method == 3 && !I.with_out_csr) {
+        fail(I, PMDD_ERR_INVALID, "resident DD lacks the bottom-up CSR needed by method 3");
+        return true;
     }
     I.blob.clear();
     I.blob.shrink_to_fit();
@@ -410,8 +433,10 @@ int Engine::step() {
             queued_.pop_front();
             continue;
         }
-        counts.push_back({&I, true, false});
-        if (I.opts.method == 3) counts.push_back({&I, false, false});
+        if (I.phase == Instance::RUNNING) {
+            counts.push_back({&I, true, false});
+            if (I.opts.method == 3) counts.push_back({&I, false, false});
+        }
         active_.push_back(std::move(queued_.front()));
         queued_.pop_front();
     }
@@ -834,6 +859,9 @@ int Engine::step() {
     cudaEventElapsedTime(&ms_expand, ev0, ev1);
     cudaEventElapsedTime(&ms_big, ev1, ev2);
     cudaEventElapsedTime(&ms_rest, ev2, ev3);
+    ktimes_.expand += ms_expand * 1e-3;
+    ktimes_.big += ms_big * 1e-3;
+    ktimes_.rest += ms_rest * 1e-3;
     cudaEventDestroy(ev0);
     cudaEventDestroy(ev1);
     cudaEventDestroy(ev2);

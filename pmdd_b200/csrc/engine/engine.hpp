@@ -95,13 +95,24 @@ struct Instance {
     pmdd_stats stats{};
     double submit_s = 0, admit_s = 0, finish_s = 0;
     int64_t est_bytes = 0;              // admission estimate
+    bool external_dd = false;           // DD already resident (owned by a pmdd_resident set)
+    bool with_out_csr = false;          // device copy carries the bottom-up CSR
 
     size_t elem() const { return wide ? 8 : 4; }
     int32_t nodes_in(int l) const { return layer_off[l + 1] - layer_off[l]; }
 };
 
-// Validates a flat DD and packs it into an Instance (host side only).
-int prepare_instance(const pmdd_dd &dd, const pmdd_options &opts, uint64_t id, Instance *inst, std::string *err);
+// Validates a flat DD and packs it into an Instance (host side only).  The device copy
+// gets the bottom-up CSR when the method needs it or `with_out_csr` asks for it.
+int prepare_instance(const pmdd_dd &dd, const pmdd_options &opts, uint64_t id, Instance *inst, std::string *err,
+                     bool with_out_csr = false);
+
+// Accumulated kernel time of an engine (seconds, CUDA events on its stream): the fused
+// expand+filter tiles, the oversized-destination path, and everything else (counting,
+// coupling, DD preparation).
+struct KernelTimes {
+    double expand = 0, big = 0, rest = 0;
+};
 
 class Engine {
   public:
@@ -123,6 +134,12 @@ class Engine {
     int64_t launches() const { return launches_; }
     const Arena &arena() const { return arena_; }
     int device() const { return device_; }
+    cudaStream_t stream() const { return stream_; }
+    KernelTimes kernel_times() const { return ktimes_; }
+    // Device copy of a prepared request's DD (with the bottom-up CSR) that stays in
+    // the arena until release_dd(); requests then share it via external_dd.
+    bool upload_dd(Instance &I);
+    void release_dd(Instance &I);
 
   private:
     struct Pinned {
@@ -152,6 +169,7 @@ class Engine {
     Pinned h_desc_, h_summary_, h_init_;
     uint32_t *d_err_ = nullptr;
     int64_t launches_ = 0;
+    KernelTimes ktimes_;
 };
 
 }  // namespace pmdd

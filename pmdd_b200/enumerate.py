@@ -101,6 +101,62 @@ def enumerate_batch(dds: Iterable[DecisionDiagram], method: int = 1, state_domin
     return res
 
 
+class ResidentSet:
+    """DDs uploaded once to device memory (pmdd_resident_*); each `enumerate` call runs
+    a batch over them with no host->device DD traffic."""
+
+    def __init__(self, dds: Iterable[DecisionDiagram], device: int = 0):
+        self.dds = list(dds)
+        lib = _native.gpu_lib()
+        n = len(self.dds)
+        views = (_native.PmddDD * max(n, 1))()
+        for i, dd in enumerate(self.dds):
+            views[i] = dd.view
+        err = ctypes.create_string_buffer(512)
+        self._h = lib.pmdd_resident_upload(views, n, device, err, len(err))
+        if not self._h:
+            raise CudaEnumerationError(3, err.value.decode(errors="replace"))
+        self._lib = lib
+        self.device = device
+
+    @property
+    def device_bytes(self) -> int:
+        return self._lib.pmdd_resident_bytes(self._h)
+
+    def enumerate(self, method: int = 1, state_dominance: int = 0, max_cand: int = DEFAULT_MAX_CAND,
+                  max_prod: int = DEFAULT_MAX_PROD, stats: Optional[dict] = None, keep: bool = True) -> list:
+        n = len(self.dds)
+        ptype = self.dds[0].problem_type if self.dds else 1
+        o = _options(method, ptype, state_dominance, True, max_cand, max_prod, self.device)
+        outs = (_native.PmddFrontier * max(n, 1))()
+        status = (ctypes.c_int32 * max(n, 1))()
+        st = _native.PmddStats()
+        err = ctypes.create_string_buffer(512)
+        rc = self._lib.pmdd_resident_enumerate(self._h, ctypes.byref(o), outs, status, ctypes.byref(st), err,
+                                               len(err))
+        try:
+            if rc != _native.PMDD_OK:
+                raise CudaEnumerationError(rc, err.value.decode(errors="replace"))
+            res = [_to_array(outs[i]) for i in range(n)] if keep else [int(outs[i].num_points) for i in range(n)]
+        finally:
+            for i in range(n):
+                self._lib.pmdd_frontier_free(ctypes.byref(outs[i]))
+        if stats is not None:
+            stats.update(st.as_dict())
+        return res
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.pmdd_resident_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 # ---------------------------------------------------------------- the seam mirror
 def topdown_cuda_enumerate(bdd: DecisionDiagram, maximization: bool = True, problem_type: int = 1,
                            state_dominance: int = 0, stats: Optional[dict] = None,
