@@ -229,6 +229,8 @@ def main():
     ap.add_argument("--impl", choices=("native", "reference"), default="native")
     ap.add_argument("--quick", action="store_true", help="smaller side measurements (development)")
     ap.add_argument("--no-extras", action="store_true", help="skip one-at-a-time, served, config-1 and CPU legs")
+    ap.add_argument("--subset", type=int, default=0,
+                    help="profile a subset: every k-th instance of the stream (k = value); not a bench line")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -239,6 +241,8 @@ def main():
 
     n_kp, n_sp = 512, 256
     specs = instances.stream_mix(n_kp, n_sp, 3, seed0=rank * (n_kp + n_sp))
+    if args.subset > 1:
+        specs = specs[:: args.subset]
     config = {"workload": "batched stream: 512 knapsack BDDs (d=3, n~U{20..60}) + 256 set-packing BDDs "
                           "(d=3, n~U{60..100}, m=20), seeds 0..767, method 1",
               "instances_per_gpu": n_kp + n_sp, "nobjs": 3, "method": 1,
@@ -314,6 +318,8 @@ def main():
     barrier()
     dev_time = 0.0
     k_expand = 0.0
+    k_big = 0.0
+    k_total = 0.0
     launches = 0
     cand = surv = 0
     stats_last = {}
@@ -325,6 +331,8 @@ def main():
             res.enumerate(method=1, stats=st, keep=False)
             dev_time += st["device_elapsed_s"]
             k_expand += st["kernel_expand_td_s"]
+            k_big += st["kernel_dominance_s"]
+            k_total += st["kernel_total_s"]
             launches += st["gpu_launches"]
             cand += st["work_candidates_total"]
             surv += st["work_frontier_survivors_total"]
@@ -385,7 +393,11 @@ def main():
                      "peak_kind": peak_kind,
                      "algorithmic_bytes_per_step": int(alg_bytes / max(1, args.steps)),
                      "kernel_s_per_step": k_expand / max(1, args.steps)},
+        "step_breakdown_s": {"device": t_max / args.steps, "tiles": k_expand / args.steps,
+                             "oversized": k_big / args.steps, "kernels_total": k_total / args.steps},
     }
+    if args.subset > 1:
+        line["config"]["subset"] = f"every {args.subset}th instance (profiling run, not a bench line)"
 
     if rank == 0 and not args.no_extras:
         # one-at-a-time through the C ABI (same stream, e2e style)

@@ -50,11 +50,16 @@ struct ExpandJob {
     const int64_t *big_list;       // (local item, scratch offset) pairs
     int32_t num_big;
     int32_t pad0;
-    void *big_pts;                 // scratch for oversized destinations (points)
-    int32_t *big_tag;              // arc of each scratch point
-    uint8_t *big_keep;             // keep flag of each scratch point
+    void *big_pts;                 // scratch: candidates of oversized destinations (AoS)
+    void *big_pts2;                // scratch: the same candidates in sum-bucket order
+    void *big_surv;                // scratch: survivors of one bucket that overflow shared memory
+    int32_t *big_idx;              // scratch: candidate index of each bucket-ordered point
+    int32_t *big_surv_idx;         // scratch: candidate index of each overflowing survivor
     uint32_t *err;
 };
+
+// Bytes of oversized-destination scratch per candidate point.
+constexpr size_t big_scratch_bytes_per_point(int d, size_t elem) { return 3 * d * elem + 2 * sizeof(int32_t); }
 
 // Counting pass for the next layer of one direction.
 struct CountJob {

@@ -396,9 +396,8 @@ struct ExpPlan {
     void *out_pts;
     int64_t *out_off;
     int32_t *out_size;
-    void *big_pts;
-    int32_t *big_tag;
-    uint8_t *big_keep;
+    void *big_mem;    // oversized-destination scratch (one block, carved per use)
+    int64_t big_total;
 };
 
 struct CountPlan {
@@ -455,7 +454,7 @@ int Engine::step() {
         const int nl = is_td ? s.layer + 1 : s.layer - 1;
         const int64_t C = s.res.total;
         const int32_t V = I.nodes_in(nl);
-        ExpPlan e{&I, is_td, nl, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+        ExpPlan e{&I, is_td, nl, nullptr, nullptr, nullptr, nullptr, 0};
         const size_t pts_bytes = static_cast<size_t>(std::max<int64_t>(C, 1)) * I.d * I.elem();
         e.out_pts = arena_.alloc(pts_bytes);
         e.out_off = static_cast<int64_t *>(arena_.alloc(sizeof(int64_t) * V));
@@ -463,14 +462,12 @@ int Engine::step() {
         bool okay = e.out_pts && e.out_off && e.out_size;
         if (okay && s.res.num_big > 0) {
             const int64_t bt = s.res.big_total;
-            e.big_pts = arena_.alloc(static_cast<size_t>(bt) * I.d * I.elem());
-            e.big_tag = static_cast<int32_t *>(arena_.alloc(sizeof(int32_t) * bt));
-            e.big_keep = static_cast<uint8_t *>(arena_.alloc(static_cast<size_t>(bt)));
-            okay = e.big_pts && e.big_tag && e.big_keep;
+            e.big_total = bt;
+            e.big_mem = arena_.alloc(static_cast<size_t>(bt) * dev::big_scratch_bytes_per_point(I.d, I.elem()) + 1024);
+            okay = e.big_mem != nullptr;
         }
         if (!okay) {
-            for (void *q : {e.out_pts, static_cast<void *>(e.out_off), static_cast<void *>(e.out_size), e.big_pts,
-                            static_cast<void *>(e.big_tag), static_cast<void *>(e.big_keep)})
+            for (void *q : {e.out_pts, static_cast<void *>(e.out_off), static_cast<void *>(e.out_size), e.big_mem})
                 arena_.release(q);
             const int64_t need = static_cast<int64_t>(pts_bytes);
             if (need > blocked_need) {
@@ -541,9 +538,16 @@ int Engine::step() {
                 gl.tiles += J.num_tiles;
                 J.big_list = s.big_list;
                 J.num_big = s.res.num_big;
-                J.big_pts = e.big_pts;
-                J.big_tag = e.big_tag;
-                J.big_keep = e.big_keep;
+                if (e.big_mem) {
+                    const size_t pb = align256(static_cast<size_t>(e.big_total) * I.d * I.elem());
+                    const size_t ib = align256(sizeof(int32_t) * static_cast<size_t>(e.big_total));
+                    char *m = static_cast<char *>(e.big_mem);
+                    J.big_pts = m;
+                    J.big_pts2 = m + pb;
+                    J.big_surv = m + 2 * pb;
+                    J.big_idx = reinterpret_cast<int32_t *>(m + 3 * pb);
+                    J.big_surv_idx = reinterpret_cast<int32_t *>(m + 3 * pb + ib);
+                }
                 J.err = d_err_;
                 for (int b = 0; b < s.res.num_big; ++b) bigwork.push_back({static_cast<int32_t>(pos - gl.first), b});
                 if (s.res.num_big > 0) gl.max_big = std::max(gl.max_big, s.res.max_item);
@@ -636,8 +640,7 @@ int Engine::step() {
             arena_.release(new_big[k]);
         }
         for (const ExpPlan &e : exps) {
-            for (void *q : {e.out_pts, static_cast<void *>(e.out_off), static_cast<void *>(e.out_size), e.big_pts,
-                            static_cast<void *>(e.big_tag), static_cast<void *>(e.big_keep)})
+            for (void *q : {e.out_pts, static_cast<void *>(e.out_off), static_cast<void *>(e.out_size), e.big_mem})
                 arena_.release(q);
         }
         for (void *q : step_scratch_) arena_.release(q);
@@ -696,9 +699,7 @@ int Engine::step() {
         to_release.push_back(s.size);
         to_release.push_back(s.arc_off);
         to_release.push_back(s.big_list);
-        to_release.push_back(e.big_pts);
-        to_release.push_back(e.big_tag);
-        to_release.push_back(e.big_keep);
+        to_release.push_back(e.big_mem);
         I.stats.work_candidates_total += s.res.total;
         I.stats.work_candidates_peak = std::max(I.stats.work_candidates_peak, s.res.total);
         s.pts = e.out_pts;

@@ -322,8 +322,24 @@ __global__ void __launch_bounds__(kTileThreads) expand_tile_kernel(const ExpandJ
 }
 
 // ------------------------------------------------------- oversized destinations
-// Scratch of a job's oversized destination `big`: its points start at big_list[2*big+1].
-// Materialise the candidates of one oversized destination (AoS) with their arcs.
+// Destinations with more than kSmallMax candidates.  Their candidates are materialised
+// in scratch, then filtered by a bucketed sort-filter-skyline sweep (the presorting
+// idea of Chomicki, Godfrey, Gryz and Liang, "Skyline with presorting", ICDE 2003):
+// points are grouped into buckets of decreasing objective sum; a dominator of p has a
+// sum >= p's, so it lies in p's bucket or an earlier one.  Each bucket's points are
+// checked against the kept set K of earlier buckets (all of which are maximal), the
+// bucket's survivors against each other, and the bucket's maxima are appended to K --
+// which is the destination's slot in the output.
+
+template <int D, typename T>
+__device__ __forceinline__ int64_t point_sum(const T *p) {
+    int64_t s = 0;
+#pragma unroll
+    for (int o = 0; o < D; ++o) s += static_cast<int64_t>(p[o]);
+    return s;
+}
+
+// Materialise the candidates of one oversized destination (AoS).
 template <int D, typename T>
 __global__ void __launch_bounds__(kBigThreads) big_expand_kernel(const ExpandJob *__restrict__ jobs,
                                                                  const BigWork *__restrict__ work) {
@@ -351,105 +367,234 @@ __global__ void __launch_bounds__(kBigThreads) big_expand_kernel(const ExpandJob
             const int64_t dst = soff + (b - c0) + idx;
 #pragma unroll
             for (int o = 0; o < D; ++o) spts[dst * D + o] = src[idx * D + o] + wv[o];
-            J.big_tag[dst] = a;
         }
     }
 }
 
-// Pairwise filter of one oversized destination: block x handles candidates
-// [x*256, ...) striding by gridDim.x*256 and sweeps shared-memory tiles of the whole
-// destination, leaving the sweep as soon as every candidate of the block is decided.
 template <int D, typename T>
-__global__ void __launch_bounds__(kBigThreads) big_filter_kernel(const ExpandJob *__restrict__ jobs,
-                                                                 const BigWork *__restrict__ work) {
-    constexpr int JT = (kBigJTile * D * static_cast<int>(sizeof(T)) > 32768)
-                           ? 32768 / (D * static_cast<int>(sizeof(T)))
-                           : kBigJTile;
-    __shared__ T sj[D][JT];
-    __shared__ int32_t st[JT];
-    const BigWork W = work[blockIdx.y];
+struct SfsCfg {
+    static constexpr int kThreads = 512;
+    static constexpr int kMaxBuckets = 8192;
+    static constexpr int kKeepCache = 65536 / (D * static_cast<int>(sizeof(T)));             // K points in smem
+    static constexpr int kSurvCache = 49152 / (D * static_cast<int>(sizeof(T)) + 8);         // survivors in smem
+    static constexpr size_t kSmem = sizeof(int32_t) * kMaxBuckets + sizeof(T) * D * kKeepCache +
+                                    (sizeof(T) * D + 2 * sizeof(int32_t)) * kSurvCache + 512;
+};
+
+template <int D, typename T>
+__global__ void __launch_bounds__(SfsCfg<D, T>::kThreads) big_sfs_kernel(const ExpandJob *__restrict__ jobs,
+                                                                         const BigWork *__restrict__ work) {
+    using Cfg = SfsCfg<D, T>;
+    constexpr int NT = Cfg::kThreads, KS = Cfg::kKeepCache, SC = Cfg::kSurvCache;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    int32_t *hist = reinterpret_cast<int32_t *>(smem_raw);
+    T *kc = reinterpret_cast<T *>(hist + Cfg::kMaxBuckets);             // [D][KS]
+    T *sc = kc + static_cast<size_t>(D) * KS;                            // [D][SC]
+    int32_t *sidx = reinterpret_cast<int32_t *>(sc + static_cast<size_t>(D) * SC);  // [SC]
+    int32_t *sflag = sidx + SC;                                          // [SC]
+    __shared__ int64_t red_min[NT / 32], red_max[NT / 32];
+    __shared__ int32_t warp_i[32];
+    __shared__ int32_t tot_i;
+    __shared__ int64_t s_min, s_max;
+    __shared__ int32_t s_kn, s_m;
+
+    const BigWork W = work[blockIdx.x];
     const ExpandJob &J = jobs[W.job];
     const int32_t item = static_cast<int32_t>(J.big_list[2 * W.big]);
     const int64_t soff = J.big_list[2 * W.big + 1];
-    const T *spts = static_cast<const T *>(J.big_pts);
-    const int32_t *stag = J.big_tag;
     const int32_t v = J.item_base + item;
-    const int64_t n = J.arc_cand_off[J.item_arc_off[v + 1] - J.arc_base] - J.arc_cand_off[J.item_arc_off[v] - J.arc_base];
-    for (int64_t i0 = static_cast<int64_t>(blockIdx.x) * kBigThreads; i0 < n;
-         i0 += static_cast<int64_t>(gridDim.x) * kBigThreads) {
-        const int64_t i = i0 + threadIdx.x;
-        const bool valid = i < n;
-        T p[D];
-        int32_t my_tag = -1;
-        if (valid) {
-#pragma unroll
-            for (int o = 0; o < D; ++o) p[o] = spts[(soff + i) * D + o];
-            my_tag = stag[soff + i];
+    const int64_t s0 = J.arc_cand_off[J.item_arc_off[v] - J.arc_base];
+    const int64_t n = J.arc_cand_off[J.item_arc_off[v + 1] - J.arc_base] - s0;
+    const T *P = static_cast<const T *>(J.big_pts) + soff * D;
+    T *P2 = static_cast<T *>(J.big_pts2) + soff * D;
+    int32_t *I2 = J.big_idx + soff;
+    T *SV = static_cast<T *>(J.big_surv) + soff * D;
+    int32_t *SVI = J.big_surv_idx + soff;
+    T *out = static_cast<T *>(J.out_pts) + s0 * D;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+
+    // 1. range of point sums
+    int64_t mn = INT64_MAX, mx = INT64_MIN;
+    for (int64_t i = tid; i < n; i += NT) {
+        const int64_t sm = point_sum<D, T>(P + i * D);
+        mn = min(mn, sm);
+        mx = max(mx, sm);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+        mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    }
+    if (lane == 0) {
+        red_min[warp] = mn;
+        red_max[warp] = mx;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        int64_t a = red_min[0], b = red_max[0];
+        for (int w = 1; w < NT / 32; ++w) {
+            a = min(a, red_min[w]);
+            b = max(b, red_max[w]);
         }
-        bool dom = !valid;
-        for (int64_t j0 = 0; j0 < n; j0 += JT) {
-            if (__syncthreads_and(dom)) break;
-            const int m = static_cast<int>(n - j0 < JT ? n - j0 : static_cast<int64_t>(JT));
-            for (int k = threadIdx.x; k < m; k += kBigThreads) {
+        s_min = a;
+        s_max = b;
+        s_kn = 0;
+    }
+    __syncthreads();
+    // 2. counting sort into buckets of decreasing sum (bucket 0 = largest sums)
+    const int64_t nb64 = n / 32 < 1 ? 1 : n / 32;
+    const int nb = static_cast<int>(nb64 < Cfg::kMaxBuckets ? nb64 : static_cast<int64_t>(Cfg::kMaxBuckets));
+    const int64_t width = (s_max - s_min) / nb + 1;
+    for (int b = tid; b < nb; b += NT) hist[b] = 0;
+    __syncthreads();
+    for (int64_t i = tid; i < n; i += NT) {
+        const int b = static_cast<int>((s_max - point_sum<D, T>(P + i * D)) / width);
+        atomicAdd(&hist[b], 1);
+    }
+    __syncthreads();
+    {
+        constexpr int PER = Cfg::kMaxBuckets / NT;
+        int32_t loc[PER];
+        int32_t run = 0;
 #pragma unroll
-                for (int o = 0; o < D; ++o) sj[o][k] = spts[(soff + j0 + k) * D + o];
-                st[k] = stag[soff + j0 + k];
-            }
-            __syncthreads();
-            if (!dom) {
-                for (int k = 0; k < m; ++k) {
-                    if (st[k] == my_tag) continue;
-                    bool ge = true, eq = true;
+        for (int r = 0; r < PER; ++r) {
+            const int b = tid * PER + r;
+            loc[r] = b < nb ? hist[b] : 0;
+            run += loc[r];
+        }
+        int32_t ex = block_exclusive_scan<int32_t, NT>(run, warp_i, &tot_i);
 #pragma unroll
-                    for (int o = 0; o < D; ++o) {
-                        const T x = sj[o][k];
-                        ge &= (x >= p[o]);
-                        eq &= (x == p[o]);
+        for (int r = 0; r < PER; ++r) {
+            const int b = tid * PER + r;
+            if (b < nb) hist[b] = ex;
+            ex += loc[r];
+        }
+    }
+    __syncthreads();
+    for (int64_t i = tid; i < n; i += NT) {
+        const T *p = P + i * D;
+        const int b = static_cast<int>((s_max - point_sum<D, T>(p)) / width);
+        const int pos = atomicAdd(&hist[b], 1);
+#pragma unroll
+        for (int o = 0; o < D; ++o) P2[static_cast<int64_t>(pos) * D + o] = p[o];
+        I2[pos] = static_cast<int32_t>(i);
+    }
+    __syncthreads();  // hist[b] is now the end of bucket b
+
+    // 3. sweep the buckets
+    for (int b = 0; b < nb; ++b) {
+        const int32_t lo = b == 0 ? 0 : hist[b - 1], hi = hist[b];
+        if (lo == hi) continue;
+        if (tid == 0) s_m = 0;
+        __syncthreads();
+        const int32_t kn = s_kn;
+        // 3a. against the maxima of earlier buckets
+        for (int32_t c0 = lo; c0 < hi; c0 += NT) {
+            const int32_t i = c0 + tid;
+            const bool valid = i < hi;
+            T p[D];
+            int32_t pidx = 0;
+            bool dom = !valid;
+            if (valid) {
+#pragma unroll
+                for (int o = 0; o < D; ++o) p[o] = P2[static_cast<int64_t>(i) * D + o];
+                pidx = I2[i];
+                for (int32_t j = 0; j < kn; ++j) {
+                    bool ge = true;
+                    if (j < KS) {
+#pragma unroll
+                        for (int o = 0; o < D; ++o) ge &= (kc[o * KS + j] >= p[o]);
+                    } else {
+#pragma unroll
+                        for (int o = 0; o < D; ++o) ge &= (out[static_cast<int64_t>(j) * D + o] >= p[o]);
                     }
-                    if (ge && (!eq || j0 + k < i)) {
+                    if (ge) {
                         dom = true;
                         break;
                     }
                 }
             }
-        }
-        if (valid) J.big_keep[soff + i] = dom ? 0 : 1;
-        __syncthreads();
-    }
-}
-
-// Compaction of one oversized destination into its slot, and its survivor count.
-template <int D, typename T>
-__global__ void __launch_bounds__(kCountThreads) big_compact_kernel(const ExpandJob *__restrict__ jobs,
-                                                                    const BigWork *__restrict__ work) {
-    __shared__ int32_t warp_buf[32];
-    __shared__ int32_t s_total;
-    __shared__ int64_t s_carry;
-    const BigWork W = work[blockIdx.x];
-    const ExpandJob &J = jobs[W.job];
-    const int32_t item = static_cast<int32_t>(J.big_list[2 * W.big]);
-    const int64_t soff = J.big_list[2 * W.big + 1];
-    const T *spts = static_cast<const T *>(J.big_pts);
-    const int32_t v = J.item_base + item;
-    const int64_t s = J.arc_cand_off[J.item_arc_off[v] - J.arc_base];
-    const int64_t n = J.arc_cand_off[J.item_arc_off[v + 1] - J.arc_base] - s;
-    T *outp = static_cast<T *>(J.out_pts);
-    if (threadIdx.x == 0) s_carry = 0;
-    __syncthreads();
-    for (int64_t base = 0; base < n; base += kCountThreads) {
-        const int64_t i = base + threadIdx.x;
-        const int32_t k = (i < n && J.big_keep[soff + i]) ? 1 : 0;
-        const int32_t ex = block_exclusive_scan<int32_t, kCountThreads>(k, warp_buf, &s_total);
-        if (k) {
-            const int64_t dst = s + s_carry + ex;
+            const int32_t ex = block_exclusive_scan<int32_t, NT>(dom ? 0 : 1, warp_i, &tot_i);
+            const int32_t m0 = s_m;
+            if (!dom) {
+                const int32_t k = m0 + ex;
+                if (k < SC) {
 #pragma unroll
-            for (int o = 0; o < D; ++o) outp[dst * D + o] = spts[(soff + i) * D + o];
+                    for (int o = 0; o < D; ++o) sc[o * SC + k] = p[o];
+                    sidx[k] = pidx;
+                } else {
+#pragma unroll
+                    for (int o = 0; o < D; ++o) SV[static_cast<int64_t>(k) * D + o] = p[o];
+                    SVI[k] = pidx;
+                }
+            }
+            __syncthreads();
+            if (tid == 0) s_m = m0 + tot_i;
+            __syncthreads();
         }
-        __syncthreads();  // every thread has read s_carry
-        if (threadIdx.x == 0) s_carry += s_total;
+        const int32_t m = s_m;
+        // 3b. survivors of this bucket against each other (first duplicate kept)
+        for (int32_t k = tid; k < m; k += NT) {
+            T p[D];
+            int32_t pidx;
+            if (k < SC) {
+#pragma unroll
+                for (int o = 0; o < D; ++o) p[o] = sc[o * SC + k];
+                pidx = sidx[k];
+            } else {
+#pragma unroll
+                for (int o = 0; o < D; ++o) p[o] = SV[static_cast<int64_t>(k) * D + o];
+                pidx = SVI[k];
+            }
+            bool dom = false;
+            for (int32_t j = 0; j < m && !dom; ++j) {
+                if (j == k) continue;
+                bool ge = true, eq = true;
+                int32_t qidx;
+                if (j < SC) {
+#pragma unroll
+                    for (int o = 0; o < D; ++o) {
+                        const T x = sc[o * SC + j];
+                        ge &= (x >= p[o]);
+                        eq &= (x == p[o]);
+                    }
+                    qidx = sidx[j];
+                } else {
+#pragma unroll
+                    for (int o = 0; o < D; ++o) {
+                        const T x = SV[static_cast<int64_t>(j) * D + o];
+                        ge &= (x >= p[o]);
+                        eq &= (x == p[o]);
+                    }
+                    qidx = SVI[j];
+                }
+                dom = ge && (!eq || qidx < pidx);
+            }
+            if (k < SC) sflag[k] = dom ? 0 : 1;
+            else I2[lo + k] = dom ? 0 : 1;  // bucket entries [lo, hi) were consumed above
+        }
         __syncthreads();
+        // 3c. append the bucket's maxima to K (the output slot) and the K cache
+        for (int32_t c0 = 0; c0 < m; c0 += NT) {
+            const int32_t k = c0 + tid;
+            int32_t keep = 0;
+            if (k < m) keep = k < SC ? sflag[k] : I2[lo + k];
+            const int32_t ex = block_exclusive_scan<int32_t, NT>(keep, warp_i, &tot_i);
+            const int32_t base = s_kn;
+            if (keep) {
+                const int32_t dst = base + ex;
+#pragma unroll
+                for (int o = 0; o < D; ++o) {
+                    const T x = k < SC ? sc[o * SC + k] : SV[static_cast<int64_t>(k) * D + o];
+                    out[static_cast<int64_t>(dst) * D + o] = x;
+                    if (dst < KS) kc[o * KS + dst] = x;
+                }
+            }
+            __syncthreads();
+            if (tid == 0) s_kn = base + tot_i;
+            __syncthreads();
+        }
     }
-    if (threadIdx.x == 0) J.out_size[item] = static_cast<int32_t>(s_carry);
+    if (tid == 0) J.out_size[item] = s_kn;
 }
 
 // ----------------------------------------------------------------- launchers
@@ -474,21 +619,23 @@ template <int D, typename T>
 static cudaError_t launch_big_t(const ExpandJob *jobs, const BigWork *work, int num_work, int64_t max_item, int sms,
                                 cudaStream_t stream) {
     if (num_work <= 0) return cudaSuccess;
+    using Cfg = SfsCfg<D, T>;
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaError_t e = cudaFuncSetAttribute(big_sfs_kernel<D, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             static_cast<int>(Cfg::kSmem));
+        if (e != cudaSuccess) return e;
+        attr_set = true;
+    }
     const int64_t chunks = (max_item + kBigThreads - 1) / kBigThreads;
     const unsigned gx_expand = static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>(chunks, 64)));
-    // enough blocks per destination to fill the SMs when few destinations are big
-    int64_t per = std::max<int64_t>(1, (static_cast<int64_t>(sms) * 8) / num_work);
-    per = std::max<int64_t>(1, std::min<int64_t>(per, chunks));
     constexpr int kMaxY = 65535;  // grid.y limit
     for (int w0 = 0; w0 < num_work; w0 += kMaxY) {
         const int nw = std::min(kMaxY, num_work - w0);
         big_expand_kernel<D, T><<<dim3(gx_expand, nw), kBigThreads, 0, stream>>>(jobs, work + w0);
     }
-    for (int w0 = 0; w0 < num_work; w0 += kMaxY) {
-        const int nw = std::min(kMaxY, num_work - w0);
-        big_filter_kernel<D, T><<<dim3(static_cast<unsigned>(per), nw), kBigThreads, 0, stream>>>(jobs, work + w0);
-    }
-    big_compact_kernel<D, T><<<num_work, kCountThreads, 0, stream>>>(jobs, work);
+    big_sfs_kernel<D, T><<<num_work, Cfg::kThreads, Cfg::kSmem, stream>>>(jobs, work);
+    (void)sms;
     return cudaGetLastError();
 }
 

@@ -118,6 +118,33 @@ def test_oversized_destinations_path():
     assert same_set(got, oracle.enumerate(dd, 1))
 
 
+def test_duplicate_heavy_instances():
+    """Identical and near-identical items create many equal candidates across arcs:
+    exactly one copy of each frontier point must survive, on every path."""
+    for n, d, spread in ((24, 3, 1), (30, 2, 2), (16, 4, 3)):
+        rng = np.random.default_rng(n + d)
+        profits = rng.integers(1, 1 + spread, size=(d, n))
+        weights = rng.integers(1, 1 + spread, size=n)
+        cap = int(weights.sum()) // 2
+        text = f"{n} 1 {d}\n" + "\n".join(" ".join(map(str, r)) for r in profits) + "\n" + \
+            " ".join(map(str, weights)) + f" {cap}\n"
+        dd = P.DecisionDiagram.from_text(text, 1, d)
+        for method in (1, 3):
+            got = P.enumerate_dd(dd, method=method)
+            assert same_set(got, oracle.enumerate(dd, method))
+            assert len(np.unique(got, axis=0)) == len(got)
+
+
+def test_high_fan_in_knapsack():
+    """A 3-objective knapsack with n=48: the last layers' destinations gather thousands
+    of parents and take the oversized path with large candidate sets."""
+    dd = P.DecisionDiagram.from_text(instances.knapsack_text(48, 3, 4), 1, 3)
+    st = {}
+    got = P.enumerate_dd(dd, method=1, stats=st)
+    assert st["work_candidates_peak"] > 100_000
+    assert same_set(got, oracle.enumerate(dd, 1))
+
+
 def test_invalid_dd_is_rejected_not_run():
     dd = P.DecisionDiagram.from_text(instances.knapsack_text(5, 3, 1), 1, 3)
     with pytest.raises(P.CudaEnumerationError):
