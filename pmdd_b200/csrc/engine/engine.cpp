@@ -17,6 +17,8 @@
 #include <algorithm>
 #include <atomic>
 #include <climits>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 
 namespace pmdd {
@@ -230,6 +232,8 @@ Engine::Engine(int device, int64_t budget_bytes, int max_slots) : device_(device
     d_err_ = static_cast<uint32_t *>(arena_.alloc(sizeof(uint32_t)));
     if (!cuda_ok(cudaMemsetAsync(d_err_, 0, sizeof(uint32_t), stream_), "cudaMemsetAsync")) return;
     if (max_slots_ <= 0) max_slots_ = 1 << 20;
+    const char *tr = std::getenv("PMDD_TRACE");
+    trace_ = tr != nullptr && tr[0] == '1';
     // constant initial frontier: one zero point (up to 8 int64 values), offset 0, size 1
     if (!h_init_.reserve(256)) {
         error_ = "cudaMallocHost failed";
@@ -398,6 +402,9 @@ struct ExpPlan {
     int32_t *out_size;
     void *big_mem;    // oversized-destination scratch (one block, carved per use)
     int64_t big_total;
+    int64_t cand;       // candidates of this expansion (trace / statistics)
+    int64_t max_item;
+    int64_t num_big;
 };
 
 struct CountPlan {
@@ -454,7 +461,7 @@ int Engine::step() {
         const int nl = is_td ? s.layer + 1 : s.layer - 1;
         const int64_t C = s.res.total;
         const int32_t V = I.nodes_in(nl);
-        ExpPlan e{&I, is_td, nl, nullptr, nullptr, nullptr, nullptr, 0};
+        ExpPlan e{&I, is_td, nl, nullptr, nullptr, nullptr, nullptr, 0, C, s.res.max_item, s.res.num_big};
         const size_t pts_bytes = static_cast<size_t>(std::max<int64_t>(C, 1)) * I.d * I.elem();
         e.out_pts = arena_.alloc(pts_bytes);
         e.out_off = static_cast<int64_t *>(arena_.alloc(sizeof(int64_t) * V));
@@ -863,6 +870,23 @@ int Engine::step() {
     ktimes_.expand += ms_expand * 1e-3;
     ktimes_.big += ms_big * 1e-3;
     ktimes_.rest += ms_rest * 1e-3;
+    if (trace_) {
+        int64_t cand = 0, big_cand = 0, max_item = 0, nbig = 0;
+        for (const ExpPlan &e : exps) {
+            const Side &s = e.td ? e.I->td : e.I->bu;  // already moved: stats come from the plan
+            (void)s;
+            cand += e.cand;
+            big_cand += e.big_total;
+            max_item = std::max(max_item, e.max_item);
+            nbig += e.num_big;
+        }
+        std::fprintf(stderr,
+                     "[pmdd step] jobs=%zu counts=%zu couple=%zu cand=%lld big_items=%lld big_cand=%lld max_item=%lld "
+                     "tiles_ms=%.3f big_ms=%.3f rest_ms=%.3f\n",
+                     exps.size(), counts.size(), ujobs.size(), static_cast<long long>(cand),
+                     static_cast<long long>(nbig), static_cast<long long>(big_cand), static_cast<long long>(max_item),
+                     ms_expand, ms_big, ms_rest);
+    }
     cudaEventDestroy(ev0);
     cudaEventDestroy(ev1);
     cudaEventDestroy(ev2);

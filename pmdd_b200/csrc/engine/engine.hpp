@@ -170,6 +170,7 @@ class Engine {
     uint32_t *d_err_ = nullptr;
     int64_t launches_ = 0;
     KernelTimes ktimes_;
+    bool trace_ = false;  // PMDD_TRACE=1: one stderr line per step
 };
 
 }  // namespace pmdd
