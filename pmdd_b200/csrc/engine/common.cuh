@@ -16,6 +16,13 @@ constexpr int kTileWindow = 1024;
 constexpr int kSmallMax = 1024;
 constexpr int kTileCap = 2 * kTileWindow;
 constexpr int kTileItemCap = 1024;   // destinations staged per pass inside one tile
+constexpr int kTileArcCap = 2048;    // arcs staged per pass inside one tile
+
+// Destinations filtered inside a tile; every other destination takes the oversized
+// path.  Both the counting pass and the tile kernel decide with this one rule.
+__host__ __device__ constexpr bool tile_resident(int64_t candidates, int64_t arcs) {
+    return candidates <= kSmallMax && arcs <= kTileArcCap / 2;
+}
 
 constexpr int kCountThreads = 1024;
 constexpr int kBigThreads = 256;
@@ -47,6 +54,7 @@ struct ExpandJob {
     int64_t total_cand;
     int64_t tile_base;             // first global tile index of this job
     int64_t num_tiles;
+    int32_t *tile_first;           // [num_tiles+1]: first destination of each tile (tile_plan_kernel)
     const int64_t *big_list;       // (local item, scratch offset) pairs
     int32_t num_big;
     int32_t pad0;

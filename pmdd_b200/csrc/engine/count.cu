@@ -39,7 +39,7 @@ __global__ void __launch_bounds__(kCountThreads) count_scan_kernel(const CountJo
         const int64_t e = J.arc_cand_off[J.item_arc_off[v + 1] - J.arc_base];
         const int64_t c = e - b;
         atomicMax(&s_max, static_cast<unsigned long long>(c));
-        if (c > kSmallMax) {
+        if (c > 0 && !tile_resident(c, J.item_arc_off[v + 1] - J.item_arc_off[v])) {
             const int k = atomicAdd(&s_nbig, 1);
             J.big_list[2 * k] = i;
             J.big_list[2 * k + 1] = c;

@@ -465,7 +465,9 @@ int Engine::step() {
         const size_t pts_bytes = static_cast<size_t>(std::max<int64_t>(C, 1)) * I.d * I.elem();
         e.out_pts = arena_.alloc(pts_bytes);
         e.out_off = static_cast<int64_t *>(arena_.alloc(sizeof(int64_t) * V));
-        e.out_size = static_cast<int32_t *>(arena_.alloc(sizeof(int32_t) * V));
+        // sizes of the new frontier, followed by the tile plan of this expansion
+        const int64_t ntiles = std::max<int64_t>(1, (C + dev::kTileWindow - 1) / dev::kTileWindow);
+        e.out_size = static_cast<int32_t *>(arena_.alloc(sizeof(int32_t) * (V + ntiles + 1)));
         bool okay = e.out_pts && e.out_off && e.out_size;
         if (okay && s.res.num_big > 0) {
             const int64_t bt = s.res.big_total;
@@ -503,14 +505,16 @@ int Engine::step() {
         int64_t tiles;
         size_t big_first, big_count;
         int64_t max_big;
+        int64_t items;             // destinations over the group's jobs
     };
     std::vector<GroupLaunch> glaunch;
+    std::vector<int64_t> tile_bases(exps.size()), item_bases(exps.size());  // group-relative
     {
         size_t pos = 0;
         std::vector<ExpPlan> ordered;
         ordered.reserve(exps.size());
         for (auto &g : groups) {
-            GroupLaunch gl{g.first.first, g.first.second, pos, g.second.size(), 0, bigwork.size(), 0, 0};
+            GroupLaunch gl{g.first.first, g.first.second, pos, g.second.size(), 0, bigwork.size(), 0, 0, 0};
             for (size_t idx : g.second) {
                 const ExpPlan &e = exps[idx];
                 Instance &I = *e.I;
@@ -541,8 +545,12 @@ int Engine::step() {
                 J.out_size = e.out_size;
                 J.total_cand = s.res.total;
                 J.num_tiles = std::max<int64_t>(1, (s.res.total + dev::kTileWindow - 1) / dev::kTileWindow);
+                J.tile_first = e.out_size + J.num_items;
                 J.tile_base = gl.tiles;
+                tile_bases[pos] = gl.tiles;
+                item_bases[pos] = gl.items;
                 gl.tiles += J.num_tiles;
+                gl.items += J.num_items;
                 J.big_list = s.big_list;
                 J.num_big = s.res.num_big;
                 if (e.big_mem) {
@@ -590,7 +598,9 @@ int Engine::step() {
     const size_t off_x = 0;
     const size_t off_b = align256(off_x + sizeof(dev::ExpandJob) * xjobs.size());
     const size_t off_c = align256(off_b + sizeof(dev::BigWork) * bigwork.size());
-    size_t off_k = align256(off_c + sizeof(dev::CountJob) * cjobs.size());
+    const size_t off_tb = align256(off_c + sizeof(dev::CountJob) * cjobs.size());
+    const size_t off_ib = align256(off_tb + sizeof(int64_t) * tile_bases.size());
+    size_t off_k = align256(off_ib + sizeof(int64_t) * item_bases.size());
     // coupling: requests at their cutset
     std::vector<Instance *> couplers;
     for (auto &p : active_)
@@ -693,6 +703,10 @@ int Engine::step() {
     if (!xjobs.empty()) std::memcpy(hs + off_x, xjobs.data(), sizeof(dev::ExpandJob) * xjobs.size());
     if (!bigwork.empty()) std::memcpy(hs + off_b, bigwork.data(), sizeof(dev::BigWork) * bigwork.size());
     if (!cjobs.empty()) std::memcpy(hs + off_c, cjobs.data(), sizeof(dev::CountJob) * cjobs.size());
+    if (!tile_bases.empty()) {
+        std::memcpy(hs + off_tb, tile_bases.data(), sizeof(int64_t) * tile_bases.size());
+        std::memcpy(hs + off_ib, item_bases.data(), sizeof(int64_t) * item_bases.size());
+    }
 
     // ------------------------------------------------- expansion bookkeeping
     // Sides move to their new layer now (host view); device work is stream-ordered.
@@ -794,11 +808,16 @@ int Engine::step() {
     cudaEventRecord(ev0, stream_);
     for (const GroupLaunch &gl : glaunch) {
         const dev::ExpandJob *dj = reinterpret_cast<const dev::ExpandJob *>(d_stage + off_x) + gl.first;
-        const int grid = sms_ * 4;
-        if (!cuda_ok(dev::launch_expand_tiles(gl.d, gl.wide, dj, static_cast<int>(gl.count), gl.tiles, grid, stream_),
+        const int64_t *dtb = reinterpret_cast<const int64_t *>(d_stage + off_tb) + gl.first;
+        const int64_t *dib = reinterpret_cast<const int64_t *>(d_stage + off_ib) + gl.first;
+        if (!cuda_ok(dev::launch_tile_plan(dj, dib, static_cast<int>(gl.count), gl.items, stream_), "tile_plan_kernel"))
+            return -1;
+        const int grid = sms_ * 8;
+        if (!cuda_ok(dev::launch_expand_tiles(gl.d, gl.wide, dj, dtb, static_cast<int>(gl.count), gl.tiles, grid,
+                                              stream_),
                      "expand_tile_kernel"))
             return -1;
-        launches_ += 1;
+        launches_ += 2;
     }
     cudaEventRecord(ev1, stream_);
     for (const GroupLaunch &gl : glaunch) {

@@ -8,8 +8,12 @@ namespace pmdd {
 namespace dev {
 
 cudaError_t launch_count_scan(const CountJob *jobs, int num_jobs, cudaStream_t stream);
-cudaError_t launch_expand_tiles(int d, bool wide, const ExpandJob *jobs, int num_jobs, int64_t total_tiles, int grid,
-                                cudaStream_t stream);
+cudaError_t launch_expand_tiles(int d, bool wide, const ExpandJob *jobs, const int64_t *tile_bases, int num_jobs,
+                                int64_t total_tiles, int grid, cudaStream_t stream);
+// Fills every job's tile_first (destination i belongs to tile min(start_i / kTileWindow,
+// num_tiles - 1)); one thread per destination over all jobs.
+cudaError_t launch_tile_plan(const ExpandJob *jobs, const int64_t *item_bases, int num_jobs, int64_t total_items,
+                             cudaStream_t stream);
 cudaError_t launch_big(int d, bool wide, const ExpandJob *jobs, const BigWork *work, int num_work, int64_t max_item,
                        int sms, cudaStream_t stream);
 
