@@ -194,10 +194,22 @@ __global__ void __launch_bounds__(SfsCfg<D, T>::kThreads) big_sfs_kernel(const E
                 for (int o = 0; o < D; ++o) p[o] = T(0);
             }
             bool dom = !valid;
-            for (int32_t j = 0; j < kn; ++j) {
-                const Pt q = j < KS ? kc[j] : load_global_pt<D, T>(out, j);
-                dom = dom || ge_all<D, T>(q, p);
-                if ((j & 31) == 31 && __all_sync(0xffffffffu, dom)) break;
+            {
+                const int32_t kn_s = kn < KS ? kn : KS;
+                int32_t j = 0;
+                int it = 0;
+                for (; j + 4 <= kn_s; j += 4) {
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) dom |= ge_all<D, T>(kc[j + u], p);
+                    if ((++it & 7) == 0 && __all_sync(0xffffffffu, dom)) break;
+                }
+                if (!__all_sync(0xffffffffu, dom)) {
+                    for (; j < kn_s; ++j) dom |= ge_all<D, T>(kc[j], p);
+                    for (j = KS; j < kn; ++j) {
+                        dom |= ge_all<D, T>(load_global_pt<D, T>(out, j), p);
+                        if ((j & 31) == 31 && __all_sync(0xffffffffu, dom)) break;
+                    }
+                }
             }
             const unsigned m = __ballot_sync(0xffffffffu, !dom);
             int32_t base = 0;

@@ -11,7 +11,7 @@ namespace dev {
 // starts inside its window of kTileWindow candidates; destinations of at most
 // kSmallMax candidates are filtered in shared memory, larger ones take the
 // global-memory ("big") path.  A tile therefore holds < 2*kTileWindow candidates.
-constexpr int kTileThreads = 256;
+constexpr int kTileThreads = 512;
 constexpr int kTileWindow = 1024;
 constexpr int kSmallMax = 1024;
 constexpr int kTileCap = 2 * kTileWindow;

@@ -52,6 +52,7 @@ struct TileSmem {
     int32_t tot_a;
     int32_t i0, i1;
     int32_t job;
+    int32_t chunk;                      // next 32-candidate chunk to filter
 };
 
 // First index in bases[0..n) with bases[idx] <= x < bases[idx+1] (bases ascending).
@@ -112,14 +113,38 @@ __device__ __forceinline__ bool sweep_range(const TileSmem<D, T> &S, int a, int 
     return dom;
 }
 
+// The common case: every lane's candidate lies in the same arc run of the same
+// destination, and [a, b) holds none of that run.  No per-lane range or arc checks;
+// the equal-point tie rule only matters for points before the lanes (j < q for all).
+template <int D, typename T>
+__device__ __forceinline__ bool sweep_other_arcs(const TileSmem<D, T> &S, int a, int b, const T (&p)[D], int q,
+                                                 bool dom) {
+    int j = a;
+    int it = 0;
+    for (; j + 4 <= b; j += 4) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const PackedPt<D, T> c = S.pts[j + u];
+            const bool ge = ge_all<D, T>(c, p);
+            dom |= ge && (j + u < q || !eq_all<D, T>(c, p));
+        }
+        if ((++it & 7) == 0 && __all_sync(0xffffffffu, dom)) return true;
+    }
+    for (; j < b; ++j) {
+        const PackedPt<D, T> c = S.pts[j];
+        const bool ge = ge_all<D, T>(c, p);
+        dom |= ge && (j < q || !eq_all<D, T>(c, p));
+    }
+    return dom;
+}
+
 template <int D, typename T>
 __global__ void __launch_bounds__(kTT) expand_tile_kernel(const ExpandJob *__restrict__ jobs,
                                                           const int64_t *__restrict__ tile_bases, int num_jobs,
                                                           int64_t total_tiles) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     TileSmem<D, T> &S = *reinterpret_cast<TileSmem<D, T> *>(smem_raw);
-    constexpr int NW = kTT / 32;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tid = threadIdx.x, lane = tid & 31;
     for (int64_t tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
         if (tid == 0) {
             const int j = find_base(tile_bases, num_jobs, tile);
@@ -204,6 +229,7 @@ __global__ void __launch_bounds__(kTT) expand_tile_kernel(const ExpandJob *__res
                 S.item_arc0[n_it] = static_cast<int16_t>(ea);
                 S.tot_i = e;
                 S.tot_a = ea;
+                S.chunk = 0;
             }
             __syncthreads();
             const int32_t total = S.tot_i, total_a = S.tot_a;
@@ -256,7 +282,11 @@ __global__ void __launch_bounds__(kTT) expand_tile_kernel(const ExpandJob *__res
             }
             __syncthreads();
             // --- filter: warp per 32 candidates, uniform sweep over their destinations
-            for (int c0 = warp * 32; c0 < total; c0 += NW * 32) {
+            while (true) {
+                int c0 = 0;
+                if (lane == 0) c0 = atomicAdd(&S.chunk, 1) * 32;
+                c0 = __shfl_sync(0xffffffffu, c0, 0);
+                if (c0 >= total) break;
                 const int q = c0 + lane;
                 const bool valid = q < total;
                 T p[D];
@@ -281,8 +311,8 @@ __global__ void __launch_bounds__(kTT) expand_tile_kernel(const ExpandJob *__res
                 const bool one_run = __all_sync(0xffffffffu, valid) && warp_min_i(my_tag) == warp_max_i(my_tag);
                 bool dom = !valid;
                 if (one_run) {
-                    dom = sweep_range<D, T>(S, J0, slo, p, q, my_tag, js, je, dom);
-                    if (!__all_sync(0xffffffffu, dom)) dom = sweep_range<D, T>(S, shi, J1, p, q, my_tag, js, je, dom);
+                    dom = sweep_other_arcs<D, T>(S, J0, slo, p, q, dom);
+                    if (!__all_sync(0xffffffffu, dom)) dom = sweep_other_arcs<D, T>(S, shi, J1, p, q, dom);
                 } else {
                     dom = sweep_range<D, T>(S, J0, J1, p, q, my_tag, js, je, dom);
                 }
