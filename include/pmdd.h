@@ -138,6 +138,15 @@ int pmdd_enumerate_batch(const pmdd_dd *dds, int32_t count, const pmdd_options *
                          pmdd_frontier *outs, int32_t *status, pmdd_stats *stats,
                          char *err, size_t errlen);
 
+/* Standalone Pareto filter of one point set on the GPU: writes the maximal points of
+ * points[0..num_points) under componentwise >= (one copy of each group of equal
+ * points) into `out` (capacity num_points*nobjs) and their count into *out_points.
+ * The merge rule of the reference's ParetoFrontier::merge
+ * (src/pmdd/enum/pareto_frontier.hpp:237-303) applied to a whole set at once; output
+ * order is unspecified.  Host buffers; num_points < 2^31, nobjs 1..8. */
+int pmdd_pareto_filter(const int32_t *points, int64_t num_points, int32_t nobjs, int32_t *out, int64_t *out_points,
+                       int32_t device, char *err, size_t errlen);
+
 /* Device-resident DD set: uploads `count` DDs once (with both arc directions) into
  * the device engine's memory; pmdd_resident_enumerate then runs a batch over them
  * with no host->device DD traffic.  Frees with pmdd_resident_free. */

@@ -7,6 +7,7 @@
 #include <unordered_map>
 
 #include "engine.hpp"
+#include "pareto.cuh"
 #include "pmdd.h"
 
 namespace {
@@ -272,6 +273,57 @@ int pmdd_enumerate_batch(const pmdd_dd *dds, int32_t count, const pmdd_options *
         return rc;
     }
     return collect_batch(reqs, outs, status, stats, info, err, errlen);
+}
+
+// ------------------------------------------------------- standalone filter
+int pmdd_pareto_filter(const int32_t *points, int64_t num_points, int32_t nobjs, int32_t *out, int64_t *out_points,
+                       int32_t device, char *err, size_t errlen) {
+    if (out_points) *out_points = 0;
+    if (nobjs < 1 || nobjs > 8 || num_points < 0 || num_points >= (static_cast<int64_t>(1) << 31) ||
+        (num_points > 0 && (!points || !out)) || !out_points) {
+        write_err(err, errlen, "invalid point set (nobjs 1..8, 0 <= num_points < 2^31, non-NULL buffers)");
+        return PMDD_ERR_INVALID;
+    }
+    if (num_points == 0) return PMDD_OK;
+    DeviceSlot &slot = slot_for(device);
+    std::lock_guard<std::mutex> lk(slot.mu);
+    std::string msg;
+    if (ensure_engine(device, slot, &msg) != PMDD_OK) {
+        write_err(err, errlen, msg);
+        return PMDD_ERR_NO_DEVICE;
+    }
+    pmdd::Engine &E = *slot.engine;
+    const size_t bytes = static_cast<size_t>(num_points) * nobjs * sizeof(int32_t);
+    void *d_in = E.alloc(bytes), *d_out = E.alloc(bytes), *d_n = E.alloc(sizeof(int64_t));
+    void *d_scratch = E.alloc(pmdd::dev::pareto_scratch_bytes(nobjs, num_points));
+    int rc = PMDD_OK;
+    if (!d_in || !d_out || !d_n || !d_scratch) {
+        write_err(err, errlen, "point set does not fit the device memory budget");
+        rc = PMDD_ERR_OOM;
+    } else {
+        cudaStream_t st = E.stream();
+        cudaError_t e = cudaMemcpyAsync(d_in, points, bytes, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess)
+            e = pmdd::dev::launch_pareto_filter(nobjs, static_cast<const int32_t *>(d_in), num_points, d_scratch,
+                                                static_cast<int32_t *>(d_out), static_cast<int64_t *>(d_n), st);
+        E.count_launches(1);
+        int64_t n_out = 0;
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&n_out, d_n, sizeof(int64_t), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e == cudaSuccess && n_out > 0)
+            e = cudaMemcpy(out, d_out, static_cast<size_t>(n_out) * nobjs * sizeof(int32_t), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) {
+            write_err(err, errlen, std::string("CUDA error: ") + cudaGetErrorString(e));
+            rc = PMDD_ERR_CUDA;
+        } else {
+            *out_points = n_out;
+        }
+    }
+    E.release(d_in);
+    E.release(d_out);
+    E.release(d_n);
+    E.release(d_scratch);
+    return rc;
 }
 
 // --------------------------------------------------------- resident DD sets

@@ -140,6 +140,13 @@ class Engine {
     // the arena until release_dd(); requests then share it via external_dd.
     bool upload_dd(Instance &I);
     void release_dd(Instance &I);
+    // Raw arena memory for standalone operations run on this engine's stream.
+    void *alloc(size_t bytes) { return arena_.alloc(bytes); }
+    void release(void *p) { arena_.release(p); }
+    void count_launches(int64_t n) {
+        launches_ += n;
+        g_total_launches += n;
+    }
 
   private:
     struct Pinned {

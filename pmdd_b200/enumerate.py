@@ -101,6 +101,22 @@ def enumerate_batch(dds: Iterable[DecisionDiagram], method: int = 1, state_domin
     return res
 
 
+def pareto_filter(points: np.ndarray, device: int = 0) -> np.ndarray:
+    """Maximal points of an (n, d) int32 set under componentwise >= (one copy of each
+    group of equal points), computed on the GPU (pmdd_pareto_filter)."""
+    pts = np.ascontiguousarray(points, dtype=np.int32)
+    n, d = pts.shape
+    out = np.empty_like(pts)
+    n_out = ctypes.c_int64()
+    err = ctypes.create_string_buffer(512)
+    P = ctypes.POINTER(ctypes.c_int32)
+    rc = _native.gpu_lib().pmdd_pareto_filter(pts.ctypes.data_as(P), n, d, out.ctypes.data_as(P),
+                                              ctypes.byref(n_out), device, err, len(err))
+    if rc != _native.PMDD_OK:
+        raise CudaEnumerationError(rc, err.value.decode(errors="replace"))
+    return out[: n_out.value].copy()
+
+
 class ResidentSet:
     """DDs uploaded once to device memory (pmdd_resident_*); each `enumerate` call runs
     a batch over them with no host->device DD traffic."""

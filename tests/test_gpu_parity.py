@@ -149,3 +149,24 @@ def test_invalid_dd_is_rejected_not_run():
     dd = P.DecisionDiagram.from_text(instances.knapsack_text(5, 3, 1), 1, 3)
     with pytest.raises(P.CudaEnumerationError):
         P.enumerate_dd(dd, method=2)
+
+
+def test_standalone_pareto_filter_against_oracle():
+    """pmdd_pareto_filter keeps exactly the maximal points, one copy of each."""
+    rng = np.random.default_rng(11)
+    for n, d, hi in ((1, 3, 5), (2, 1, 3), (700, 3, 40), (5000, 4, 60), (20000, 3, 2000), (3000, 8, 6),
+                     (40000, 2, 100000)):
+        pts = rng.integers(-hi, hi, size=(n, d)).astype(np.int32)
+        keep = oracle.nd_keep(pts) if n <= 5000 else None
+        got = P.pareto_filter(pts)
+        if keep is not None:
+            assert same_set(got, pts[keep])
+        # properties that hold at any size: an antichain without duplicates that covers the set
+        assert len(np.unique(got, axis=0)) == len(got)
+        g = got.astype(np.int64)
+        sample = pts[rng.choice(n, size=min(n, 300), replace=False)].astype(np.int64)
+        for p in sample:
+            assert np.any(np.all(g >= p, axis=1))
+        for i in range(min(len(g), 200)):
+            dom = np.all(g >= g[i], axis=1) & np.any(g != g[i], axis=1)
+            assert not dom.any()
