@@ -147,6 +147,20 @@ int pmdd_enumerate_batch(const pmdd_dd *dds, int32_t count, const pmdd_options *
 int pmdd_pareto_filter(const int32_t *points, int64_t num_points, int32_t nobjs, int32_t *out, int64_t *out_points,
                        int32_t device, char *err, size_t errlen);
 
+/* Allocation-free variant of pmdd_pareto_filter, for callers that cannot allocate
+ * device memory (inside stream capture, under an allocator that owns the device, or
+ * in services that forbid allocation after start-up).  No counterpart in the
+ * reference.  Device buffers: d_points (num_points*nobjs) in, d_out (same capacity)
+ * out; *out_points (host) receives the count; `stream` is a cudaStream_t (NULL: the
+ * default stream).  Scratch comes from a fixed device array of about 9.4 MB that every
+ * device loading this library holds until exit: at most 131072 points of at most 8
+ * objectives per call (larger sets return PMDD_ERR_RANGE).  Calls share that array, so
+ * calls that overlap on the GPU race; serialise them.  The first call on a device
+ * looks up the array's address and should happen before any stream capture.
+ * Allocates nothing; synchronises `stream` before returning. */
+int pmdd_pareto_filter_noalloc(const int32_t *d_points, int64_t num_points, int32_t nobjs, int32_t *d_out,
+                               int64_t *out_points, void *stream, char *err, size_t errlen);
+
 /* Device-resident DD set: uploads `count` DDs once (with both arc directions) into
  * the device engine's memory; pmdd_resident_enumerate then runs a batch over them
  * with no host->device DD traffic.  Frees with pmdd_resident_free. */

@@ -151,6 +151,9 @@ GPU_SYMBOLS = {
     ),
     "pmdd_pareto_filter": (ctypes.c_int, [P_i32, c_i64, c_i32, P_i32, ctypes.POINTER(c_i64), c_i32, ctypes.c_char_p,
                                           ctypes.c_size_t]),
+    "pmdd_pareto_filter_noalloc": (ctypes.c_int, [ctypes.c_void_p, c_i64, c_i32, ctypes.c_void_p,
+                                                  ctypes.POINTER(c_i64), ctypes.c_void_p, ctypes.c_char_p,
+                                                  ctypes.c_size_t]),
     "pmdd_resident_upload": (ctypes.c_void_p, [ctypes.POINTER(PmddDD), c_i32, c_i32, ctypes.c_char_p,
                                                 ctypes.c_size_t]),
     "pmdd_resident_enumerate": (
