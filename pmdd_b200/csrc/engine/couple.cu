@@ -2,11 +2,14 @@
 //  - out-arc CSR (transpose of the in-arc CSR) for the bottom-up direction;
 //  - the cutset join  F = ND( U_v { t + b : t in TD_v, b in BU_v } )  of
 //    src/pmdd/enum/gpu/couple.cu:340-498 / src/pmdd/enum/cpu/enum.cpp:333-398, done in
-//    rounds without ever materialising all products: a round streams products of the
-//    remaining cutset nodes against the running frontier F held in shared memory (with
-//    per-node and per-row ideal-point bounds that discard whole groups of products),
-//    appends survivors behind F, and re-filters F + survivors.
+//    rounds without ever materialising all products.  A seed round builds a first
+//    running frontier from a few extreme products per cutset node; each product round
+//    streams the remaining products against the running frontier F held in shared
+//    memory (per-node and per-row ideal-point bounds discard whole groups of products
+//    first), appends survivors behind F, and re-filters F + survivors with the
+//    sort-filter-skyline block routine of sfs.cuh.
 #include "couple.cuh"
+#include "sfs.cuh"
 
 namespace pmdd {
 namespace dev {
@@ -87,43 +90,148 @@ cudaError_t launch_build_out_csr(const int32_t *in_off, const int32_t *arc_src, 
 }
 
 // ------------------------------------------------------------------ coupling
-template <int D, typename T>
-__device__ __forceinline__ bool weakly_dominated_by_smem(const T (&p)[D], const T *fs, int nf, int stride) {
-    for (int j = 0; j < nf; ++j) {
-        bool ge = true;
-#pragma unroll
-        for (int o = 0; o < D; ++o) ge &= (fs[o * stride + j] >= p[o]);
-        if (ge) return true;
-    }
-    return false;
+__global__ void couple_products_kernel(const CoupleJob *__restrict__ jobs) {
+    const CoupleJob &J = jobs[blockIdx.x];
+    unsigned long long acc = 0;
+    for (int32_t v = threadIdx.x; v < J.num_nodes; v += blockDim.x)
+        acc += static_cast<unsigned long long>(J.td_size[v]) * static_cast<unsigned long long>(J.bu_size[v]);
+    for (int s = 16; s > 0; s >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, s);
+    if ((threadIdx.x & 31) == 0 && acc) atomicAdd(reinterpret_cast<unsigned long long *>(&J.ctr[kCtrProducts]), acc);
 }
 
-// Warp-cooperative test: is `p` weakly dominated by any staged frontier point?
+cudaError_t launch_couple_products(const CoupleJob *jobs, int num_jobs, cudaStream_t stream) {
+    if (num_jobs <= 0) return cudaSuccess;
+    couple_products_kernel<<<num_jobs, 256, 0, stream>>>(jobs);
+    return cudaGetLastError();
+}
+
+// Appends points behind F; warp-aggregated.  Returns false (and records where the
+// round must resume) when U is full.
 template <int D, typename T>
-__device__ __forceinline__ bool warp_dominated(const T (&p)[D], const T *fs, int nf, int stride, int lane) {
-    bool hit = false;
-    for (int j = lane; j < nf && !hit; j += 32) {
-        bool ge = true;
-#pragma unroll
-        for (int o = 0; o < D; ++o) ge &= (fs[o * stride + j] >= p[o]);
-        hit = ge;
+__device__ __forceinline__ bool append_points(const CoupleJob &J, T *U, int64_t fn, bool keep, const T (&p)[D],
+                                              int32_t v, int lane) {
+    const unsigned m = __ballot_sync(0xffffffffu, keep);
+    if (m == 0) return true;
+    unsigned long long base = 0;
+    if (lane == 0)
+        base = atomicAdd(reinterpret_cast<unsigned long long *>(&J.ctr[kCtrB]), static_cast<unsigned long long>(__popc(m)));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    const int64_t pos0 = fn + static_cast<int64_t>(base);
+    if (pos0 + __popc(m) > J.ucap) {
+        // every later append lands further out, so [F, pos0) is complete
+        if (lane == 0) {
+            atomicMin(reinterpret_cast<unsigned long long *>(&J.ctr[kCtrResume]), static_cast<unsigned long long>(v));
+            atomicMin(reinterpret_cast<unsigned long long *>(&J.ctr[kCtrValidEnd]),
+                      static_cast<unsigned long long>(pos0));
+        }
+        return false;
     }
+    if (keep) {
+        const int64_t pos = pos0 + __popc(m & ((1u << lane) - 1u));
+#pragma unroll
+        for (int o = 0; o < D; ++o) U[pos * D + o] = p[o];
+    }
+    return true;
+}
+
+// Seed round: per cutset node, the products of the two frontiers' maximisers of each
+// objective and of the objective sum (warp per node).
+template <int D, typename T>
+__global__ void __launch_bounds__(kCoupleThreads) couple_seed_kernel(const CoupleJob *__restrict__ jobs) {
+    const CoupleJob &J = jobs[blockIdx.y];
+    T *U = static_cast<T *>(J.U);
+    const T *td = static_cast<const T *>(J.td_pts);
+    const T *bu = static_cast<const T *>(J.bu_pts);
+    const int lane = threadIdx.x & 31;
+    const int warps = gridDim.x * (kCoupleThreads / 32);
+    for (int32_t v = blockIdx.x * (kCoupleThreads / 32) + (threadIdx.x >> 5); v < J.num_nodes; v += warps) {
+        const int32_t nt = J.td_size[v], nb = J.bu_size[v];
+        if (nt == 0 || nb == 0) continue;
+        const T *tdv = td + J.td_off[v] * D;
+        const T *buv = bu + J.bu_off[v] * D;
+        // argmax per objective (0..D-1) and of the sum (D), per side
+        int64_t bt[D + 1], bb[D + 1];
+        int32_t it[D + 1], ib[D + 1];
+#pragma unroll
+        for (int k = 0; k <= D; ++k) {
+            bt[k] = bb[k] = INT64_MIN;
+            it[k] = ib[k] = 0;
+        }
+        for (int32_t i = lane; i < nt; i += 32) {
+            int64_t s = 0;
+#pragma unroll
+            for (int o = 0; o < D; ++o) {
+                const int64_t x = tdv[static_cast<int64_t>(i) * D + o];
+                s += x;
+                if (x > bt[o]) { bt[o] = x; it[o] = i; }
+            }
+            if (s > bt[D]) { bt[D] = s; it[D] = i; }
+        }
+        for (int32_t i = lane; i < nb; i += 32) {
+            int64_t s = 0;
+#pragma unroll
+            for (int o = 0; o < D; ++o) {
+                const int64_t x = buv[static_cast<int64_t>(i) * D + o];
+                s += x;
+                if (x > bb[o]) { bb[o] = x; ib[o] = i; }
+            }
+            if (s > bb[D]) { bb[D] = s; ib[D] = i; }
+        }
+#pragma unroll
+        for (int k = 0; k <= D; ++k) {
+            for (int sft = 16; sft > 0; sft >>= 1) {
+                const int64_t ot = __shfl_xor_sync(0xffffffffu, bt[k], sft);
+                const int32_t oi = __shfl_xor_sync(0xffffffffu, it[k], sft);
+                if (ot > bt[k] || (ot == bt[k] && oi < it[k])) { bt[k] = ot; it[k] = oi; }
+                const int64_t ob = __shfl_xor_sync(0xffffffffu, bb[k], sft);
+                const int32_t oj = __shfl_xor_sync(0xffffffffu, ib[k], sft);
+                if (ob > bb[k] || (ob == bb[k] && oj < ib[k])) { bb[k] = ob; ib[k] = oj; }
+            }
+        }
+        // lane k < D+1 emits product k
+        T p[D];
+        bool keep = false;
+#pragma unroll
+        for (int k = 0; k <= D; ++k) {
+            if (lane == k) {
+#pragma unroll
+                for (int o = 0; o < D; ++o)
+                    p[o] = tdv[static_cast<int64_t>(it[k]) * D + o] + buv[static_cast<int64_t>(ib[k]) * D + o];
+                keep = true;
+            }
+        }
+        if (!keep) {
+#pragma unroll
+            for (int o = 0; o < D; ++o) p[o] = T(0);
+        }
+        if (!append_points<D, T>(J, U, 0, keep, p, v, lane)) break;
+    }
+}
+
+// Is a single point weakly dominated by any staged frontier point?  (lanes split F)
+template <int D, typename T>
+__device__ __forceinline__ bool warp_point_dominated(const PackedPt<D, T> *fs, int nf, const T (&p)[D], int lane) {
+    bool hit = false;
+    for (int j = lane; j < nf && !hit; j += 32) hit = ge_all<D, T>(fs[j], p);
     return __any_sync(0xffffffffu, hit);
 }
 
 template <int D, typename T>
 __global__ void __launch_bounds__(kCoupleThreads) couple_prune_kernel(const CoupleJob *__restrict__ jobs) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T *fs = reinterpret_cast<T *>(smem_raw);  // [D][kCoupleFS]
+    PackedPt<D, T> *fs = reinterpret_cast<PackedPt<D, T> *>(smem_raw);  // [kCoupleFS]
     const CoupleJob &J = jobs[blockIdx.y];
     T *U = static_cast<T *>(J.U);
     const T *td = static_cast<const T *>(J.td_pts);
     const T *bu = static_cast<const T *>(J.bu_pts);
     const int64_t fn = J.ctr[kCtrF];
     const int nf = static_cast<int>(fn < kCoupleFS ? fn : kCoupleFS);
-    for (int k = threadIdx.x; k < nf; k += blockDim.x)
+    for (int k = threadIdx.x; k < nf; k += blockDim.x) {
+        PackedPt<D, T> q;
 #pragma unroll
-        for (int o = 0; o < D; ++o) fs[o * kCoupleFS + k] = U[static_cast<int64_t>(k) * D + o];
+        for (int o = 0; o < PackedPt<D, T>::kPad; ++o) q.v[o] = o < D ? U[static_cast<int64_t>(k) * D + o] : T(0);
+        fs[k] = q;
+    }
     __syncthreads();
     const int lane = threadIdx.x & 31;
     unsigned long long evaluated = 0;
@@ -163,7 +271,7 @@ __global__ void __launch_bounds__(kCoupleThreads) couple_prune_kernel(const Coup
         T ub[D];
 #pragma unroll
         for (int o = 0; o < D; ++o) ub[o] = mt[o] + mb[o];
-        if (warp_dominated<D, T>(ub, fs, nf, kCoupleFS, lane)) continue;
+        if (warp_point_dominated<D, T>(fs, nf, ub, lane)) continue;
         bool overflowed = false;
         for (int t = 0; t < nt && !overflowed; ++t) {
             T tp[D], rub[D];
@@ -172,40 +280,27 @@ __global__ void __launch_bounds__(kCoupleThreads) couple_prune_kernel(const Coup
                 tp[o] = tdv[static_cast<int64_t>(t) * D + o];
                 rub[o] = tp[o] + mb[o];
             }
-            if (warp_dominated<D, T>(rub, fs, nf, kCoupleFS, lane)) continue;
+            if (warp_point_dominated<D, T>(fs, nf, rub, lane)) continue;
             for (int b0 = 0; b0 < nb; b0 += 32) {
                 const int b = b0 + lane;
-                bool keep = false;
+                const bool valid = b < nb;
                 T p[D];
-                if (b < nb) {
 #pragma unroll
-                    for (int o = 0; o < D; ++o) p[o] = tp[o] + buv[static_cast<int64_t>(b) * D + o];
-                    keep = !weakly_dominated_by_smem<D, T>(p, fs, nf, kCoupleFS);
-                    ++evaluated;
+                for (int o = 0; o < D; ++o) p[o] = valid ? tp[o] + buv[static_cast<int64_t>(b) * D + o] : T(0);
+                bool dom = !valid;
+                // warp-uniform sweep of the staged frontier
+                int j = 0, it = 0;
+                for (; j + 4 <= nf; j += 4) {
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) dom |= ge_all<D, T>(fs[j + u], p);
+                    if ((++it & 7) == 0 && __all_sync(0xffffffffu, dom)) break;
                 }
-                const unsigned m = __ballot_sync(0xffffffffu, keep);
-                if (m == 0) continue;
-                unsigned long long base = 0;
-                if (lane == 0)
-                    base = atomicAdd(reinterpret_cast<unsigned long long *>(&J.ctr[kCtrB]),
-                                     static_cast<unsigned long long>(__popc(m)));
-                base = __shfl_sync(0xffffffffu, base, 0);
-                const int64_t pos0 = fn + static_cast<int64_t>(base);
-                if (pos0 + __popc(m) > J.ucap) {
-                    // every later append lands further out, so [F, pos0) is complete
-                    if (lane == 0) {
-                        atomicMin(reinterpret_cast<unsigned long long *>(&J.ctr[kCtrResume]),
-                                  static_cast<unsigned long long>(v));
-                        atomicMin(reinterpret_cast<unsigned long long *>(&J.ctr[kCtrValidEnd]),
-                                  static_cast<unsigned long long>(pos0));
-                    }
+                if (!__all_sync(0xffffffffu, dom))
+                    for (; j < nf; ++j) dom |= ge_all<D, T>(fs[j], p);
+                if (valid) ++evaluated;
+                if (!append_points<D, T>(J, U, fn, !dom, p, v, lane)) {
                     overflowed = true;
                     break;
-                }
-                if (keep) {
-                    const int64_t pos = pos0 + __popc(m & ((1u << lane) - 1u));
-#pragma unroll
-                    for (int o = 0; o < D; ++o) U[pos * D + o] = p[o];
                 }
             }
         }
@@ -214,169 +309,67 @@ __global__ void __launch_bounds__(kCoupleThreads) couple_prune_kernel(const Coup
     if (lane == 0 && evaluated) atomicAdd(reinterpret_cast<unsigned long long *>(&J.ctr[kCtrEvaluated]), evaluated);
 }
 
-// Keep flags of F + survivors: a point is dropped iff another point is >= on every
-// objective and (differs, or comes first).  Points of the old frontier (index < F)
-// are mutually non-dominated, so they are only compared with the new points.
+// F + survivors -> next running frontier in U_alt (one block per job), and the round's
+// bookkeeping.
 template <int D, typename T>
-__global__ void __launch_bounds__(kBigThreads) couple_filter_kernel(const CoupleJob *__restrict__ jobs) {
-    constexpr int JT = (kBigJTile * D * static_cast<int>(sizeof(T)) > 32768) ? 32768 / (D * static_cast<int>(sizeof(T)))
-                                                                            : kBigJTile;
-    __shared__ T sj[D][JT];
-    const CoupleJob &J = jobs[blockIdx.y];
-    const T *U = static_cast<const T *>(J.U);
-    const int64_t fn = J.ctr[kCtrF];
-    int64_t n = fn + J.ctr[kCtrB];
-    if (n > J.ctr[kCtrValidEnd]) n = J.ctr[kCtrValidEnd];
-    if (n > J.ucap) n = J.ucap;
-    for (int64_t i0 = static_cast<int64_t>(blockIdx.x) * kBigThreads; i0 < n;
-         i0 += static_cast<int64_t>(gridDim.x) * kBigThreads) {
-        const int64_t i = i0 + threadIdx.x;
-        const bool valid = i < n;
-        T p[D];
-        if (valid)
-#pragma unroll
-            for (int o = 0; o < D; ++o) p[o] = U[i * D + o];
-        bool dom = !valid;
-        const int64_t jstart = (i0 + kBigThreads <= fn) ? fn : 0;  // whole block in old F: compare new points only
-        for (int64_t j0 = jstart; j0 < n; j0 += JT) {
-            if (__syncthreads_and(dom)) break;
-            const int m = static_cast<int>(n - j0 < JT ? n - j0 : static_cast<int64_t>(JT));
-            for (int k = threadIdx.x; k < m; k += kBigThreads)
-#pragma unroll
-                for (int o = 0; o < D; ++o) sj[o][k] = U[(j0 + k) * D + o];
-            __syncthreads();
-            if (!dom) {
-                for (int k = 0; k < m; ++k) {
-                    const int64_t j = j0 + k;
-                    if (j == i) continue;
-                    bool ge = true, eq = true;
-#pragma unroll
-                    for (int o = 0; o < D; ++o) {
-                        const T x = sj[o][k];
-                        ge &= (x >= p[o]);
-                        eq &= (x == p[o]);
-                    }
-                    if (ge && (!eq || j < i)) {
-                        dom = true;
-                        break;
-                    }
-                }
-            }
-        }
-        if (valid) J.keep[i] = dom ? 0 : 1;
-        __syncthreads();
-    }
-}
-
-// In-place compaction of F + survivors (one block per job) and round bookkeeping.
-template <int D, typename T>
-__global__ void __launch_bounds__(1024) couple_compact_kernel(const CoupleJob *__restrict__ jobs) {
-    __shared__ int32_t warp_buf[32];
-    __shared__ int64_t s_carry;
+__global__ void __launch_bounds__(SfsCfg<D, T>::kThreads) couple_sfs_kernel(const CoupleJob *__restrict__ jobs,
+                                                                            int seed) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     const CoupleJob &J = jobs[blockIdx.x];
-    T *U = static_cast<T *>(J.U);
     const int64_t fn = J.ctr[kCtrF];
     int64_t n = fn + J.ctr[kCtrB];
     if (n > J.ctr[kCtrValidEnd]) n = J.ctr[kCtrValidEnd];
     if (n > J.ucap) n = J.ucap;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (threadIdx.x == 0) s_carry = 0;
-    __syncthreads();
-    for (int64_t base = 0; base < n; base += 1024) {
-        const int64_t i = base + threadIdx.x;
-        const int32_t k = (i < n && J.keep[i]) ? 1 : 0;
-        T p[D];
-        if (k)
-#pragma unroll
-            for (int o = 0; o < D; ++o) p[o] = U[i * D + o];
-        int32_t inc = k;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int32_t y = __shfl_up_sync(0xffffffffu, inc, o);
-            if (lane >= o) inc += y;
-        }
-        if (lane == 31) warp_buf[warp] = inc;
-        __syncthreads();  // also: every read of this chunk happens before any write below
-        if (warp == 0) {
-            const int32_t w = warp_buf[lane];
-            int32_t winc = w;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int32_t y = __shfl_up_sync(0xffffffffu, winc, o);
-                if (lane >= o) winc += y;
-            }
-            warp_buf[lane] = winc - w;
-        }
-        __syncthreads();
-        if (k) {
-            const int64_t dst = s_carry + warp_buf[warp] + inc - 1;
-#pragma unroll
-            for (int o = 0; o < D; ++o) U[dst * D + o] = p[o];
-        }
-        __syncthreads();
-        if (threadIdx.x == 1023) s_carry += warp_buf[31] + inc;
-        __syncthreads();
-    }
+    SfsScratch<T> s;
+    s.P2 = static_cast<T *>(J.sc_pts2);
+    s.I2 = J.sc_idx;
+    s.SV = static_cast<T *>(J.sc_surv);
+    s.SVI = J.sc_sidx;
+    const int32_t kept = sfs_block<D, T>(smem_raw, static_cast<const T *>(J.U), n, s, static_cast<T *>(J.U_alt));
     if (threadIdx.x == 0) {
         const int64_t resume = J.ctr[kCtrResume];
-        J.ctr[kCtrF] = s_carry;
+        J.ctr[kCtrF] = kept;
         J.ctr[kCtrB] = 0;
-        J.ctr[kCtrCursor] = resume < J.num_nodes ? resume : J.num_nodes;
-        J.ctr[kCtrDone] = resume >= J.num_nodes ? 1 : 0;
+        if (seed) {
+            J.ctr[kCtrCursor] = 0;
+            J.ctr[kCtrDone] = 0;
+        } else {
+            J.ctr[kCtrCursor] = resume < J.num_nodes ? resume : J.num_nodes;
+            J.ctr[kCtrDone] = resume >= J.num_nodes ? 1 : 0;
+        }
         J.ctr[kCtrResume] = J.num_nodes;
         J.ctr[kCtrValidEnd] = J.ucap;
     }
 }
 
 template <int D, typename T>
-static cudaError_t launch_couple_round_t(const CoupleJob *jobs, int num_jobs, int blocks_per_job, cudaStream_t stream) {
-    const size_t smem = static_cast<size_t>(kCoupleFS) * D * sizeof(T);
+static cudaError_t launch_couple_round_t(const CoupleJob *jobs, int num_jobs, int blocks_per_job, bool seed,
+                                        cudaStream_t stream) {
+    const size_t smem = static_cast<size_t>(kCoupleFS) * sizeof(PackedPt<D, T>);
+    using Cfg = SfsCfg<D, T>;
     static bool attr_set = false;
     if (!attr_set) {
         cudaError_t e = cudaFuncSetAttribute(couple_prune_kernel<D, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              static_cast<int>(smem));
         if (e != cudaSuccess) return e;
+        e = cudaFuncSetAttribute(couple_sfs_kernel<D, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(Cfg::kSmem));
+        if (e != cudaSuccess) return e;
         attr_set = true;
     }
-    couple_prune_kernel<D, T><<<dim3(blocks_per_job, num_jobs), kCoupleThreads, smem, stream>>>(jobs);
-    couple_filter_kernel<D, T><<<dim3(blocks_per_job * 2, num_jobs), kBigThreads, 0, stream>>>(jobs);
-    couple_compact_kernel<D, T><<<num_jobs, 1024, 0, stream>>>(jobs);
+    if (seed) couple_seed_kernel<D, T><<<dim3(blocks_per_job, num_jobs), kCoupleThreads, 0, stream>>>(jobs);
+    else couple_prune_kernel<D, T><<<dim3(blocks_per_job, num_jobs), kCoupleThreads, smem, stream>>>(jobs);
+    couple_sfs_kernel<D, T><<<num_jobs, Cfg::kThreads, Cfg::kSmem, stream>>>(jobs, seed ? 1 : 0);
     return cudaGetLastError();
 }
 
-__global__ void couple_products_kernel(const CoupleJob *__restrict__ jobs) {
-    const CoupleJob &J = jobs[blockIdx.x];
-    unsigned long long acc = 0;
-    for (int32_t v = threadIdx.x; v < J.num_nodes; v += blockDim.x)
-        acc += static_cast<unsigned long long>(J.td_size[v]) * static_cast<unsigned long long>(J.bu_size[v]);
-    for (int s = 16; s > 0; s >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, s);
-    if ((threadIdx.x & 31) == 0 && acc) atomicAdd(reinterpret_cast<unsigned long long *>(&J.ctr[kCtrProducts]), acc);
-}
-
-cudaError_t launch_couple_products(const CoupleJob *jobs, int num_jobs, cudaStream_t stream) {
-    if (num_jobs <= 0) return cudaSuccess;
-    couple_products_kernel<<<num_jobs, 256, 0, stream>>>(jobs);
-    return cudaGetLastError();
-}
-
-#define PMDD_DISPATCH_D(D_, CALL)                  \
-    switch (D_) {                                  \
-    case 1: { constexpr int DD = 1; return CALL; } \
-    case 2: { constexpr int DD = 2; return CALL; } \
-    case 3: { constexpr int DD = 3; return CALL; } \
-    case 4: { constexpr int DD = 4; return CALL; } \
-    case 5: { constexpr int DD = 5; return CALL; } \
-    case 6: { constexpr int DD = 6; return CALL; } \
-    case 7: { constexpr int DD = 7; return CALL; } \
-    case 8: { constexpr int DD = 8; return CALL; } \
-    default: return cudaErrorInvalidValue;         \
-    }
-
-cudaError_t launch_couple_round(int d, bool wide, const CoupleJob *jobs, int num_jobs, int blocks_per_job,
+cudaError_t launch_couple_round(int d, bool wide, const CoupleJob *jobs, int num_jobs, int blocks_per_job, bool seed,
                                 cudaStream_t stream) {
     if (num_jobs <= 0) return cudaSuccess;
-    if (wide) { PMDD_DISPATCH_D(d, (launch_couple_round_t<DD, int64_t>(jobs, num_jobs, blocks_per_job, stream))); }
-    PMDD_DISPATCH_D(d, (launch_couple_round_t<DD, int32_t>(jobs, num_jobs, blocks_per_job, stream)));
+    if (wide) {
+        PMDD_DISPATCH_D(d, (launch_couple_round_t<DD, int64_t>(jobs, num_jobs, blocks_per_job, seed, stream)));
+    }
+    PMDD_DISPATCH_D(d, (launch_couple_round_t<DD, int32_t>(jobs, num_jobs, blocks_per_job, seed, stream)));
 }
 
 }  // namespace dev

@@ -18,7 +18,7 @@ enum CoupleCtr {
     kCtrResume = 2,     // first cutset node whose survivors did not fit (num_nodes: none)
     kCtrCursor = 3,     // next cutset node to hand out this round
     kCtrEvaluated = 4,  // products compared one by one (statistics)
-    kCtrDone = 5,       // 1 once a round finished every node
+    kCtrDone = 5,       // 1 once a product round finished every node
     kCtrValidEnd = 6,   // U slots below this index hold written points (set on overflow)
     kCtrProducts = 7,   // sum over cutset nodes of |TD_v| * |BU_v| (statistics)
     kCtrCount = 8
@@ -34,17 +34,33 @@ struct CoupleJob {
     int32_t num_nodes;
     int32_t pad0;
     void *U;            // running frontier followed by this round's survivors
-    int64_t ucap;       // points U can hold
-    uint8_t *keep;      // ucap flags
+    void *U_alt;        // receives the next running frontier (the buffers swap each round)
+    int64_t ucap;       // points each of U / U_alt can hold
+    void *sc_pts2;      // filter scratch: ucap points
+    void *sc_surv;      // filter scratch: ucap points
+    int32_t *sc_idx;    // filter scratch: ucap ints
+    int32_t *sc_sidx;   // filter scratch: ucap ints
     int64_t *ctr;       // kCtrCount counters
 };
+
+// Bytes of device memory a coupling job with capacity ucap needs besides the counters.
+inline size_t couple_bytes(int64_t ucap, int d, size_t elem) {
+    const size_t pts = (static_cast<size_t>(ucap) * d * elem + 255) / 256 * 256;
+    const size_t idx = (static_cast<size_t>(ucap) * 4 + 255) / 256 * 256;
+    return 4 * pts + 2 * idx;
+}
 
 cudaError_t launch_build_out_csr(const int32_t *in_off, const int32_t *arc_src, const int32_t *arc_w,
                                  int32_t num_nodes, int32_t num_arcs, int32_t *out_off, int32_t *cursor,
                                  int32_t *out_head, int32_t *out_w, cudaStream_t stream);
 
+// One coupling round for `num_jobs` jobs of one (d, wide) group.  A seed round appends,
+// per cutset node, the sums of the two frontiers' per-objective and sum maximisers and
+// filters them into the first running frontier; a product round streams the remaining
+// products against the running frontier and re-filters frontier + survivors.  Either
+// way the next running frontier lands in U_alt.
 cudaError_t launch_couple_round(int d, bool wide, const CoupleJob *jobs, int num_jobs, int blocks_per_job,
-                                cudaStream_t stream);
+                                bool seed, cudaStream_t stream);
 // Once per job at the start of coupling: kCtrProducts = sum of |TD_v| * |BU_v|.
 cudaError_t launch_couple_products(const CoupleJob *jobs, int num_jobs, cudaStream_t stream);
 

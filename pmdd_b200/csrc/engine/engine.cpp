@@ -17,6 +17,7 @@
 #include <algorithm>
 #include <atomic>
 #include <climits>
+#include <tuple>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -284,12 +285,11 @@ void Engine::release_instance(Instance &I) {
     release_side(I.td);
     release_side(I.bu);
     if (!I.external_dd) arena_.release(I.dd);
-    arena_.release(I.cu_U);
-    arena_.release(I.cu_keep);
+    arena_.release(I.cu_mem);
     arena_.release(I.cu_ctr);
     I.dd = nullptr;
-    I.cu_U = nullptr;
-    I.cu_keep = nullptr;
+    I.cu_mem = I.cu_U = I.cu_U_alt = I.cu_p2 = I.cu_sv = nullptr;
+    I.cu_i2 = I.cu_si = nullptr;
     I.cu_ctr = nullptr;
     I.blob.clear();
     I.blob.shrink_to_fit();
@@ -318,6 +318,28 @@ bool Engine::cancel(uint64_t id) {
         }
     }
     return false;
+}
+
+bool Engine::carve_couple(Instance &I, int64_t ucap) {
+    void *mem = arena_.alloc(dev::couple_bytes(ucap, I.d, I.elem()));
+    if (!mem) return false;
+    const size_t pts = align256(static_cast<size_t>(ucap) * I.d * I.elem());
+    const size_t idx = align256(static_cast<size_t>(ucap) * sizeof(int32_t));
+    char *m = static_cast<char *>(mem);
+    void *old_U = I.cu_U, *old_mem = I.cu_mem;
+    I.cu_mem = mem;
+    I.cu_U = m;
+    I.cu_U_alt = m + pts;
+    I.cu_p2 = m + 2 * pts;
+    I.cu_sv = m + 3 * pts;
+    I.cu_i2 = reinterpret_cast<int32_t *>(m + 4 * pts);
+    I.cu_si = reinterpret_cast<int32_t *>(m + 4 * pts + idx);
+    if (old_U && I.result_n > 0)  // carry the running frontier over (growth)
+        cudaMemcpyAsync(I.cu_U, old_U, static_cast<size_t>(I.result_n) * I.d * I.elem(), cudaMemcpyDeviceToDevice,
+                        stream_);
+    arena_.release(old_mem);  // stream-ordered: the copy above runs first
+    I.cu_ucap = ucap;
+    return true;
 }
 
 bool Engine::upload_dd(Instance &I) {
@@ -738,13 +760,10 @@ int Engine::step() {
         I->phase = Instance::COUPLING;
         I->stats.layer_coupling = I->td.layer;
         I->stats.cutset_size = I->nodes_in(I->td.layer);
-        // running frontier + one round of survivors
-        const int64_t ucap = std::max<int64_t>(std::max<int64_t>(I->opts.max_prod, 1 << 16), 1 << 18);
-        I->cu_ucap = ucap;
-        I->cu_U = arena_.alloc(static_cast<size_t>(ucap) * I->d * I->elem());
-        I->cu_keep = static_cast<uint8_t *>(arena_.alloc(static_cast<size_t>(ucap)));
+        // running frontier + one round of survivors; the seed round needs d+1 per node
+        const int64_t ucap = std::max<int64_t>(1 << 17, static_cast<int64_t>(I->stats.cutset_size) * (I->d + 1) + 4096);
         I->cu_ctr = static_cast<int64_t *>(arena_.alloc(sizeof(int64_t) * dev::kCtrCount));
-        if (!I->cu_U || !I->cu_keep || !I->cu_ctr) {
+        if (!I->cu_ctr || !carve_couple(*I, ucap)) {
             fail(*I, PMDD_ERR_OOM, "device memory budget exhausted at the cutset join");
             continue;
         }
@@ -765,9 +784,15 @@ int Engine::step() {
         J.bu_size = I->bu.size;
         J.num_nodes = I->nodes_in(I->td.layer);
         J.U = I->cu_U;
+        J.U_alt = I->cu_U_alt;
         J.ucap = I->cu_ucap;
-        J.keep = I->cu_keep;
+        J.sc_pts2 = I->cu_p2;
+        J.sc_surv = I->cu_sv;
+        J.sc_idx = I->cu_i2;
+        J.sc_sidx = I->cu_si;
         J.ctr = I->cu_ctr;
+        // the next running frontier lands in U_alt: swap now (host view)
+        std::swap(I->cu_U, I->cu_U_alt);
         const bool is_new = std::find(entering.begin(), entering.end(), I) != entering.end();
         int64_t *ci = reinterpret_cast<int64_t *>(hs + off_ctrinit) + dev::kCtrCount * ujobs.size();
         std::memset(ci, 0, sizeof(int64_t) * dev::kCtrCount);
@@ -837,10 +862,11 @@ int Engine::step() {
             return -1;
         launches_ += 1;
     }
-    // coupling rounds, grouped by (d, wide)
+    // coupling rounds, grouped by (d, wide, seed round)
     {
-        std::map<std::pair<int, bool>, std::vector<size_t>> ug;
-        for (size_t k = 0; k < ujobs.size(); ++k) ug[{ujob_inst[k]->d, ujob_inst[k]->wide}].push_back(k);
+        std::map<std::tuple<int, bool, bool>, std::vector<size_t>> ug;
+        for (size_t k = 0; k < ujobs.size(); ++k)
+            ug[std::make_tuple(ujob_inst[k]->d, ujob_inst[k]->wide, ujob_inst[k]->couple_rounds == 0)].push_back(k);
         const dev::CoupleJob *du = reinterpret_cast<const dev::CoupleJob *>(d_stage + off_u);
         // new requests: product statistics once
         for (size_t k = 0; k < ujobs.size(); ++k) {
@@ -856,10 +882,11 @@ int Engine::step() {
                 while (j + 1 < g.second.size() && g.second[j + 1] == g.second[j] + 1) ++j;
                 const int n = static_cast<int>(j - i + 1);
                 const int per = std::max(1, (sms_ * 2) / n);
-                if (!cuda_ok(dev::launch_couple_round(g.first.first, g.first.second, du + g.second[i], n, per, stream_),
+                if (!cuda_ok(dev::launch_couple_round(std::get<0>(g.first), std::get<1>(g.first), du + g.second[i], n,
+                                                      per, std::get<2>(g.first), stream_),
                              "coupling round"))
                     return -1;
-                launches_ += 3;
+                launches_ += 2;
                 i = j + 1;
             }
         }
@@ -967,25 +994,15 @@ int Engine::step() {
             I.stats.work_frontier_peak_points = std::max<int64_t>(I.stats.work_frontier_peak_points, n);
             I.phase = Instance::DONE;
         } else if (c[dev::kCtrF] > I.cu_ucap / 2) {
-            // the running frontier crowds out the survivors of a round: grow U
-            const int64_t ncap = I.cu_ucap * 2;
-            void *nU = arena_.alloc(static_cast<size_t>(ncap) * I.d * I.elem());
-            uint8_t *nk = static_cast<uint8_t *>(arena_.alloc(static_cast<size_t>(ncap)));
-            if (!nU || !nk) {
-                arena_.release(nU);
-                arena_.release(nk);
+            // the running frontier crowds out the survivors of a round: grow the block
+            I.result_n = c[dev::kCtrF];
+            const bool grown = carve_couple(I, I.cu_ucap * 2);
+            I.result_n = 0;
+            if (!grown) {
                 fail(I, PMDD_ERR_OOM, "device memory budget exhausted growing the cutset frontier");
                 continue;
             }
-            cudaMemcpyAsync(nU, I.cu_U, static_cast<size_t>(c[dev::kCtrF]) * I.d * I.elem(), cudaMemcpyDeviceToDevice,
-                            stream_);
-            int64_t upd[2] = {ncap, 0};
-            (void)upd;
-            arena_.release(I.cu_U);
-            arena_.release(I.cu_keep);
-            I.cu_U = nU;
-            I.cu_keep = nk;
-            I.cu_ucap = ncap;
+            const int64_t ncap = I.cu_ucap;
             // ValidEnd must follow the capacity
             int64_t *hv = reinterpret_cast<int64_t *>(h_init_.p) + 24;  // scratch slot in the init block
             *hv = ncap;

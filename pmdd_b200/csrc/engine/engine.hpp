@@ -82,8 +82,11 @@ struct Instance {
     Side td, bu;
     Phase phase = QUEUED;
     // coupling state
-    void *cu_U = nullptr;
-    uint8_t *cu_keep = nullptr;
+    void *cu_mem = nullptr;             // one block: U | U_alt | filter scratch (couple_bytes)
+    void *cu_U = nullptr;               // current running frontier (+ this round's survivors)
+    void *cu_U_alt = nullptr;           // receives the next running frontier
+    void *cu_p2 = nullptr, *cu_sv = nullptr;
+    int32_t *cu_i2 = nullptr, *cu_si = nullptr;
     int64_t *cu_ctr = nullptr;
     int64_t cu_ucap = 0;
     int couple_rounds = 0;
@@ -156,6 +159,9 @@ class Engine {
         ~Pinned();
     };
     bool admit(Instance &I);
+    // (Re)allocates the coupling block for capacity ucap and points U, U_alt and the
+    // filter scratch into it; false if it does not fit (old block kept).
+    bool carve_couple(Instance &I, int64_t ucap);
     void fail(Instance &I, int status, const std::string &msg);
     void release_instance(Instance &I);
     void release_side(Side &s);
