@@ -321,7 +321,7 @@ def main():
     k_big = 0.0
     k_total = 0.0
     launches = 0
-    cand = surv = 0
+    cand = surv = tile_launches = all_cand = 0
     stats_last = {}
     with ClockSampler(device) as clk:
         for _ in range(args.steps):
@@ -334,8 +334,10 @@ def main():
             k_big += st["kernel_dominance_s"]
             k_total += st["kernel_total_s"]
             launches += st["gpu_launches"]
-            cand += st["work_candidates_total"]
-            surv += st["work_frontier_survivors_total"]
+            cand += st["work_tile_candidates_total"]
+            surv += st["work_tile_survivors_total"]
+            tile_launches += st["tile_launches"]
+            all_cand += st["work_candidates_total"]
             stats_last = st
     barrier()
     clocks = clk.summary()
@@ -345,22 +347,26 @@ def main():
     ms_per_step = 1e3 * t_max / args.steps
     res.close()
 
-    # roofline of the fused expand+filter kernel: algorithmic bytes = candidates read
-    # (parent points) + survivors written, D int32 each
+    # roofline of the fused expand+filter tile kernel: algorithmic bytes of a launch =
+    # (candidates it filters, read as parent points + survivors it writes) x d x 4 B;
+    # achieved = those bytes / its CUDA-event time (sums over the K timed steps, i.e.
+    # per-launch bytes over the average launch duration)
     peak, peak_kind = read_peaks()
     alg_bytes = (cand + surv) * 3 * 4
     achieved = alg_bytes / k_expand / 1e9 if k_expand > 0 else 0.0
+    alg_per_launch = alg_bytes / max(1, tile_launches)
     traffic = None
+    issue = None
     tpath = os.path.join(ROOT, "profiles", "expand_tile_kernel_stream_traffic.json")
     if os.path.exists(tpath):
         try:
             tj = json.load(open(tpath))
-            traffic = tj.get("dram_bytes_per_algorithmic_byte")
-            if traffic is not None:
-                traffic = traffic * alg_bytes / max(1, stats_last.get("layers_td", 0) or 1)
+            ratio = tj.get("dram_bytes_per_algorithmic_byte")
+            if ratio is not None:
+                traffic = ratio * alg_per_launch
+            issue = tj.get("issue")
         except Exception:
             traffic = None
-    tile_launches_per_step = None
 
     # ---------------------------------------------------------------- e2e
     barrier()
@@ -391,8 +397,12 @@ def main():
                      "frac": achieved / peak if peak else None, "traffic": traffic,
                      "kernel": "expand_tile_kernel<3,int32> (fused expand + dominance filter)",
                      "peak_kind": peak_kind,
-                     "algorithmic_bytes_per_step": int(alg_bytes / max(1, args.steps)),
-                     "kernel_s_per_step": k_expand / max(1, args.steps)},
+                     "launches": int(tile_launches),
+                     "algorithmic_bytes_per_launch": int(alg_per_launch),
+                     "avg_launch_s": k_expand / max(1, tile_launches),
+                     "tile_candidates_per_step": int(cand / max(1, args.steps)),
+                     "all_candidates_per_step": int(all_cand / max(1, args.steps)),
+                     "issue": issue},
         "step_breakdown_s": {"device": t_max / args.steps, "tiles": k_expand / args.steps,
                              "oversized": k_big / args.steps, "kernels_total": k_total / args.steps},
     }
@@ -423,11 +433,17 @@ def main():
         flush.zero_()
         torch.cuda.synchronize()
         r1.enumerate(method=1, stats=st1, keep=False)
-        b1 = (st1["work_candidates_total"] + st1["work_frontier_survivors_total"]) * 3 * 4
+        # tile kernel alone, and the whole filter (tiles + oversized-destination path)
+        b1 = (st1["work_tile_candidates_total"] + st1["work_tile_survivors_total"]) * 3 * 4
         a1 = b1 / st1["kernel_expand_td_s"] / 1e9
+        bf = (st1["work_candidates_total"] + st1["work_frontier_survivors_total"]) * 3 * 4
+        tf = st1["kernel_expand_td_s"] + st1["kernel_dominance_s"]
+        af = bf / tf / 1e9
         line["config1_filter"] = {"instances": n1, "solves_per_s": n1 / st1["device_elapsed_s"],
                                   "achieved_gbs": a1, "frac_of_peak": a1 / peak,
-                                  "kernel_s": st1["kernel_expand_td_s"], "algorithmic_bytes": int(b1)}
+                                  "kernel_s": st1["kernel_expand_td_s"], "algorithmic_bytes": int(b1),
+                                  "filter_achieved_gbs": af, "filter_frac_of_peak": af / peak,
+                                  "filter_kernel_s": tf, "filter_algorithmic_bytes": int(bf)}
         r1.close()
         # reference CPU baseline on the box's cores
         if world == 1:

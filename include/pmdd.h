@@ -123,6 +123,9 @@ typedef struct pmdd_stats {
     int32_t cutset_size;
     int64_t gpu_launches;   /* kernels this call launched */
     double device_elapsed_s;  /* CUDA-event time on the engine stream, first to last op of the call */
+    int64_t work_tile_candidates_total;  /* candidates filtered in shared-memory tiles */
+    int64_t work_tile_survivors_total;   /* survivors the tile kernel wrote */
+    int64_t tile_launches;               /* expand+filter tile kernels this call launched */
 } pmdd_stats;
 
 /* ------------------------------------------------------------ one-shot entry

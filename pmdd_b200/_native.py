@@ -79,6 +79,9 @@ class PmddStats(ctypes.Structure):
         ("cutset_size", c_i32),
         ("gpu_launches", c_i64),
         ("device_elapsed_s", ctypes.c_double),
+        ("work_tile_candidates_total", c_i64),
+        ("work_tile_survivors_total", c_i64),
+        ("tile_launches", c_i64),
     ]
 
     def as_dict(self) -> dict:

@@ -379,6 +379,8 @@ int main(int argc, char **argv) {
         return 1;
     }
     const int nobjs = nobjs_from_name(argv[0]);
+    // one instance per process: let the engine use most of the free device memory
+    setenv("PMDD_ARENA_FRACTION", "0.85", 0);
     typedef std::chrono::steady_clock Clock;
     RunTimes rt;
     // compile: read + DD construction (for TSP the reference times construction only)

@@ -21,7 +21,8 @@ void write_err(char *err, size_t errlen, const std::string &msg) {
 
 // One engine per device for the one-shot, batch and resident entries, created on
 // first use and kept for the life of the process (its arena is sized by
-// PMDD_ARENA_BYTES, default a quarter of the device's free memory).  `generation`
+// PMDD_ARENA_BYTES, else PMDD_ARENA_FRACTION of the device's free memory, default a
+// quarter).  `generation`
 // changes whenever the engine is rebuilt after a CUDA failure, which invalidates
 // resident DD sets made on the old one.
 struct DeviceSlot {
@@ -45,9 +46,15 @@ int64_t default_arena_bytes(int device) {
         const long long v = std::atoll(env);
         if (v > 0) return v;
     }
+    double frac = 0.25;
+    const char *fenv = std::getenv("PMDD_ARENA_FRACTION");
+    if (fenv && *fenv) {
+        const double f = std::atof(fenv);
+        if (f > 0.0 && f <= 0.95) frac = f;
+    }
     size_t free_b = 0, total_b = 0;
     if (cudaSetDevice(device) != cudaSuccess || cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return 0;
-    return static_cast<int64_t>(free_b / 4);
+    return static_cast<int64_t>(static_cast<double>(free_b) * frac);
 }
 
 // Caller holds slot.mu.
@@ -86,6 +93,7 @@ struct RunInfo {
     double device_elapsed_s = 0;
     int64_t launches = 0;
     double t_expand = 0, t_big = 0, t_rest = 0;  // kernel time of this call on the engine stream
+    int64_t tile_launches = 0;
 };
 
 // Runs prepared requests to completion on the device's shared engine.  Caller holds
@@ -133,6 +141,7 @@ int run_locked(DeviceSlot &slot, std::vector<std::unique_ptr<pmdd::Instance>> &r
             info->t_expand = k1.expand - k0.expand;
             info->t_big = k1.big - k0.big;
             info->t_rest = k1.rest - k0.rest;
+            info->tile_launches = k1.tile_launches - k0.tile_launches;
         }
     }
     cudaEventDestroy(e0);
@@ -146,11 +155,60 @@ int run_locked(DeviceSlot &slot, std::vector<std::unique_ptr<pmdd::Instance>> &r
     return rc;
 }
 
-int run_on_device(int device, std::vector<std::unique_ptr<pmdd::Instance>> &reqs, RunInfo *info, std::string *err) {
+// Validates every DD and lays it out, on the host threads; nothing is packed yet.
+int prepare_all(const pmdd_dd *dds, int32_t count, const pmdd_options &o, bool with_out_csr,
+                std::vector<std::unique_ptr<pmdd::Instance>> &reqs, int32_t *status, std::string *err) {
+    reqs.resize(count);
+    std::vector<int> rcs(count, PMDD_OK);
+    std::vector<std::string> msgs(count);
+    pmdd::parallel_for(count, pmdd::host_threads(), [&](int64_t i) {
+        reqs[i].reset(new pmdd::Instance);
+        rcs[i] = pmdd::prepare_instance(dds[i], o, static_cast<uint64_t>(i), reqs[i].get(), &msgs[i], with_out_csr,
+                                        false);
+    });
+    for (int32_t i = 0; i < count; ++i) {
+        if (rcs[i] != PMDD_OK) {
+            *err = count > 1 ? "instance " + std::to_string(i) + ": " + msgs[i] : msgs[i];
+            if (status) status[i] = rcs[i];
+            return rcs[i];
+        }
+    }
+    return PMDD_OK;
+}
+
+// Largest pinned staging the engine keeps for DD uploads; bigger sets are packed into
+// per-instance pageable buffers instead.
+constexpr size_t kMaxStagingBytes = size_t(4) << 30;
+
+// Packs the prepared DDs, on the host threads, into the engine's pinned staging (one
+// 256-byte aligned region per instance) so that each upload is one asynchronous DMA, or
+// into per-instance host buffers when the staging cannot be had.  The caller holds
+// slot.mu until the uploads have completed.
+void pack_all(pmdd::Engine &E, const pmdd_dd *dds, std::vector<std::unique_ptr<pmdd::Instance>> &reqs) {
+    const size_t n = reqs.size();
+    std::vector<size_t> off(n + 1, 0);
+    for (size_t i = 0; i < n; ++i) off[i + 1] = off[i] + ((reqs[i]->blob_bytes + 255) & ~static_cast<size_t>(255));
+    unsigned char *st = off[n] > 0 && off[n] <= kMaxStagingBytes ? E.staging(off[n]) : nullptr;
+    pmdd::parallel_for(static_cast<int64_t>(n), pmdd::host_threads(), [&](int64_t i) {
+        pmdd::Instance &I = *reqs[i];
+        if (st) {
+            pmdd::pack_instance(dds[i], I, st + off[i]);
+            I.blob_src = st + off[i];
+        } else {
+            I.blob.assign(I.blob_bytes, 0);
+            pmdd::pack_instance(dds[i], I, I.blob.data());
+        }
+    });
+}
+
+// Packs (when `dds` is given) and runs prepared requests on the device's shared engine.
+int run_on_device(int device, std::vector<std::unique_ptr<pmdd::Instance>> &reqs, RunInfo *info, std::string *err,
+                  const pmdd_dd *dds = nullptr) {
     DeviceSlot &slot = slot_for(device);
     std::lock_guard<std::mutex> lk(slot.mu);
     const int rc = ensure_engine(device, slot, err);
     if (rc != PMDD_OK) return rc;
+    if (dds) pack_all(*slot.engine, dds, reqs);
     return run_locked(slot, reqs, info, err);
 }
 
@@ -163,6 +221,7 @@ int collect_batch(std::vector<std::unique_ptr<pmdd::Instance>> &reqs, pmdd_front
         stats->kernel_expand_td_s = info.t_expand;
         stats->kernel_dominance_s = info.t_big;
         stats->kernel_total_s = info.t_expand + info.t_big + info.t_rest;
+        stats->tile_launches = info.tile_launches;
     }
     int first_bad = PMDD_OK;
     for (int32_t i = 0; i < count; ++i) {
@@ -179,6 +238,9 @@ int collect_batch(std::vector<std::unique_ptr<pmdd::Instance>> &reqs, pmdd_front
             stats->work_frontier_survivors_total += st.work_frontier_survivors_total;
             stats->work_frontier_peak_points = std::max(stats->work_frontier_peak_points, st.work_frontier_peak_points);
             stats->work_join_products_total += st.work_join_products_total;
+            stats->dominance_filtered_total += st.dominance_filtered_total;
+            stats->work_tile_candidates_total += st.work_tile_candidates_total;
+            stats->work_tile_survivors_total += st.work_tile_survivors_total;
             stats->gpu_mem_peak_used_bytes = std::max(stats->gpu_mem_peak_used_bytes, st.gpu_mem_peak_used_bytes);
             stats->gpu_mem_peak_reserved_bytes = st.gpu_mem_peak_reserved_bytes;
         }
@@ -220,17 +282,16 @@ int pmdd_enumerate(const pmdd_dd *dd, const pmdd_options *opts, pmdd_frontier *o
     pmdd_options o;
     if (opts) o = *opts;
     else pmdd_options_default(&o);
-    std::vector<std::unique_ptr<pmdd::Instance>> reqs(1);
-    reqs[0].reset(new pmdd::Instance);
+    std::vector<std::unique_ptr<pmdd::Instance>> reqs;
     std::string msg;
     const double t0 = pmdd::now_s();
-    int rc = pmdd::prepare_instance(*dd, o, 0, reqs[0].get(), &msg);
+    int rc = prepare_all(dd, 1, o, false, reqs, nullptr, &msg);
     if (rc != PMDD_OK) {
         write_err(err, errlen, msg);
         return rc;
     }
     RunInfo info;
-    rc = run_on_device(o.device, reqs, &info, &msg);
+    rc = run_on_device(o.device, reqs, &info, &msg, dd);
     if (rc != PMDD_OK) {
         write_err(err, errlen, msg);
         return rc;
@@ -239,6 +300,7 @@ int pmdd_enumerate(const pmdd_dd *dd, const pmdd_options *opts, pmdd_frontier *o
     I.stats.wall_pack_transfer_s = I.admit_s - t0;
     I.stats.device_elapsed_s = info.device_elapsed_s;
     I.stats.gpu_launches = info.launches;
+    I.stats.tile_launches = info.tile_launches;
     rc = export_result(I, out, stats);
     if (rc != PMDD_OK) write_err(err, errlen, I.error);
     return rc;
@@ -254,20 +316,17 @@ int pmdd_enumerate_batch(const pmdd_dd *dds, int32_t count, const pmdd_options *
     pmdd_options o;
     if (opts) o = *opts;
     else pmdd_options_default(&o);
-    std::vector<std::unique_ptr<pmdd::Instance>> reqs(count);
+    if (outs)
+        for (int32_t i = 0; i < count; ++i) std::memset(&outs[i], 0, sizeof(outs[i]));
+    std::vector<std::unique_ptr<pmdd::Instance>> reqs;
     std::string msg;
-    for (int32_t i = 0; i < count; ++i) {
-        if (outs) std::memset(&outs[i], 0, sizeof(outs[i]));
-        reqs[i].reset(new pmdd::Instance);
-        const int rc = pmdd::prepare_instance(dds[i], o, static_cast<uint64_t>(i), reqs[i].get(), &msg);
-        if (rc != PMDD_OK) {
-            write_err(err, errlen, "instance " + std::to_string(i) + ": " + msg);
-            if (status) status[i] = rc;
-            return rc;
-        }
+    int rc = prepare_all(dds, count, o, false, reqs, status, &msg);
+    if (rc != PMDD_OK) {
+        write_err(err, errlen, count > 1 ? msg : "instance 0: " + msg);
+        return rc;
     }
     RunInfo info;
-    int rc = run_on_device(o.device, reqs, &info, &msg);
+    rc = run_on_device(o.device, reqs, &info, &msg, dds);
     if (rc != PMDD_OK) {
         write_err(err, errlen, msg);
         return rc;
@@ -344,13 +403,9 @@ pmdd_resident *pmdd_resident_upload(const pmdd_dd *dds, int32_t count, int32_t d
     pmdd_options o;
     pmdd_options_default(&o);
     std::string msg;
-    for (int32_t i = 0; i < count; ++i) {
-        std::unique_ptr<pmdd::Instance> I(new pmdd::Instance);
-        if (pmdd::prepare_instance(dds[i], o, static_cast<uint64_t>(i), I.get(), &msg, true) != PMDD_OK) {
-            write_err(err, errlen, "instance " + std::to_string(i) + ": " + msg);
-            return nullptr;
-        }
-        R->tmpl.push_back(std::move(I));
+    if (prepare_all(dds, count, o, true, R->tmpl, nullptr, &msg) != PMDD_OK) {
+        write_err(err, errlen, count > 1 ? msg : "instance 0: " + msg);
+        return nullptr;
     }
     DeviceSlot &slot = slot_for(device);
     std::lock_guard<std::mutex> lk(slot.mu);
@@ -359,6 +414,7 @@ pmdd_resident *pmdd_resident_upload(const pmdd_dd *dds, int32_t count, int32_t d
         return nullptr;
     }
     R->generation = slot.generation;
+    pack_all(*slot.engine, dds, R->tmpl);
     for (size_t i = 0; i < R->tmpl.size(); ++i) {
         pmdd::Instance &I = *R->tmpl[i];
         if (!slot.engine->upload_dd(I)) {
@@ -376,6 +432,8 @@ pmdd_resident *pmdd_resident_upload(const pmdd_dd *dds, int32_t count, int32_t d
     for (auto &I : R->tmpl) {
         I->blob.clear();
         I->blob.shrink_to_fit();
+        I->blob_src = nullptr;
+        std::vector<int32_t>().swap(I->sd_order);
     }
     return R.release();
 }
@@ -427,6 +485,9 @@ int pmdd_resident_enumerate(pmdd_resident *R, const pmdd_options *opts, pmdd_fro
         I->d_arc_src = T.d_arc_src;
         I->d_arc_w = T.d_arc_w;
         I->d_weights = T.d_weights;
+        I->has_sd_order = T.has_sd_order;
+        I->off_sdord = T.off_sdord;
+        I->d_sd_order = T.d_sd_order;
         I->d_out_off = T.d_out_off;
         I->d_out_head = T.d_out_head;
         I->d_out_w = T.d_out_w;

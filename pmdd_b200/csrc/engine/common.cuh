@@ -64,6 +64,7 @@ struct ExpandJob {
     int32_t *big_idx;              // scratch: candidate index of each bucket-ordered point
     int32_t *big_surv_idx;         // scratch: candidate index of each overflowing survivor
     uint32_t *err;
+    unsigned long long *tile_surv; // survivors written by the tile kernel (added to)
 };
 
 // Bytes of oversized-destination scratch per candidate point.

@@ -21,6 +21,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <thread>
 
 namespace pmdd {
 
@@ -105,8 +106,47 @@ Engine::Pinned::~Pinned() {
 }
 
 // ------------------------------------------------------ request preparation
+int host_threads() {
+    int t = static_cast<int>(std::thread::hardware_concurrency());
+    if (t <= 0) t = 1;
+    t = std::min(t, 32);
+    const char *env = std::getenv("PMDD_HOST_THREADS");
+    if (env && *env && std::atoi(env) > 0) t = std::atoi(env);
+    return t;
+}
+
+void parallel_for(int64_t n, int threads, const std::function<void(int64_t)> &fn) {
+    threads = static_cast<int>(std::min<int64_t>(std::max(threads, 1), n));
+    if (threads <= 1) {
+        for (int64_t i = 0; i < n; ++i) fn(i);
+        return;
+    }
+    std::atomic<int64_t> next(0);
+    auto worker = [&]() {
+        for (int64_t i = next++; i < n; i = next++) fn(i);
+    };
+    std::vector<std::thread> pool;
+    pool.reserve(threads - 1);
+    for (int t = 1; t < threads; ++t) pool.emplace_back(worker);
+    worker();
+    for (auto &th : pool) th.join();
+}
+
+void pack_instance(const pmdd_dd &dd, const Instance &I, unsigned char *dst) {
+    const size_t N = static_cast<size_t>(I.N), A = static_cast<size_t>(I.A), K = static_cast<size_t>(I.K);
+    std::memcpy(dst + I.off_layer, dd.layer_offsets, sizeof(int32_t) * (I.L + 1));
+    std::memcpy(dst + I.off_in, dd.in_arc_offsets, sizeof(int32_t) * (N + 1));
+    if (A > 0) {
+        std::memcpy(dst + I.off_src, dd.arc_src, sizeof(int32_t) * A);
+        std::memcpy(dst + I.off_w, dd.arc_weight, sizeof(int32_t) * A);
+    }
+    std::memcpy(dst + I.off_weights, dd.weights, sizeof(int32_t) * K * I.d);
+    if (dd.min_weight) std::memcpy(dst + I.off_minw, dd.min_weight, sizeof(int32_t) * N);
+    if (I.has_sd_order) std::memcpy(dst + I.off_sdord, I.sd_order.data(), sizeof(int32_t) * N);
+}
+
 int prepare_instance(const pmdd_dd &dd, const pmdd_options &o, uint64_t id, Instance *I, std::string *err,
-                     bool with_out_csr) {
+                     bool with_out_csr, bool pack) {
     auto bad = [&](const std::string &m) {
         if (err) *err = m;
         return static_cast<int>(PMDD_ERR_INVALID);
@@ -129,19 +169,25 @@ int prepare_instance(const pmdd_dd &dd, const pmdd_options &o, uint64_t id, Inst
     for (int32_t v = 0; v < N; ++v)
         if (dd.in_arc_offsets[v + 1] < dd.in_arc_offsets[v]) return bad("in_arc_offsets must be non-decreasing");
     // every arc runs from the layer right above its head; bound on |path sums|
+    std::vector<int64_t> row_max(K, 0);
+    for (int32_t r = 0; r < K; ++r)
+        for (int k = 0; k < d; ++k)
+            row_max[r] = std::max<int64_t>(row_max[r], std::llabs(static_cast<int64_t>(dd.weights[static_cast<int64_t>(r) * d + k])));
     int64_t bound = 0;
     for (int l = 1; l < L; ++l) {
         int64_t layer_max = 0;
         const int32_t lo = dd.layer_offsets[l - 1], hi = dd.layer_offsets[l];
-        for (int32_t v = dd.layer_offsets[l]; v < dd.layer_offsets[l + 1]; ++v) {
-            for (int32_t a = dd.in_arc_offsets[v]; a < dd.in_arc_offsets[v + 1]; ++a) {
-                const int32_t s = dd.arc_src[a], w = dd.arc_weight[a];
-                if (s < lo || s >= hi) return bad("arc tail is not in the layer above its head");
-                if (w < 0 || w >= K) return bad("arc weight row out of range");
-                for (int k = 0; k < d; ++k)
-                    layer_max = std::max<int64_t>(layer_max, std::llabs(static_cast<int64_t>(dd.weights[static_cast<int64_t>(w) * d + k])));
-            }
+        const int32_t a0 = dd.in_arc_offsets[dd.layer_offsets[l]], a1 = dd.in_arc_offsets[dd.layer_offsets[l + 1]];
+        bool bad_src = false, bad_w = false;
+        for (int32_t a = a0; a < a1; ++a) {
+            const int32_t s = dd.arc_src[a], w = dd.arc_weight[a];
+            bad_src |= (s < lo) | (s >= hi);
+            const bool wb = (w < 0) | (w >= K);
+            bad_w |= wb;
+            if (!wb) layer_max = std::max<int64_t>(layer_max, row_max[w]);
         }
+        if (bad_src) return bad("arc tail is not in the layer above its head");
+        if (bad_w) return bad("arc weight row out of range");
         bound += layer_max;
     }
     I->id = id;
@@ -170,16 +216,25 @@ int prepare_instance(const pmdd_dd &dd, const pmdd_options &o, uint64_t id, Inst
     const bool has_minw = dd.min_weight != nullptr;
     I->off_minw = has_minw ? off : 0;
     if (has_minw) off = align256(off + sizeof(int32_t) * static_cast<size_t>(N));
-    I->blob_bytes = off;
-    I->blob.assign(off, 0);
-    std::memcpy(I->blob.data() + I->off_layer, dd.layer_offsets, sizeof(int32_t) * (L + 1));
-    std::memcpy(I->blob.data() + I->off_in, dd.in_arc_offsets, sizeof(int32_t) * (static_cast<size_t>(N) + 1));
-    if (A > 0) {
-        std::memcpy(I->blob.data() + I->off_src, dd.arc_src, sizeof(int32_t) * static_cast<size_t>(A));
-        std::memcpy(I->blob.data() + I->off_w, dd.arc_weight, sizeof(int32_t) * static_cast<size_t>(A));
+    I->has_sd_order = has_minw && (with_out_csr || (o.state_dominance > 0 && o.problem_type == 1 && o.method == 1));
+    I->off_sdord = 0;
+    if (I->has_sd_order) {
+        I->off_sdord = off;
+        off = align256(off + sizeof(int32_t) * static_cast<size_t>(N));
+        I->sd_order.resize(N);
+        for (int l = 0; l < L; ++l) {
+            const int32_t b = dd.layer_offsets[l], e = dd.layer_offsets[l + 1];
+            int32_t *ord = I->sd_order.data() + b;
+            for (int32_t i = 0; i < e - b; ++i) ord[i] = i;
+            const int32_t *mw = dd.min_weight + b;
+            std::stable_sort(ord, ord + (e - b), [mw](int32_t x, int32_t y) { return mw[x] > mw[y]; });
+        }
     }
-    std::memcpy(I->blob.data() + I->off_weights, dd.weights, sizeof(int32_t) * static_cast<size_t>(K) * d);
-    if (has_minw) std::memcpy(I->blob.data() + I->off_minw, dd.min_weight, sizeof(int32_t) * static_cast<size_t>(N));
+    I->blob_bytes = off;
+    if (pack) {
+        I->blob.assign(off, 0);
+        pack_instance(dd, *I, I->blob.data());
+    }
     size_t dev = off;
     I->with_out_csr = with_out_csr || o.method == 3;
     if (I->with_out_csr) {
@@ -293,6 +348,8 @@ void Engine::release_instance(Instance &I) {
     I.cu_ctr = nullptr;
     I.blob.clear();
     I.blob.shrink_to_fit();
+    I.blob_src = nullptr;
+    std::vector<int32_t>().swap(I.sd_order);
 }
 
 void Engine::fail(Instance &I, int status, const std::string &msg) {
@@ -345,12 +402,13 @@ bool Engine::carve_couple(Instance &I, int64_t ucap) {
 bool Engine::upload_dd(Instance &I) {
     I.dd = static_cast<unsigned char *>(arena_.alloc(I.dev_bytes));
     if (!I.dd) return false;
-    if (!cuda_ok(cudaMemcpyAsync(I.dd, I.blob.data(), I.blob_bytes, cudaMemcpyHostToDevice, stream_), "DD upload"))
+    if (!cuda_ok(cudaMemcpyAsync(I.dd, I.blob_src ? I.blob_src : I.blob.data(), I.blob_bytes, cudaMemcpyHostToDevice, stream_), "DD upload"))
         return false;
     I.d_in_off = reinterpret_cast<const int32_t *>(I.dd + I.off_in);
     I.d_arc_src = reinterpret_cast<const int32_t *>(I.dd + I.off_src);
     I.d_arc_w = reinterpret_cast<const int32_t *>(I.dd + I.off_w);
     I.d_weights = reinterpret_cast<const int32_t *>(I.dd + I.off_weights);
+    I.d_sd_order = I.has_sd_order ? reinterpret_cast<const int32_t *>(I.dd + I.off_sdord) : nullptr;
     if (I.with_out_csr) {
         size_t off = I.blob_bytes;
         I.d_out_off = reinterpret_cast<int32_t *>(I.dd + off);
@@ -408,6 +466,8 @@ bool Engine::admit(Instance &I) {
     }
     I.blob.clear();
     I.blob.shrink_to_fit();
+    I.blob_src = nullptr;
+    std::vector<int32_t>().swap(I.sd_order);
     I.phase = Instance::RUNNING;
     I.admit_s = now_s();
     return true;
@@ -510,6 +570,17 @@ int Engine::step() {
         exps.push_back(e);
     }
 
+    // survivors written by the tile kernel, one counter per expansion (statistics)
+    unsigned long long *d_tile_surv = nullptr;
+    if (!exps.empty()) {
+        d_tile_surv = static_cast<unsigned long long *>(scratch(sizeof(unsigned long long) * exps.size()));
+        if (!d_tile_surv) {
+            error_ = "engine bookkeeping allocation failed";
+            ok_ = false;
+            return -1;
+        }
+    }
+
     // group by (d, wide) and build descriptors
     std::map<std::pair<int, bool>, std::vector<size_t>> groups;
     for (size_t i = 0; i < exps.size(); ++i) groups[{exps[i].I->d, exps[i].I->wide}].push_back(i);
@@ -586,6 +657,7 @@ int Engine::step() {
                     J.big_surv_idx = reinterpret_cast<int32_t *>(m + 3 * pb + ib);
                 }
                 J.err = d_err_;
+                J.tile_surv = d_tile_surv + pos;
                 for (int b = 0; b < s.res.num_big; ++b) bigwork.push_back({static_cast<int32_t>(pos - gl.first), b});
                 if (s.res.num_big > 0) gl.max_big = std::max(gl.max_big, s.res.max_item);
                 ordered.push_back(e);
@@ -595,6 +667,69 @@ int Engine::step() {
             glaunch.push_back(gl);
         }
         exps.swap(ordered);
+    }
+
+    // knapsack state dominance on the layers that method-1 knapsack requests asking for it
+    // expand this step (jobs follow the expansion order, so (d, wide) groups stay contiguous)
+    struct SdGroup {
+        int d;
+        bool wide;
+        size_t first, count;
+        int64_t total;  // nodes over the group's jobs
+    };
+    std::vector<dev::StateDomJob> sdjobs;
+    std::vector<int64_t> sd_bases;
+    std::vector<Instance *> sd_inst;
+    std::vector<SdGroup> sdg;
+    int64_t *d_removed = nullptr;
+    {
+        std::vector<size_t> pick;
+        size_t keep_bytes = 0;
+        for (size_t i = 0; i < exps.size(); ++i) {
+            const ExpPlan &e = exps[i];
+            const Instance &I = *e.I;
+            if (e.td && I.opts.method == 1 && I.opts.problem_type == 1 && I.opts.state_dominance > 0 &&
+                I.d_sd_order != nullptr && I.nodes_in(e.nl) > 1) {
+                pick.push_back(i);
+                keep_bytes += align256(static_cast<size_t>(std::max<int64_t>(e.cand, 1)));
+            }
+        }
+        if (!pick.empty()) {
+            char *mem = static_cast<char *>(scratch(align256(sizeof(int64_t) * pick.size()) + keep_bytes));
+            if (!mem) {
+                error_ = "engine bookkeeping allocation failed";
+                ok_ = false;
+                return -1;
+            }
+            d_removed = reinterpret_cast<int64_t *>(mem);
+            char *keep = mem + align256(sizeof(int64_t) * pick.size());
+            for (size_t k = 0; k < pick.size(); ++k) {
+                const ExpPlan &e = exps[pick[k]];
+                Instance &I = *e.I;
+                dev::StateDomJob J;
+                std::memset(&J, 0, sizeof(J));
+                J.order = I.d_sd_order + I.layer_off[e.nl];
+                J.in_off = I.d_in_off;
+                J.arc_src = I.d_arc_src;
+                J.arc_w = I.d_arc_w;
+                J.pts = e.out_pts;
+                J.off = e.out_off;
+                J.size = e.out_size;
+                J.keep = reinterpret_cast<uint8_t *>(keep);
+                keep += align256(static_cast<size_t>(std::max<int64_t>(e.cand, 1)));
+                J.removed = d_removed + k;
+                J.node_base = I.layer_off[e.nl];
+                J.num_nodes = I.nodes_in(e.nl);
+                if (sdg.empty() || sdg.back().d != I.d || sdg.back().wide != I.wide)
+                    sdg.push_back({I.d, I.wide, k, 0, 0});
+                SdGroup &g = sdg.back();
+                sd_bases.push_back(g.total);
+                g.total += J.num_nodes;
+                g.count++;
+                sdjobs.push_back(J);
+                sd_inst.push_back(&I);
+            }
+        }
     }
 
     // count plans for sides that move this step
@@ -622,7 +757,9 @@ int Engine::step() {
     const size_t off_c = align256(off_b + sizeof(dev::BigWork) * bigwork.size());
     const size_t off_tb = align256(off_c + sizeof(dev::CountJob) * cjobs.size());
     const size_t off_ib = align256(off_tb + sizeof(int64_t) * tile_bases.size());
-    size_t off_k = align256(off_ib + sizeof(int64_t) * item_bases.size());
+    const size_t off_sd = align256(off_ib + sizeof(int64_t) * item_bases.size());
+    const size_t off_sdb = align256(off_sd + sizeof(dev::StateDomJob) * sdjobs.size());
+    size_t off_k = align256(off_sdb + sizeof(int64_t) * sd_bases.size());
     // coupling: requests at their cutset
     std::vector<Instance *> couplers;
     for (auto &p : active_)
@@ -729,6 +866,10 @@ int Engine::step() {
         std::memcpy(hs + off_tb, tile_bases.data(), sizeof(int64_t) * tile_bases.size());
         std::memcpy(hs + off_ib, item_bases.data(), sizeof(int64_t) * item_bases.size());
     }
+    if (!sdjobs.empty()) {
+        std::memcpy(hs + off_sd, sdjobs.data(), sizeof(dev::StateDomJob) * sdjobs.size());
+        std::memcpy(hs + off_sdb, sd_bases.data(), sizeof(int64_t) * sd_bases.size());
+    }
 
     // ------------------------------------------------- expansion bookkeeping
     // Sides move to their new layer now (host view); device work is stream-ordered.
@@ -810,7 +951,9 @@ int Engine::step() {
     const size_t s_counts = 0;
     const size_t s_ctr = align256(s_counts + sizeof(dev::CountResult) * counts.size());
     const size_t s_fin = align256(s_ctr + sizeof(int64_t) * dev::kCtrCount * ujobs.size());
-    const size_t s_err = align256(s_fin + sizeof(int32_t) * finishing.size());
+    const size_t s_sd = align256(s_fin + sizeof(int32_t) * finishing.size());
+    const size_t s_ts = align256(s_sd + sizeof(int64_t) * sdjobs.size());
+    const size_t s_err = align256(s_ts + sizeof(unsigned long long) * exps.size());
     const size_t s_total = s_err + sizeof(uint32_t);
     if ((stage_bytes && !d_stage) || !h_summary_.reserve(s_total)) {
         error_ = "engine bookkeeping allocation failed";
@@ -830,6 +973,7 @@ int Engine::step() {
         cudaMemcpyAsync(ujobs[k].ctr, d_stage + off_ctrinit + sizeof(int64_t) * dev::kCtrCount * k,
                         sizeof(int64_t) * dev::kCtrCount, cudaMemcpyDeviceToDevice, stream_);
     }
+    if (d_tile_surv) cudaMemsetAsync(d_tile_surv, 0, sizeof(unsigned long long) * exps.size(), stream_);
     cudaEventRecord(ev0, stream_);
     for (const GroupLaunch &gl : glaunch) {
         const dev::ExpandJob *dj = reinterpret_cast<const dev::ExpandJob *>(d_stage + off_x) + gl.first;
@@ -843,6 +987,7 @@ int Engine::step() {
                      "expand_tile_kernel"))
             return -1;
         launches_ += 2;
+        ktimes_.tile_launches += 1;
     }
     cudaEventRecord(ev1, stream_);
     for (const GroupLaunch &gl : glaunch) {
@@ -853,6 +998,18 @@ int Engine::step() {
                      "oversized-destination kernels"))
             return -1;
         launches_ += 3;
+    }
+    if (!sdjobs.empty()) {
+        cudaMemsetAsync(d_removed, 0, sizeof(int64_t) * sdjobs.size(), stream_);
+        for (const SdGroup &g : sdg) {
+            const dev::StateDomJob *dj = reinterpret_cast<const dev::StateDomJob *>(d_stage + off_sd) + g.first;
+            const int64_t *db = reinterpret_cast<const int64_t *>(d_stage + off_sdb) + g.first;
+            if (!cuda_ok(dev::launch_state_dominance(g.d, g.wide, dj, db, static_cast<int>(g.count), g.total, sms_,
+                                                     stream_),
+                         "state dominance"))
+                return -1;
+            launches_ += 2;
+        }
     }
     cudaEventRecord(ev2, stream_);
     if (!cjobs.empty()) {
@@ -902,6 +1059,11 @@ int Engine::step() {
     for (size_t k = 0; k < finishing.size(); ++k)
         cudaMemcpyAsync(hsum + s_fin + sizeof(int32_t) * k, finishing[k]->td.size, sizeof(int32_t),
                         cudaMemcpyDeviceToHost, stream_);
+    if (!sdjobs.empty())
+        cudaMemcpyAsync(hsum + s_sd, d_removed, sizeof(int64_t) * sdjobs.size(), cudaMemcpyDeviceToHost, stream_);
+    if (d_tile_surv)
+        cudaMemcpyAsync(hsum + s_ts, d_tile_surv, sizeof(unsigned long long) * exps.size(), cudaMemcpyDeviceToHost,
+                        stream_);
     cudaMemcpyAsync(hsum + s_err, d_err_, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream_);
     for (void *q : to_release) arena_.release(q);
     const cudaError_t se = cudaStreamSynchronize(stream_);
@@ -926,12 +1088,15 @@ int Engine::step() {
             max_item = std::max(max_item, e.max_item);
             nbig += e.num_big;
         }
+        unsigned long long tile_surv = 0;
+        for (size_t k = 0; k < exps.size(); ++k)
+            tile_surv += reinterpret_cast<const unsigned long long *>(static_cast<char *>(h_summary_.p) + s_ts)[k];
         std::fprintf(stderr,
                      "[pmdd step] jobs=%zu counts=%zu couple=%zu cand=%lld big_items=%lld big_cand=%lld max_item=%lld "
-                     "tiles_ms=%.3f big_ms=%.3f rest_ms=%.3f\n",
+                     "tile_cand=%lld tile_surv=%llu tiles_ms=%.3f big_ms=%.3f rest_ms=%.3f\n",
                      exps.size(), counts.size(), ujobs.size(), static_cast<long long>(cand),
                      static_cast<long long>(nbig), static_cast<long long>(big_cand), static_cast<long long>(max_item),
-                     ms_expand, ms_big, ms_rest);
+                     static_cast<long long>(cand - big_cand), tile_surv, ms_expand, ms_big, ms_rest);
     }
     cudaEventDestroy(ev0);
     cudaEventDestroy(ev1);
@@ -947,11 +1112,17 @@ int Engine::step() {
         for (auto &p : active_)
             if (p->phase != Instance::DONE) fail(*p, PMDD_ERR_INTERNAL, "device-side index check failed");
     }
-    for (const ExpPlan &e : exps) {
+    for (size_t k = 0; k < exps.size(); ++k) {
+        const ExpPlan &e = exps[k];
         e.I->stats.kernel_expand_td_s += ms_expand * 1e-3;
         e.I->stats.kernel_dominance_s += ms_big * 1e-3;
         e.I->stats.kernel_total_s += (ms_expand + ms_big + ms_rest) * 1e-3;
+        e.I->stats.work_tile_candidates_total += e.cand - e.big_total;
+        e.I->stats.work_tile_survivors_total +=
+            static_cast<int64_t>(reinterpret_cast<const unsigned long long *>(hsum + s_ts)[k]);
     }
+    for (size_t k = 0; k < sdjobs.size(); ++k)
+        sd_inst[k]->stats.dominance_filtered_total += reinterpret_cast<const int64_t *>(hsum + s_sd)[k];
     const dev::CountResult *hres = reinterpret_cast<const dev::CountResult *>(hsum + s_counts);
     for (size_t k = 0; k < counts.size(); ++k) {
         Instance &I = *counts[k].I;

@@ -9,6 +9,7 @@
 #include <chrono>
 #include <cstdint>
 #include <deque>
+#include <functional>
 #include <map>
 #include <memory>
 #include <string>
@@ -17,6 +18,7 @@
 
 #include "common.cuh"
 #include "couple.cuh"
+#include "statedom.cuh"
 #include "kernels.cuh"
 #include "pmdd.h"
 
@@ -73,7 +75,14 @@ struct Instance {
     std::vector<int32_t> layer_off;     // L+1
     std::vector<int32_t> arc_at_layer;  // L+1: in-arcs of layers < l
     std::vector<unsigned char> blob;    // packed DD arrays, uploaded at admission
+    const unsigned char *blob_src = nullptr;  // packed arrays in the engine's pinned staging (instead of blob)
     size_t off_layer = 0, off_in = 0, off_src = 0, off_w = 0, off_weights = 0, off_minw = 0, blob_bytes = 0;
+    // knapsack state dominance: per layer, the layer-local node ids by min_weight
+    // descending (ties by id); packed into the blob at off_sdord when present
+    std::vector<int32_t> sd_order;
+    size_t off_sdord = 0;
+    bool has_sd_order = false;
+    const int32_t *d_sd_order = nullptr;
     size_t dev_bytes = 0;               // blob + out-arc CSR
     // device DD
     unsigned char *dd = nullptr;
@@ -105,16 +114,30 @@ struct Instance {
     int32_t nodes_in(int l) const { return layer_off[l + 1] - layer_off[l]; }
 };
 
-// Validates a flat DD and packs it into an Instance (host side only).  The device copy
-// gets the bottom-up CSR when the method needs it or `with_out_csr` asks for it.
+// Validates a flat DD and lays it out in an Instance (host side only).  The device copy
+// gets the bottom-up CSR when the method needs it or `with_out_csr` asks for it, and the
+// state-dominance node order when the DD has min_weight and either the options ask for
+// knapsack state dominance (method 1, problem type 1) or `with_out_csr` is set (resident
+// sets, which serve any options).  With
+// `pack` the arrays are also copied into inst->blob; without it the caller packs them
+// later with pack_instance (e.g. straight into pinned staging memory).
 int prepare_instance(const pmdd_dd &dd, const pmdd_options &opts, uint64_t id, Instance *inst, std::string *err,
-                     bool with_out_csr = false);
+                     bool with_out_csr = false, bool pack = true);
+// Writes the DD arrays of a prepared instance into dst (inst.blob_bytes bytes, laid out
+// at the instance's offsets; the alignment gaps are left as they are).
+void pack_instance(const pmdd_dd &dd, const Instance &inst, unsigned char *dst);
+
+// Runs fn(i) for i in [0, n) on up to `threads` host threads (PMDD_HOST_THREADS caps
+// the default, which is the hardware concurrency, at most 32).
+void parallel_for(int64_t n, int threads, const std::function<void(int64_t)> &fn);
+int host_threads();
 
 // Accumulated kernel time of an engine (seconds, CUDA events on its stream): the fused
 // expand+filter tiles, the oversized-destination path, and everything else (counting,
 // coupling, DD preparation).
 struct KernelTimes {
     double expand = 0, big = 0, rest = 0;
+    int64_t tile_launches = 0;
 };
 
 class Engine {
@@ -143,6 +166,12 @@ class Engine {
     // the arena until release_dd(); requests then share it via external_dd.
     bool upload_dd(Instance &I);
     void release_dd(Instance &I);
+    // Pinned host memory for packing DD uploads (grow-only, kept across calls); nullptr
+    // when it cannot be had.  Contents must stay untouched until the uploads that read
+    // them have completed on the stream.
+    unsigned char *staging(size_t bytes) {
+        return h_stage_.reserve(bytes) ? static_cast<unsigned char *>(h_stage_.p) : nullptr;
+    }
     // Raw arena memory for standalone operations run on this engine's stream.
     void *alloc(size_t bytes) { return arena_.alloc(bytes); }
     void release(void *p) { arena_.release(p); }
@@ -179,7 +208,7 @@ class Engine {
     std::vector<std::unique_ptr<Instance>> active_;
     std::deque<std::unique_ptr<Instance>> finished_;
     std::vector<void *> step_scratch_;
-    Pinned h_desc_, h_summary_, h_init_;
+    Pinned h_desc_, h_summary_, h_init_, h_stage_;
     uint32_t *d_err_ = nullptr;
     int64_t launches_ = 0;
     KernelTimes ktimes_;

@@ -52,6 +52,12 @@ __device__ __forceinline__ int warp_max_i(int x) {
     return x;
 }
 
+__device__ __forceinline__ int64_t warp_min_i64(int64_t x) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x = min(x, static_cast<int64_t>(__shfl_xor_sync(0xffffffffu, x, o)));
+    return x;
+}
+
 // A point padded to a 16-byte multiple so that a warp reads one candidate from shared
 // memory with vector loads that broadcast to all lanes.
 template <int D, typename T>

@@ -96,6 +96,16 @@ def record(name, path, problem_type, nobjs, methods):
         out["structure"] = {k: st[k] for k in ("original_width", "reduced_width", "original_num_nodes",
                                               "reduced_num_nodes", "max_num_nodes_per_layer", "max_num_in_arcs",
                                               "total_num_in_arcs")}
+    if problem_type == 1 and 1 in methods:
+        # knapsack state dominance (method 1, state_dominance 1): same frontier, fewer labels
+        r = oracle.run_ref(path, problem_type, 1, nobjs, threads=1, state_dominance=1)
+        s = r["stats"]
+        out["state_dominance_1"] = {
+            "num_solutions": s["outputs"]["num_solutions"],
+            "work_candidates_total": s["work"]["work_candidates_total"],
+            "work_frontier_survivors_total": s["work"]["work_frontier_survivors_total"],
+            "dominance_filtered_total": s["dominance"]["dominance_filtered_total"],
+        }
     with open(os.path.join(HERE, f"{name}.json"), "w") as f:
         json.dump(out, f, indent=1)
     print(name, {m: out["methods"][m]["num_solutions"] for m in out["methods"]})

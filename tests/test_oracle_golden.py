@@ -54,6 +54,11 @@ def test_oracle_knapsack_state_dominance_keeps_frontier(rec):
     st = {}
     got = oracle.enumerate(dd, 1, state_dominance=1, stats=st)
     assert np.array_equal(oracle.sorted_set(got), golden_frontier(rec, 1))
+    # and prunes exactly the labels the reference's run with state_dominance=1 prunes
+    want = rec["state_dominance_1"]
+    assert st["dominance_filtered_total"] == want["dominance_filtered_total"]
+    assert st["candidates_total"] == want["work_candidates_total"]
+    assert st["survivors_total"] == want["work_frontier_survivors_total"]
 
 
 def test_nd_keep_rule_against_bruteforce():
