@@ -170,6 +170,45 @@ def cpu_reference_sample(specs, workers, budget_s=25.0, max_items=96):
     return (done[0] / makespan if makespan > 0 else None), done[0]
 
 
+def single_instances(P, instances, device, with_ref):
+    """The single-instance configurations (seed 0): 3-objective knapsack n=40, 4-objective
+    knapsack n=60, 7-objective knapsack n=25, 3-objective set packing n=100 (m=20), each by
+    methods 1 and 3.  GPU: device time of one pmdd_enumerate after a warm-up call, and the
+    wall time of the call from host buffers.  Reference CPU (when built): its own binary
+    with every host thread, wall_enumeration_s of its stats record (DD build excluded)."""
+    import oracle  # reference CPU leg only
+
+    cases = [("kp3_n40", 1, 3, instances.knapsack_text(40, 3, 0)),
+             ("kp4_n60", 1, 4, instances.knapsack_text(60, 4, 0)),
+             ("kp7_n25", 1, 7, instances.knapsack_text(25, 7, 0)),
+             ("sp3_n100_m20", 2, 3, instances.setpacking_text(100, 20, 3, 0))]
+    threads = os.cpu_count() or 1
+    out = []
+    tmp = tempfile.mkdtemp()
+    for name, ptype, d, text in cases:
+        dd = P.DecisionDiagram.from_text(text, ptype, d)
+        path = os.path.join(tmp, name + ".dat")
+        with open(path, "w") as f:
+            f.write(text)
+        for method in (1, 3):
+            P.enumerate_dd(dd, method=method)
+            st = {}
+            t0 = time.perf_counter()
+            pts = P.enumerate_dd(dd, method=method, stats=st)
+            wall = time.perf_counter() - t0
+            rec = {"instance": name, "method": method, "solutions": int(len(pts)),
+                   "gpu_device_s": st["device_elapsed_s"], "gpu_call_s": wall,
+                   "candidates": int(st["work_candidates_total"]), "join_products": int(st["work_join_products_total"]),
+                   "candidates_filtered_per_s": st["work_candidates_total"] / st["device_elapsed_s"]}
+            if with_ref and oracle.have_ref(d):
+                r = oracle.run_ref(path, ptype, method, d, threads=threads)
+                rec["ref_cpu_s"] = float(r["stats"]["timing"]["wall"]["wall_enumeration_s"])
+                rec["ref_cpu_threads"] = threads
+                rec["ref_solutions"] = int(r["stats"]["outputs"]["num_solutions"])
+            out.append(rec)
+    return out
+
+
 # --------------------------------------------------------------- served loop
 def served_loop(rate, n_req, seed, P, instances):
     """Poisson arrivals at `rate` req/s; KP (n~U{20..60}) / SP (n~U{60..100}) method 1 and
@@ -237,10 +276,10 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
 
-    from pmdd_b200 import instances
+    from pmdd_b200 import instances, replicas
 
     n_kp, n_sp = 512, 256
-    specs = instances.stream_mix(n_kp, n_sp, 3, seed0=rank * (n_kp + n_sp))
+    specs = replicas.rank_stream(rank, n_kp, n_sp, 3)
     if args.subset > 1:
         specs = specs[:: args.subset]
     config = {"workload": "batched stream: 512 knapsack BDDs (d=3, n~U{20..60}) + 256 set-packing BDDs "
@@ -304,11 +343,7 @@ def main():
         torch.cuda.synchronize()
 
     def max_over_ranks(x):
-        if dist is None:
-            return x
-        tt = torch.tensor([x], dtype=torch.float64, device=f"cuda:{device}")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        return float(tt.item())
+        return replicas.max_over_ranks(x, dist, f"cuda:{device}")
 
     # ---------------------------------------------- device-resident (value)
     res = P.ResidentSet(dds, device=device)
@@ -453,6 +488,8 @@ def main():
                 line["cpu_baseline"] = {"value": r[0], "unit": "solves/s", "cores": cores, "kind": "reference",
                                         "sample": f"{r[1]} stream instances, {cores} concurrent single-threaded "
                                                   f"reference processes (wall_enumeration_s, DD build excluded)"}
+        # single large instances, GPU next to the reference CPU path
+        line["single_instance"] = single_instances(P, instances, device, with_ref=(world == 1 and not args.quick))
     if rank == 0:
         print(json.dumps(line))
     if dist is not None:

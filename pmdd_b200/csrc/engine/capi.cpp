@@ -101,6 +101,7 @@ struct RunInfo {
 int run_locked(DeviceSlot &slot, std::vector<std::unique_ptr<pmdd::Instance>> &reqs, RunInfo *info,
                std::string *err) {
     pmdd::Engine &E = *slot.engine;
+    E.reset_mem_peak();  // the peak reported for this call is this call's
     const int64_t l0 = E.launches();
     const pmdd::KernelTimes k0 = E.kernel_times();
     cudaEvent_t e0 = nullptr, e1 = nullptr;

@@ -15,8 +15,10 @@ constexpr int kTileThreads = 512;
 constexpr int kTileWindow = 1024;
 constexpr int kSmallMax = 1024;
 constexpr int kTileCap = 2 * kTileWindow;
-constexpr int kTileItemCap = 1024;   // destinations staged per pass inside one tile
-constexpr int kTileArcCap = 2048;    // arcs staged per pass inside one tile
+// Per-pass staging caps, sized so that a tile's shared memory (about 70 KB at d=3) lets
+// three 512-thread blocks share an SM.
+constexpr int kTileItemCap = 512;    // destinations staged per pass inside one tile
+constexpr int kTileArcCap = 1024;    // arcs staged per pass inside one tile
 
 // Destinations filtered inside a tile; every other destination takes the oversized
 // path.  Both the counting pass and the tile kernel decide with this one rule.
@@ -63,6 +65,9 @@ struct ExpandJob {
     void *big_surv;                // scratch: survivors of one bucket that overflow shared memory
     int32_t *big_idx;              // scratch: candidate index of each bucket-ordered point
     int32_t *big_surv_idx;         // scratch: candidate index of each overflowing survivor
+    int64_t big_mark_min;          // oversized destinations of at least this many candidates use the GPU-wide pass
+    int64_t big_window;            // pass p takes the destinations whose scratch offset is in
+                                   // [p * big_window, (p + 1) * big_window) (--max-cand)
     uint32_t *err;
     unsigned long long *tile_surv; // survivors written by the tile kernel (added to)
 };

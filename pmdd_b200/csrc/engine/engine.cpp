@@ -17,6 +17,7 @@
 #include <algorithm>
 #include <atomic>
 #include <climits>
+#include <cmath>
 #include <tuple>
 #include <cstdio>
 #include <cstdlib>
@@ -290,6 +291,8 @@ Engine::Engine(int device, int64_t budget_bytes, int max_slots) : device_(device
     if (max_slots_ <= 0) max_slots_ = 1 << 20;
     const char *tr = std::getenv("PMDD_TRACE");
     trace_ = tr != nullptr && tr[0] == '1';
+    const char *bm = std::getenv("PMDD_BIG_MARK_MIN");
+    if (bm && *bm && std::atoll(bm) > 0) big_mark_min_ = std::atoll(bm);
     // constant initial frontier: one zero point (up to 8 int64 values), offset 0, size 1
     if (!h_init_.reserve(256)) {
         error_ = "cudaMallocHost failed";
@@ -487,6 +490,11 @@ struct ExpPlan {
     int64_t cand;       // candidates of this expansion (trace / statistics)
     int64_t max_item;
     int64_t num_big;
+    // oversized scratch in passes of whole destinations (--max-cand): pass p holds the
+    // destinations whose scratch offset is in [p * big_window, (p + 1) * big_window),
+    // so big_rows = min(big_total, big_window + largest destination) rows suffice
+    int64_t big_window = 1;
+    int64_t big_rows = 0;
 };
 
 struct CountPlan {
@@ -553,8 +561,12 @@ int Engine::step() {
         bool okay = e.out_pts && e.out_off && e.out_size;
         if (okay && s.res.num_big > 0) {
             const int64_t bt = s.res.big_total;
+            const int64_t cap = I.opts.max_cand > 0 ? I.opts.max_cand : bt;
             e.big_total = bt;
-            e.big_mem = arena_.alloc(static_cast<size_t>(bt) * dev::big_scratch_bytes_per_point(I.d, I.elem()) + 1024);
+            e.big_window = std::max<int64_t>(1, std::min<int64_t>(cap, bt));
+            e.big_rows = std::min<int64_t>(bt, e.big_window + s.res.max_item);
+            e.big_mem =
+                arena_.alloc(static_cast<size_t>(e.big_rows) * dev::big_scratch_bytes_per_point(I.d, I.elem()) + 1024);
             okay = e.big_mem != nullptr;
         }
         if (!okay) {
@@ -599,6 +611,8 @@ int Engine::step() {
         size_t big_first, big_count;
         int64_t max_big;
         int64_t items;             // destinations over the group's jobs
+        int64_t big_passes;        // scratch passes of the oversized path
+        int64_t mark_min;          // oversized destinations from this size up take the GPU-wide pass
     };
     std::vector<GroupLaunch> glaunch;
     std::vector<int64_t> tile_bases(exps.size()), item_bases(exps.size());  // group-relative
@@ -607,7 +621,7 @@ int Engine::step() {
         std::vector<ExpPlan> ordered;
         ordered.reserve(exps.size());
         for (auto &g : groups) {
-            GroupLaunch gl{g.first.first, g.first.second, pos, g.second.size(), 0, bigwork.size(), 0, 0, 0};
+            GroupLaunch gl{g.first.first, g.first.second, pos, g.second.size(), 0, bigwork.size(), 0, 0, 0, 0, 0};
             for (size_t idx : g.second) {
                 const ExpPlan &e = exps[idx];
                 Instance &I = *e.I;
@@ -647,14 +661,16 @@ int Engine::step() {
                 J.big_list = s.big_list;
                 J.num_big = s.res.num_big;
                 if (e.big_mem) {
-                    const size_t pb = align256(static_cast<size_t>(e.big_total) * I.d * I.elem());
-                    const size_t ib = align256(sizeof(int32_t) * static_cast<size_t>(e.big_total));
+                    const size_t pb = align256(static_cast<size_t>(e.big_rows) * I.d * I.elem());
+                    const size_t ib = align256(sizeof(int32_t) * static_cast<size_t>(e.big_rows));
                     char *m = static_cast<char *>(e.big_mem);
                     J.big_pts = m;
                     J.big_pts2 = m + pb;
                     J.big_surv = m + 2 * pb;
                     J.big_idx = reinterpret_cast<int32_t *>(m + 3 * pb);
                     J.big_surv_idx = reinterpret_cast<int32_t *>(m + 3 * pb + ib);
+                    J.big_window = e.big_window;
+                    gl.big_passes = std::max<int64_t>(gl.big_passes, (e.big_total + e.big_window - 1) / e.big_window);
                 }
                 J.err = d_err_;
                 J.tile_surv = d_tile_surv + pos;
@@ -664,6 +680,8 @@ int Engine::step() {
                 ++pos;
             }
             gl.big_count = bigwork.size() - gl.big_first;
+            gl.mark_min = big_mark_min_;
+            for (size_t k = gl.first; k < gl.first + gl.count; ++k) xjobs[k].big_mark_min = gl.mark_min;
             glaunch.push_back(gl);
         }
         exps.swap(ordered);
@@ -994,10 +1012,14 @@ int Engine::step() {
         if (gl.big_count == 0) continue;
         const dev::ExpandJob *dj = reinterpret_cast<const dev::ExpandJob *>(d_stage + off_x) + gl.first;
         const dev::BigWork *bw = reinterpret_cast<const dev::BigWork *>(d_stage + off_b) + gl.big_first;
-        if (!cuda_ok(dev::launch_big(gl.d, gl.wide, dj, bw, static_cast<int>(gl.big_count), gl.max_big, sms_, stream_),
-                     "oversized-destination kernels"))
-            return -1;
-        launches_ += 3;
+        const bool with_mark = gl.max_big >= gl.mark_min;
+        for (int64_t pass = 0; pass < gl.big_passes; ++pass) {
+            if (!cuda_ok(dev::launch_big(gl.d, gl.wide, dj, bw, static_cast<int>(gl.big_count), gl.max_big, with_mark,
+                                         pass, stream_),
+                         "oversized-destination kernels"))
+                return -1;
+            launches_ += with_mark ? 4 : 2;
+        }
     }
     if (!sdjobs.empty()) {
         cudaMemsetAsync(d_removed, 0, sizeof(int64_t) * sdjobs.size(), stream_);

@@ -159,6 +159,8 @@ class Engine {
     bool cancel(uint64_t id);
     int64_t launches() const { return launches_; }
     const Arena &arena() const { return arena_; }
+    // Restarts the arena's high-water mark (gpu_mem_peak_used_bytes of later requests).
+    void reset_mem_peak() { arena_.reset_peak(); }
     int device() const { return device_; }
     cudaStream_t stream() const { return stream_; }
     KernelTimes kernel_times() const { return ktimes_; }
@@ -213,6 +215,9 @@ class Engine {
     int64_t launches_ = 0;
     KernelTimes ktimes_;
     bool trace_ = false;  // PMDD_TRACE=1: one stderr line per step
+    // oversized destinations of at least this many candidates are filtered by the
+    // GPU-wide mark/write pass instead of one SFS block (PMDD_BIG_MARK_MIN overrides)
+    int64_t big_mark_min_ = 65536;
 };
 
 }  // namespace pmdd

@@ -229,39 +229,22 @@ __device__ int32_t sfs_block(unsigned char *smem_raw, const T *__restrict__ P, i
             }
         }
         __syncthreads();
-        // 3c. append the bucket's maxima to K (the output) and the K cache in order of
-        // decreasing sum (ties by bucket position): buckets come in decreasing sum
-        // ranges, so the whole output is sorted by decreasing sum
-        if (tid == 0) s_m = 0;
-        __syncthreads();
+        // 3c. append the bucket's maxima to K (the output) and the K cache
         for (int32_t c0 = warp * 32; c0 < m; c0 += NW * 32) {
             const int32_t k = c0 + lane;
             const bool keep = k < m && (k < SC ? sflag[k] != 0 : I2[lo + k] != 0);
             const unsigned bal = __ballot_sync(0xffffffffu, keep);
-            if (bal == 0) continue;
-            Pt x;
-            int64_t sk = 0;
+            int32_t base = 0;
+            if (lane == 0 && bal) base = atomicAdd(&s_kn, __popc(bal));
+            base = __shfl_sync(0xffffffffu, base, 0);
             if (keep) {
-                x = k < SC ? sc[k] : load_global_pt<D, T>(SV, k);
-                sk = point_sum<D, T>(x.v);
-            }
-            int32_t rank = 0;
-            for (int32_t j = 0; j < m; ++j) {
-                if (!(j < SC ? sflag[j] != 0 : I2[lo + j] != 0)) continue;
-                const Pt q = j < SC ? sc[j] : load_global_pt<D, T>(SV, j);
-                const int64_t sj = point_sum<D, T>(q.v);
-                rank += (sj > sk || (sj == sk && j < k)) ? 1 : 0;
-            }
-            if (keep) {
-                const int32_t dst = kn + rank;
+                const int32_t dst = base + __popc(bal & ((1u << lane) - 1u));
+                const Pt x = k < SC ? sc[k] : load_global_pt<D, T>(SV, k);
 #pragma unroll
                 for (int o = 0; o < D; ++o) out[static_cast<int64_t>(dst) * D + o] = x.v[o];
                 if (dst < KS) kc[dst] = x;
             }
-            if (lane == 0) atomicAdd(&s_m, __popc(bal));
         }
-        __syncthreads();
-        if (tid == 0) s_kn = kn + s_m;
         __syncthreads();
     }
     return s_kn;

@@ -15,12 +15,8 @@
 //            destinations with warp-uniform shared-memory broadcast reads, skipping the
 //            candidates' own arc (shifts of one non-dominated, duplicate-free parent
 //            frontier never dominate each other) and leaving as soon as all 32 are
-//            decided.  Every frontier is kept sorted by decreasing objective sum, so each
-//            arc run is too, and a warp whose 32 candidates share one run sweeps, per
-//            other run, only the prefix whose sums reach its smallest undecided sum (a
-//            dominator's sum is never smaller);
-//   write:   survivors go to the destination's slot in the next layer's frontier,
-//            merged across the destination's runs so the slot stays sorted by sum.
+//            decided;
+//   write:   survivors go to the destination's slot in the next layer's frontier.
 //
 // Dominance rule (the reference GPU filter's dominates_or_tie_before,
 // src/pmdd/enum/gpu/dominance_utils.cuh:10-23, and the weak-dominance insert of
@@ -40,7 +36,6 @@ constexpr int kTT = kTileThreads;
 template <int D, typename T>
 struct TileSmem {
     PackedPt<D, T> pts[kTileCap];
-    int64_t sum[kTileCap];              // objective sum of each candidate
     int16_t tag[kTileCap];              // staged arc of each candidate
     uint16_t item_of[kTileCap];         // staged destination of each candidate
     uint8_t keep[kTileCap];
@@ -119,26 +114,27 @@ __device__ __forceinline__ bool sweep_range(const TileSmem<D, T> &S, int a, int 
 }
 
 // The common case: every lane's candidate lies in the same arc run of the same
-// destination, and [a, b) holds none of that run.  No per-lane range or arc checks;
-// the equal-point tie rule only matters for points before the lanes (j < q for all).
-template <int D, typename T>
-__device__ __forceinline__ bool sweep_other_arcs(const TileSmem<D, T> &S, int a, int b, const T (&p)[D], int q,
-                                                 bool dom) {
+// destination, and [a, b) holds none of that run, so [a, b) lies wholly before or
+// wholly after every lane's candidate.  No per-lane range or arc checks.  Points before
+// the lanes dominate on >= alone (of equal points the first stays); points after them
+// only when they also differ.
+template <int D, typename T, bool kBefore>
+__device__ __forceinline__ bool sweep_other_arcs(const TileSmem<D, T> &S, int a, int b, const T (&p)[D], bool dom) {
     int j = a;
     int it = 0;
     for (; j + 4 <= b; j += 4) {
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             const PackedPt<D, T> c = S.pts[j + u];
-            const bool ge = ge_all<D, T>(c, p);
-            dom |= ge && (j + u < q || !eq_all<D, T>(c, p));
+            if (kBefore) dom |= ge_all<D, T>(c, p);
+            else dom |= ge_all<D, T>(c, p) && !eq_all<D, T>(c, p);
         }
         if ((++it & 7) == 0 && __all_sync(0xffffffffu, dom)) return true;
     }
     for (; j < b; ++j) {
         const PackedPt<D, T> c = S.pts[j];
-        const bool ge = ge_all<D, T>(c, p);
-        dom |= ge && (j < q || !eq_all<D, T>(c, p));
+        if (kBefore) dom |= ge_all<D, T>(c, p);
+        else dom |= ge_all<D, T>(c, p) && !eq_all<D, T>(c, p);
     }
     return dom;
 }
@@ -282,7 +278,6 @@ __global__ void __launch_bounds__(kTT) expand_tile_kernel(const ExpandJob *__res
 #pragma unroll
                 for (int o = 0; o < PackedPt<D, T>::kPad; ++o) pt.v[o] = o < D ? src[o] + static_cast<T>(w[o]) : T(0);
                 S.pts[q] = pt;
-                S.sum[q] = point_sum<D, T>(pt.v);
                 S.tag[q] = static_cast<int16_t>(x);
                 S.item_of[q] = static_cast<uint16_t>(k);
             }
@@ -297,7 +292,7 @@ __global__ void __launch_bounds__(kTT) expand_tile_kernel(const ExpandJob *__res
                 const bool valid = q < total;
                 T p[D];
                 int my_tag = -1;
-                int js = INT_MAX, je = INT_MIN;
+                int js = INT_MAX, je = INT_MIN, slo = 0, shi = 0;
                 if (valid) {
                     const PackedPt<D, T> me = S.pts[q];
 #pragma unroll
@@ -306,6 +301,8 @@ __global__ void __launch_bounds__(kTT) expand_tile_kernel(const ExpandJob *__res
                     const int k = S.item_of[q];
                     js = S.item_s[k];
                     je = S.item_s[k + 1];
+                    slo = S.arc_pos[my_tag];
+                    shi = my_tag + 1 < S.item_arc0[k + 1] ? S.arc_pos[my_tag + 1] : je;
                 } else {
 #pragma unroll
                     for (int o = 0; o < D; ++o) p[o] = T(0);
@@ -315,25 +312,8 @@ __global__ void __launch_bounds__(kTT) expand_tile_kernel(const ExpandJob *__res
                 const bool one_run = __all_sync(0xffffffffu, valid) && warp_min_i(my_tag) == warp_max_i(my_tag);
                 bool dom = !valid;
                 if (one_run) {
-                    // Every arc run is sorted by decreasing sum (parent frontiers are), and
-                    // a dominator's sum is >= the point's: per other run only the prefix
-                    // with sum >= the smallest undecided lane's sum can hold one.
-                    const int k = S.item_of[c0];
-                    const int r0 = S.item_arc0[k], r1 = S.item_arc0[k + 1];
-                    const int64_t my_sum = S.sum[q];
-                    for (int r = r0; r < r1; ++r) {
-                        if (r == my_tag) continue;
-                        const int64_t thr = warp_min_i64(dom ? INT64_MAX : my_sum);
-                        if (thr == INT64_MAX) break;
-                        const int a = S.arc_pos[r], b = r + 1 < r1 ? S.arc_pos[r + 1] : J1;
-                        int lo = a, hi = b;
-                        while (lo < hi) {
-                            const int mid = (lo + hi) >> 1;
-                            if (S.sum[mid] >= thr) lo = mid + 1;
-                            else hi = mid;
-                        }
-                        dom = sweep_other_arcs<D, T>(S, a, lo, p, q, dom);
-                    }
+                    dom = sweep_other_arcs<D, T, true>(S, J0, slo, p, dom);
+                    if (!__all_sync(0xffffffffu, dom)) dom = sweep_other_arcs<D, T, false>(S, shi, J1, p, dom);
                 } else {
                     dom = sweep_range<D, T>(S, J0, J1, p, q, my_tag, js, je, dom);
                 }
@@ -364,30 +344,11 @@ __global__ void __launch_bounds__(kTT) expand_tile_kernel(const ExpandJob *__res
             __syncthreads();
             if (tid == 0 && J.tile_surv != nullptr && S.keep_ex[total] > 0)
                 atomicAdd(J.tile_surv, static_cast<unsigned long long>(S.keep_ex[total]));
-            // --- write survivors into each destination's slot, merging the destination's
-            // arc runs (each sorted by decreasing sum) so that the slot is sorted too:
-            // rank = survivors before q in (sum desc, run, position) order
+            // --- write survivors into each destination's slot
             for (int q = tid; q < total; q += kTT) {
                 if (!S.keep[q]) continue;
                 const int k = S.item_of[q];
-                const int r = S.tag[q];
-                const int r0 = S.item_arc0[k], r1 = S.item_arc0[k + 1];
-                const int je = S.item_s[k + 1];
-                const int64_t s = S.sum[q];
-                int32_t rank = S.keep_ex[q] - S.keep_ex[S.arc_pos[r]];
-                for (int r2 = r0; r2 < r1; ++r2) {
-                    if (r2 == r) continue;
-                    const int a = S.arc_pos[r2], b = r2 + 1 < r1 ? S.arc_pos[r2 + 1] : je;
-                    int lo = a, hi = b;
-                    while (lo < hi) {
-                        const int mid = (lo + hi) >> 1;
-                        const bool before = r2 < r ? S.sum[mid] >= s : S.sum[mid] > s;
-                        if (before) lo = mid + 1;
-                        else hi = mid;
-                    }
-                    rank += S.keep_ex[lo] - S.keep_ex[a];
-                }
-                const int64_t dst = S.item_c0[k] + rank;
+                const int64_t dst = S.item_c0[k] + (S.keep_ex[q] - S.keep_ex[S.item_s[k]]);
                 T *o_ = outp + dst * D;
                 const PackedPt<D, T> me = S.pts[q];
 #pragma unroll

@@ -145,6 +145,59 @@ def test_high_fan_in_knapsack():
     assert same_set(got, oracle.enumerate(dd, 1))
 
 
+SFS_VARIANT = r"""
+import sys
+sys.path.insert(0, {root!r})
+import numpy as np
+import oracle
+import pmdd_b200 as P
+from pmdd_b200 import instances
+cases = [(3, 5, instances.tsp_text(10, 5, 77)), (1, 3, instances.knapsack_text(48, 3, 4)),
+         (1, 3, instances.knapsack_text(30, 3, 9))]
+for ptype, d, text in cases:
+    dd = P.DecisionDiagram.from_text(text, ptype, d)
+    for method in (1, 3):
+        got = oracle.sorted_set(np.asarray(P.enumerate_dd(dd, method=method), dtype=np.int64))
+        want = oracle.sorted_set(np.asarray(oracle.enumerate(dd, method), dtype=np.int64))
+        assert np.array_equal(got, want), (ptype, d, method)
+print("ok")
+"""
+
+
+def test_oversized_destinations_through_the_gpu_wide_pass():
+    """With PMDD_BIG_MARK_MIN lowered, every oversized destination goes through the
+    GPU-wide mark/write pass instead of a single-block sort-filter-skyline: same
+    frontiers."""
+    import os
+    import subprocess
+    import sys
+
+    from conftest import ROOT
+
+    env = dict(os.environ, PMDD_BIG_MARK_MIN="1025")
+    p = subprocess.run([sys.executable, "-c", SFS_VARIANT.format(root=ROOT)], env=env, capture_output=True, text=True,
+                       timeout=600)
+    assert p.returncode == 0 and p.stdout.strip().endswith("ok"), p.stdout + p.stderr
+
+
+@pytest.mark.parametrize("method", (1, 3))
+def test_max_cand_bounds_the_oversized_scratch(method):
+    """--max-cand (the reference's destination batching, topdown.cu:671-860) caps the
+    candidates materialised at once: oversized destinations are filtered in passes of
+    whole destinations.  Same frontier, less device memory at the peak."""
+    dd = P.DecisionDiagram.from_text(instances.tsp_text(10, 5, 77), 3, 5)
+    st_all, st_cap = {}, {}
+    whole = P.enumerate_dd(dd, method=method, stats=st_all)
+    capped = P.enumerate_dd(dd, method=method, max_cand=3000, stats=st_cap)
+    assert same_set(whole, capped)
+    assert same_set(capped, oracle.enumerate(dd, method))
+    assert st_cap["work_candidates_total"] == st_all["work_candidates_total"]
+    if method == 1:
+        assert st_cap["gpu_mem_peak_used_bytes"] < st_all["gpu_mem_peak_used_bytes"]
+    else:  # the cutset join's buffers may set the peak instead
+        assert st_cap["gpu_mem_peak_used_bytes"] <= st_all["gpu_mem_peak_used_bytes"]
+
+
 def test_invalid_dd_is_rejected_not_run():
     dd = P.DecisionDiagram.from_text(instances.knapsack_text(5, 3, 1), 1, 3)
     with pytest.raises(P.CudaEnumerationError):
