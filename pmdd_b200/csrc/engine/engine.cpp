@@ -276,6 +276,8 @@ Engine::Engine(int device, int64_t budget_bytes, int max_slots) : device_(device
     }
     sms_ = prop.multiProcessorCount;
     if (!cuda_ok(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate")) return;
+    for (cudaEvent_t &ev : ev_)
+        if (!cuda_ok(cudaEventCreate(&ev), "cudaEventCreate")) return;
     size_t free_b = 0, total_b = 0;
     if (!cuda_ok(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo")) return;
     int64_t budget = budget_bytes;
@@ -308,6 +310,8 @@ Engine::~Engine() {
         cudaStreamSynchronize(stream_);
         cudaStreamDestroy(stream_);
     }
+    for (cudaEvent_t ev : ev_)
+        if (ev) cudaEventDestroy(ev);
 }
 
 bool Engine::cuda_ok(cudaError_t e, const char *what) {
@@ -509,6 +513,7 @@ std::atomic<int64_t> g_total_launches{0};
 
 int Engine::step() {
     if (!ok_) return -1;
+    const double step_t0 = trace_ ? now_s() : 0.0;
     struct LaunchTally {
         const int64_t &n;
         int64_t start;
@@ -978,11 +983,7 @@ int Engine::step() {
         ok_ = false;
         return -1;
     }
-    cudaEvent_t ev0, ev1, ev2, ev3;
-    cudaEventCreate(&ev0);
-    cudaEventCreate(&ev1);
-    cudaEventCreate(&ev2);
-    cudaEventCreate(&ev3);
+    cudaEvent_t ev0 = ev_[0], ev1 = ev_[1], ev2 = ev_[2], ev3 = ev_[3];
     if (stage_bytes && !cuda_ok(cudaMemcpyAsync(d_stage, hs, stage_bytes, cudaMemcpyHostToDevice, stream_), "H2D"))
         return -1;
     // coupling counters of requests that just reached their cutset start from the staged init values
@@ -1115,15 +1116,12 @@ int Engine::step() {
             tile_surv += reinterpret_cast<const unsigned long long *>(static_cast<char *>(h_summary_.p) + s_ts)[k];
         std::fprintf(stderr,
                      "[pmdd step] jobs=%zu counts=%zu couple=%zu cand=%lld big_items=%lld big_cand=%lld max_item=%lld "
-                     "tile_cand=%lld tile_surv=%llu tiles_ms=%.3f big_ms=%.3f rest_ms=%.3f\n",
+                     "tile_cand=%lld tile_surv=%llu tiles_ms=%.3f big_ms=%.3f rest_ms=%.3f host_to_sync_us=%.1f\n",
                      exps.size(), counts.size(), ujobs.size(), static_cast<long long>(cand),
                      static_cast<long long>(nbig), static_cast<long long>(big_cand), static_cast<long long>(max_item),
-                     static_cast<long long>(cand - big_cand), tile_surv, ms_expand, ms_big, ms_rest);
+                     static_cast<long long>(cand - big_cand), tile_surv, ms_expand, ms_big, ms_rest,
+                     (now_s() - step_t0) * 1e6);
     }
-    cudaEventDestroy(ev0);
-    cudaEventDestroy(ev1);
-    cudaEventDestroy(ev2);
-    cudaEventDestroy(ev3);
     for (void *q : step_scratch_) arena_.release(q);
     step_scratch_.clear();
 

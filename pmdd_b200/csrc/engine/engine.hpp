@@ -205,6 +205,7 @@ class Engine {
     int sms_ = 148;
     int max_slots_ = 0;
     cudaStream_t stream_ = nullptr;
+    cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};  // per-step phase timing, reused
     Arena arena_;
     std::deque<std::unique_ptr<Instance>> queued_;
     std::vector<std::unique_ptr<Instance>> active_;
