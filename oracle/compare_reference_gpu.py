@@ -57,7 +57,8 @@ def run(binary, path, ptype, method, timeout):
             return {"status": "failed: " + (tail[-1][:80] if tail else f"rc {p.returncode}")}
         rec = json.loads(open(sp).read().strip().splitlines()[-1])
         return {"status": "ok", "solutions": rec["outputs"]["num_solutions"],
-                "enum_s": rec["timing"]["wall"]["wall_enumeration_s"], "process_s": wall}
+                "enum_s": rec["timing"]["wall"]["wall_enumeration_s"],
+                "kernel_s": rec["timing"]["kernel"]["kernel_total_s"], "process_s": wall}
 
 
 def main():
@@ -67,8 +68,9 @@ def main():
     args = ap.parse_args()
     only = set(filter(None, args.only.split(",")))
     tmp = tempfile.mkdtemp()
-    print("| instance | method | solutions (this / reference) | this engine enum s | reference GPU enum s | ratio |")
-    print("|---|---:|---|---:|---:|---:|")
+    print("| instance | method | solutions (this / reference) | enum s, this / reference | ratio "
+          "| kernel s, this / reference | ratio | process s, this / reference |")
+    print("|---|---:|---|---|---:|---|---:|---|")
     for name, ptype, d, text, methods in cases():
         if only and name not in only:
             continue
@@ -81,10 +83,18 @@ def main():
             a = run(mine_bin, path, ptype, m, args.timeout)
             b = run(ref_bin, path, ptype, m, args.timeout) if os.path.exists(ref_bin) else {"status": "not built"}
             sols = f"{a.get('solutions', a['status'])} / {b.get('solutions', b['status'])}"
-            ea = f"{a['enum_s']:.4f}" if a["status"] == "ok" else a["status"]
-            eb = f"{b['enum_s']:.4f}" if b["status"] == "ok" else b["status"]
-            ratio = f"{b['enum_s'] / a['enum_s']:.1f}x" if a["status"] == b["status"] == "ok" and a["enum_s"] > 0 else ""
-            print(f"| {name} | {m} | {sols} | {ea} | {eb} | {ratio} |", flush=True)
+            both = a["status"] == b["status"] == "ok"
+
+            def pair(key):
+                fa = f"{a[key]:.4f}" if a["status"] == "ok" else a["status"]
+                fb = f"{b[key]:.4f}" if b["status"] == "ok" else b["status"]
+                r = f"{b[key] / a[key]:.1f}x" if both and a[key] > 0 else ""
+                return f"{fa} / {fb}", r
+
+            e, er = pair("enum_s")
+            k, kr = pair("kernel_s")
+            pw, _ = pair("process_s")
+            print(f"| {name} | {m} | {sols} | {e} | {er} | {k} | {kr} | {pw} |", flush=True)
 
 
 if __name__ == "__main__":

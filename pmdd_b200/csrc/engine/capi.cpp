@@ -1,9 +1,12 @@
 // extern "C" boundary of libpmdd_gpu.so (declared in include/pmdd.h).
+#include <atomic>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <unordered_map>
 
 #include "engine.hpp"
@@ -97,9 +100,11 @@ struct RunInfo {
 };
 
 // Runs prepared requests to completion on the device's shared engine.  Caller holds
-// slot.mu and has called ensure_engine.
+// slot.mu and has called ensure_engine.  With `ready`, request i is submitted only once
+// ready(i) holds (its DD is being packed by other threads meanwhile); requests are
+// submitted in order, and the engine steps on those already submitted.
 int run_locked(DeviceSlot &slot, std::vector<std::unique_ptr<pmdd::Instance>> &reqs, RunInfo *info,
-               std::string *err) {
+               std::string *err, const std::function<bool(size_t)> &ready = nullptr) {
     pmdd::Engine &E = *slot.engine;
     E.reset_mem_peak();  // the peak reported for this call is this call's
     const int64_t l0 = E.launches();
@@ -108,20 +113,29 @@ int run_locked(DeviceSlot &slot, std::vector<std::unique_ptr<pmdd::Instance>> &r
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     cudaEventRecord(e0, E.stream());
-    std::unordered_map<uint64_t, size_t> index;
-    for (size_t i = 0; i < reqs.size(); ++i) {
-        reqs[i]->id = i;
-        index[i] = i;
-        E.submit(std::move(reqs[i]));
-    }
+    const size_t n = reqs.size();
+    size_t next_submit = 0;
+    auto submit_ready = [&]() {
+        while (next_submit < n && (!ready || ready(next_submit))) {
+            reqs[next_submit]->id = next_submit;
+            E.submit(std::move(reqs[next_submit]));
+            ++next_submit;
+        }
+    };
     size_t got = 0;
     int rc = PMDD_OK;
-    while (got < index.size()) {
+    while (got < n) {
+        submit_ready();
+        if (E.idle()) {  // every submitted request is done; the rest are still being packed
+            std::this_thread::yield();
+            continue;
+        }
         const int r = E.step();
         while (!E.finished().empty()) {
             std::unique_ptr<pmdd::Instance> q = std::move(E.finished().front());
             E.finished().pop_front();
-            reqs[index[q->id]] = std::move(q);
+            const size_t at = static_cast<size_t>(q->id);
+            reqs[at] = std::move(q);
             ++got;
         }
         if (r < 0) {
@@ -203,14 +217,49 @@ void pack_all(pmdd::Engine &E, const pmdd_dd *dds, std::vector<std::unique_ptr<p
 }
 
 // Packs (when `dds` is given) and runs prepared requests on the device's shared engine.
+// The packing runs on host threads beside the engine: request i is submitted as soon as
+// its DD sits in the pinned staging, so its upload and the first layers of the earlier
+// requests overlap the packing of the later ones.
 int run_on_device(int device, std::vector<std::unique_ptr<pmdd::Instance>> &reqs, RunInfo *info, std::string *err,
                   const pmdd_dd *dds = nullptr) {
     DeviceSlot &slot = slot_for(device);
     std::lock_guard<std::mutex> lk(slot.mu);
     const int rc = ensure_engine(device, slot, err);
     if (rc != PMDD_OK) return rc;
-    if (dds) pack_all(*slot.engine, dds, reqs);
-    return run_locked(slot, reqs, info, err);
+    if (!dds) return run_locked(slot, reqs, info, err);
+    if (reqs.size() < 2) {
+        pack_all(*slot.engine, dds, reqs);
+        return run_locked(slot, reqs, info, err);
+    }
+    const size_t n = reqs.size();
+    std::vector<size_t> off(n + 1, 0);
+    for (size_t i = 0; i < n; ++i) off[i + 1] = off[i] + ((reqs[i]->blob_bytes + 255) & ~static_cast<size_t>(255));
+    unsigned char *st = off[n] > 0 && off[n] <= kMaxStagingBytes ? slot.engine->staging(off[n]) : nullptr;
+    std::vector<pmdd::Instance *> inst(n);
+    for (size_t i = 0; i < n; ++i) inst[i] = reqs[i].get();
+    std::unique_ptr<std::atomic<int>[]> packed(new std::atomic<int>[n]);
+    for (size_t i = 0; i < n; ++i) packed[i].store(0, std::memory_order_relaxed);
+    std::atomic<size_t> next(0);
+    auto worker = [&]() {
+        for (size_t i = next++; i < n; i = next++) {
+            pmdd::Instance &I = *inst[i];
+            if (st) {
+                pmdd::pack_instance(dds[i], I, st + off[i]);
+                I.blob_src = st + off[i];
+            } else {
+                I.blob.assign(I.blob_bytes, 0);
+                pmdd::pack_instance(dds[i], I, I.blob.data());
+            }
+            packed[i].store(1, std::memory_order_release);
+        }
+    };
+    const int threads = static_cast<int>(std::min<size_t>(static_cast<size_t>(pmdd::host_threads()), n));
+    std::vector<std::thread> pool;
+    for (int t = 0; t < threads; ++t) pool.emplace_back(worker);
+    const int r = run_locked(slot, reqs, info, err,
+                             [&](size_t i) { return packed[i].load(std::memory_order_acquire) != 0; });
+    for (auto &th : pool) th.join();
+    return r;
 }
 
 int collect_batch(std::vector<std::unique_ptr<pmdd::Instance>> &reqs, pmdd_frontier *outs, int32_t *status,

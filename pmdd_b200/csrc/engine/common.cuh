@@ -65,9 +65,10 @@ struct ExpandJob {
     void *big_surv;                // scratch: survivors of one bucket that overflow shared memory
     int32_t *big_idx;              // scratch: candidate index of each bucket-ordered point
     int32_t *big_surv_idx;         // scratch: candidate index of each overflowing survivor
-    int64_t big_mark_min;          // oversized destinations of at least this many candidates use the GPU-wide pass
+    int64_t big_mark_min;          // oversized destinations of at least this many candidates take the mark path
     int64_t big_window;            // pass p takes the destinations whose scratch offset is in
                                    // [p * big_window, (p + 1) * big_window) (--max-cand)
+    int64_t big_rows;              // scratch rows (candidates) one pass can use
     uint32_t *err;
     unsigned long long *tile_surv; // survivors written by the tile kernel (added to)
 };

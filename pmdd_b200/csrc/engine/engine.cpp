@@ -34,54 +34,75 @@ static size_t align256(size_t x) { return (x + 255) & ~static_cast<size_t>(255);
 
 // ------------------------------------------------------------------- Arena
 Arena::~Arena() {
-    if (base_) cudaFree(base_);
+    for (auto &c : chunks_) cudaFree(reinterpret_cast<void *>(c.first));
 }
 
-bool Arena::init(size_t bytes, std::string *err) {
-    bytes &= ~static_cast<size_t>(255);
-    cudaError_t e = cudaMalloc(reinterpret_cast<void **>(&base_), bytes);
-    if (e != cudaSuccess) {
-        if (err) *err = std::string("cudaMalloc of the engine arena failed: ") + cudaGetErrorString(e);
-        base_ = nullptr;
+bool Arena::init(size_t budget, size_t initial, std::string *err) {
+    cap_ = budget & ~static_cast<size_t>(255);
+    if (!grow(std::min(std::max<size_t>(initial, 256), cap_))) {
+        if (err) *err = "cudaMalloc of the engine arena failed";
         return false;
     }
-    cap_ = bytes;
-    free_.clear();
-    free_[0] = bytes;
+    return true;
+}
+
+bool Arena::grow(size_t at_least) {
+    size_t bytes = align256(std::max(at_least, std::min<size_t>(reserved_, size_t(16) << 30)));
+    if (reserved_ + bytes > cap_) bytes = align256(at_least);
+    if (reserved_ + bytes > cap_) return false;
+    void *p = nullptr;
+    const double t0 = now_s();
+    if (cudaMalloc(&p, bytes) != cudaSuccess) {
+        cudaGetLastError();  // clear the sticky-free allocation error
+        return false;
+    }
+    grow_s_ += now_s() - t0;
+    const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+    chunks_[a] = bytes;
+    free_[a] = bytes;
+    reserved_ += bytes;
     return true;
 }
 
 void *Arena::alloc(size_t bytes) {
     bytes = align256(bytes == 0 ? 1 : bytes);
-    for (auto it = free_.begin(); it != free_.end(); ++it) {
-        if (it->second < bytes) continue;
-        const size_t off = it->first, rem = it->second - bytes;
-        free_.erase(it);
-        if (rem) free_[off + bytes] = rem;
-        live_[off] = bytes;
-        used_ += bytes;
-        peak_ = std::max(peak_, used_);
-        return base_ + off;
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        for (auto it = free_.begin(); it != free_.end(); ++it) {
+            if (it->second < bytes) continue;
+            const uintptr_t a = it->first;
+            const size_t rem = it->second - bytes;
+            free_.erase(it);
+            if (rem) free_[a + bytes] = rem;
+            live_[a] = bytes;
+            used_ += bytes;
+            peak_ = std::max(peak_, used_);
+            return reinterpret_cast<void *>(a);
+        }
+        if (attempt == 0 && !grow(bytes)) return nullptr;
     }
     return nullptr;
 }
 
 void Arena::release(void *p) {
     if (p == nullptr) return;
-    const size_t off = static_cast<size_t>(static_cast<char *>(p) - base_);
-    auto lv = live_.find(off);
+    const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+    auto lv = live_.find(a);
     if (lv == live_.end()) return;
-    size_t start = off, bytes = lv->second;
+    uintptr_t start = a;
+    size_t bytes = lv->second;
     live_.erase(lv);
     used_ -= bytes;
+    // coalesce with free neighbours of the same cudaMalloc chunk only
+    auto ch = std::prev(chunks_.upper_bound(a));
+    const uintptr_t c0 = ch->first, c1 = ch->first + ch->second;
     auto next = free_.lower_bound(start);
-    if (next != free_.end() && next->first == start + bytes) {
+    if (next != free_.end() && next->first == start + bytes && next->first < c1) {
         bytes += next->second;
         next = free_.erase(next);
     }
     if (next != free_.begin()) {
         auto prev = std::prev(next);
-        if (prev->first + prev->second == start) {
+        if (prev->first + prev->second == start && prev->first >= c0) {
             start = prev->first;
             bytes += prev->second;
             free_.erase(prev);
@@ -255,6 +276,15 @@ int prepare_instance(const pmdd_dd &dd, const pmdd_options &o, uint64_t id, Inst
 
 // ------------------------------------------------------------------ Engine
 Engine::Engine(int device, int64_t budget_bytes, int max_slots) : device_(device), max_slots_(max_slots) {
+    const double init_t0 = now_s();
+    struct InitTrace {
+        const double &t0;
+        const bool &ok;
+        ~InitTrace() {
+            const char *tr = std::getenv("PMDD_TRACE");
+            if (tr && tr[0] == '1') std::fprintf(stderr, "[pmdd engine] init_ms=%.1f ok=%d\n", (now_s() - t0) * 1e3, ok);
+        }
+    } init_trace{init_t0, ok_};
     int count = 0;
     cudaError_t e = cudaGetDeviceCount(&count);
     if (e != cudaSuccess || count <= 0) {
@@ -287,7 +317,11 @@ Engine::Engine(int device, int64_t budget_bytes, int max_slots) : device_(device
         error_ = "not enough free device memory for the engine arena";
         return;
     }
-    if (!arena_.init(static_cast<size_t>(budget), &error_)) return;
+    // device memory is taken as it is needed: 2 GB now (PMDD_ARENA_INITIAL), more later
+    int64_t initial = static_cast<int64_t>(2) << 30;
+    const char *ini = std::getenv("PMDD_ARENA_INITIAL");
+    if (ini && *ini && std::atoll(ini) > 0) initial = std::atoll(ini);
+    if (!arena_.init(static_cast<size_t>(budget), static_cast<size_t>(std::min(initial, budget)), &error_)) return;
     d_err_ = static_cast<uint32_t *>(arena_.alloc(sizeof(uint32_t)));
     if (!cuda_ok(cudaMemsetAsync(d_err_, 0, sizeof(uint32_t), stream_), "cudaMemsetAsync")) return;
     if (max_slots_ <= 0) max_slots_ = 1 << 20;
@@ -617,16 +651,18 @@ int Engine::step() {
         int64_t max_big;
         int64_t items;             // destinations over the group's jobs
         int64_t big_passes;        // scratch passes of the oversized path
-        int64_t mark_min;          // oversized destinations from this size up take the GPU-wide pass
+        int64_t big_rows;          // oversized candidate rows over the group's jobs (flat space)
+        int64_t mark_cap;          // upper bound on the group's mark-path destinations per pass
     };
     std::vector<GroupLaunch> glaunch;
     std::vector<int64_t> tile_bases(exps.size()), item_bases(exps.size());  // group-relative
+    std::vector<int64_t> big_bases(exps.size());                           // group-relative
     {
         size_t pos = 0;
         std::vector<ExpPlan> ordered;
         ordered.reserve(exps.size());
         for (auto &g : groups) {
-            GroupLaunch gl{g.first.first, g.first.second, pos, g.second.size(), 0, bigwork.size(), 0, 0, 0, 0, 0};
+            GroupLaunch gl{g.first.first, g.first.second, pos, g.second.size(), 0, bigwork.size(), 0, 0, 0, 0, 0, 0};
             for (size_t idx : g.second) {
                 const ExpPlan &e = exps[idx];
                 Instance &I = *e.I;
@@ -675,8 +711,13 @@ int Engine::step() {
                     J.big_idx = reinterpret_cast<int32_t *>(m + 3 * pb);
                     J.big_surv_idx = reinterpret_cast<int32_t *>(m + 3 * pb + ib);
                     J.big_window = e.big_window;
+                    J.big_rows = e.big_rows;
+                    J.big_mark_min = big_mark_min_;
+                    if (s.res.max_item >= big_mark_min_) gl.mark_cap += e.big_rows / big_mark_min_ + 1;
                     gl.big_passes = std::max<int64_t>(gl.big_passes, (e.big_total + e.big_window - 1) / e.big_window);
                 }
+                big_bases[pos] = gl.big_rows;
+                gl.big_rows += J.big_rows;
                 J.err = d_err_;
                 J.tile_surv = d_tile_surv + pos;
                 for (int b = 0; b < s.res.num_big; ++b) bigwork.push_back({static_cast<int32_t>(pos - gl.first), b});
@@ -685,8 +726,6 @@ int Engine::step() {
                 ++pos;
             }
             gl.big_count = bigwork.size() - gl.big_first;
-            gl.mark_min = big_mark_min_;
-            for (size_t k = gl.first; k < gl.first + gl.count; ++k) xjobs[k].big_mark_min = gl.mark_min;
             glaunch.push_back(gl);
         }
         exps.swap(ordered);
@@ -780,7 +819,8 @@ int Engine::step() {
     const size_t off_c = align256(off_b + sizeof(dev::BigWork) * bigwork.size());
     const size_t off_tb = align256(off_c + sizeof(dev::CountJob) * cjobs.size());
     const size_t off_ib = align256(off_tb + sizeof(int64_t) * tile_bases.size());
-    const size_t off_sd = align256(off_ib + sizeof(int64_t) * item_bases.size());
+    const size_t off_bb = align256(off_ib + sizeof(int64_t) * item_bases.size());
+    const size_t off_sd = align256(off_bb + sizeof(int64_t) * big_bases.size());
     const size_t off_sdb = align256(off_sd + sizeof(dev::StateDomJob) * sdjobs.size());
     size_t off_k = align256(off_sdb + sizeof(int64_t) * sd_bases.size());
     // coupling: requests at their cutset
@@ -888,6 +928,7 @@ int Engine::step() {
     if (!tile_bases.empty()) {
         std::memcpy(hs + off_tb, tile_bases.data(), sizeof(int64_t) * tile_bases.size());
         std::memcpy(hs + off_ib, item_bases.data(), sizeof(int64_t) * item_bases.size());
+        std::memcpy(hs + off_bb, big_bases.data(), sizeof(int64_t) * big_bases.size());
     }
     if (!sdjobs.empty()) {
         std::memcpy(hs + off_sd, sdjobs.data(), sizeof(dev::StateDomJob) * sdjobs.size());
@@ -1012,14 +1053,29 @@ int Engine::step() {
     for (const GroupLaunch &gl : glaunch) {
         if (gl.big_count == 0) continue;
         const dev::ExpandJob *dj = reinterpret_cast<const dev::ExpandJob *>(d_stage + off_x) + gl.first;
-        const dev::BigWork *bw = reinterpret_cast<const dev::BigWork *>(d_stage + off_b) + gl.big_first;
-        const bool with_mark = gl.max_big >= gl.mark_min;
-        for (int64_t pass = 0; pass < gl.big_passes; ++pass) {
-            if (!cuda_ok(dev::launch_big(gl.d, gl.wide, dj, bw, static_cast<int>(gl.big_count), gl.max_big, with_mark,
-                                         pass, stream_),
-                         "oversized-destination kernels"))
+        dev::BigLaunch L;
+        L.jobs = dj;
+        L.work = reinterpret_cast<const dev::BigWork *>(d_stage + off_b) + gl.big_first;
+        L.num_work = static_cast<int>(gl.big_count);
+        L.job_bases = reinterpret_cast<const int64_t *>(d_stage + off_bb) + gl.first;
+        L.num_jobs = static_cast<int>(gl.count);
+        L.total = gl.big_rows;
+        L.sms = sms_;
+        L.with_sfs = true;
+        L.mark_cap = static_cast<int>(std::min<int64_t>(gl.mark_cap, static_cast<int64_t>(gl.big_count)));
+        L.plan = nullptr;
+        if (L.mark_cap > 0) {
+            L.plan = scratch(dev::big_plan_bytes(L.mark_cap));
+            if (!L.plan) {
+                error_ = "engine bookkeeping allocation failed";
+                ok_ = false;
                 return -1;
-            launches_ += with_mark ? 4 : 2;
+            }
+        }
+        for (int64_t pass = 0; pass < gl.big_passes; ++pass) {
+            L.pass = pass;
+            if (!cuda_ok(dev::launch_big(gl.d, gl.wide, L, stream_), "oversized-destination kernels")) return -1;
+            launches_ += L.mark_cap > 0 ? 5 : 2;
         }
     }
     if (!sdjobs.empty()) {
@@ -1116,11 +1172,12 @@ int Engine::step() {
             tile_surv += reinterpret_cast<const unsigned long long *>(static_cast<char *>(h_summary_.p) + s_ts)[k];
         std::fprintf(stderr,
                      "[pmdd step] jobs=%zu counts=%zu couple=%zu cand=%lld big_items=%lld big_cand=%lld max_item=%lld "
-                     "tile_cand=%lld tile_surv=%llu tiles_ms=%.3f big_ms=%.3f rest_ms=%.3f host_to_sync_us=%.1f\n",
+                     "tile_cand=%lld tile_surv=%llu tiles_ms=%.3f big_ms=%.3f rest_ms=%.3f host_to_sync_us=%.1f "
+                     "arena_reserved_mb=%.0f arena_grow_ms=%.1f\n",
                      exps.size(), counts.size(), ujobs.size(), static_cast<long long>(cand),
                      static_cast<long long>(nbig), static_cast<long long>(big_cand), static_cast<long long>(max_item),
                      static_cast<long long>(cand - big_cand), tile_surv, ms_expand, ms_big, ms_rest,
-                     (now_s() - step_t0) * 1e6);
+                     (now_s() - step_t0) * 1e6, arena_.reserved() / 1e6, arena_.grow_seconds() * 1e3);
     }
     for (void *q : step_scratch_) arena_.release(q);
     step_scratch_.clear();
@@ -1210,7 +1267,7 @@ int Engine::step() {
         if ((*it)->phase == Instance::DONE) {
             Instance &I = **it;
             I.stats.gpu_mem_peak_used_bytes = static_cast<int64_t>(arena_.peak());
-            I.stats.gpu_mem_peak_reserved_bytes = static_cast<int64_t>(arena_.capacity());
+            I.stats.gpu_mem_peak_reserved_bytes = static_cast<int64_t>(arena_.reserved());
             release_instance(I);
             I.finish_s = now_s();
             finished_.push_back(std::move(*it));

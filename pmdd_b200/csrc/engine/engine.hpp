@@ -29,25 +29,32 @@ double now_s();
 // Kernels launched by every engine of this process.
 extern std::atomic<int64_t> g_total_launches;
 
-// First-fit allocator over one device allocation.  Bookkeeping is host-side; every
-// kernel of the engine runs on one stream, so memory released on the host may be
-// handed out again immediately (later work on the stream runs after earlier work).
+// First-fit allocator over device memory taken in a few large cudaMalloc chunks, the
+// first of `initial` bytes at start-up and more (doubling, at most 16 GB at a time) when
+// a request does not fit, up to `budget` in all.  Bookkeeping is host-side; every kernel
+// of the engine runs on one stream, so memory released on the host may be handed out
+// again immediately (later work on the stream runs after earlier work).  Free blocks
+// never merge across chunks.
 class Arena {
   public:
     ~Arena();
-    bool init(size_t bytes, std::string *err);
+    bool init(size_t budget, size_t initial, std::string *err);
     void *alloc(size_t bytes);
     void release(void *p);
-    size_t capacity() const { return cap_; }
+    size_t capacity() const { return cap_; }       // the budget
+    size_t reserved() const { return reserved_; }  // device memory taken so far
     size_t used() const { return used_; }
     size_t peak() const { return peak_; }
     void reset_peak() { peak_ = used_; }
+    double grow_seconds() const { return grow_s_; }  // host time spent in cudaMalloc
 
   private:
-    char *base_ = nullptr;
-    size_t cap_ = 0, used_ = 0, peak_ = 0;
-    std::map<size_t, size_t> free_;             // offset -> bytes
-    std::unordered_map<size_t, size_t> live_;   // offset -> bytes
+    bool grow(size_t at_least);
+    size_t cap_ = 0, reserved_ = 0, used_ = 0, peak_ = 0;
+    double grow_s_ = 0;
+    std::map<uintptr_t, size_t> chunks_;            // cudaMalloc base -> bytes
+    std::map<uintptr_t, size_t> free_;              // address -> bytes
+    std::unordered_map<uintptr_t, size_t> live_;    // address -> bytes
 };
 
 // Frontiers of one direction at its current layer, in slot layout: node i's points

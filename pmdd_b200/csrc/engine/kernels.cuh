@@ -14,11 +14,23 @@ cudaError_t launch_expand_tiles(int d, bool wide, const ExpandJob *jobs, const i
 // num_tiles - 1)); one thread per destination over all jobs.
 cudaError_t launch_tile_plan(const ExpandJob *jobs, const int64_t *item_bases, int num_jobs, int64_t total_items,
                              cudaStream_t stream);
-// Oversized destinations of scratch pass `pass` (see ExpandJob::big_window): expand,
-// then the single-block SFS for those below ExpandJob::big_mark_min candidates;
-// `with_mark` also launches the GPU-wide mark and write passes for the larger ones.
-cudaError_t launch_big(int d, bool wide, const ExpandJob *jobs, const BigWork *work, int num_work, int64_t max_item,
-                       bool with_mark, int64_t pass, cudaStream_t stream);
+// One scratch pass (see ExpandJob::big_window) of the oversized destinations of one
+// (d, wide) group.
+struct BigLaunch {
+    const ExpandJob *jobs;
+    const BigWork *work;         // every oversized destination of the group
+    int num_work;
+    const int64_t *job_bases;    // exclusive prefix of the jobs' big_rows (flat candidate space)
+    int num_jobs;
+    int64_t total;               // sum of the jobs' big_rows
+    int64_t pass;
+    int sms;
+    bool with_sfs;               // launch the SFS blocks (destinations below big_mark_min)
+    void *plan;                  // big_plan_bytes(mark_cap) of scratch for the mark path
+    int mark_cap;                // upper bound on mark-path destinations in the pass; 0: none
+};
+size_t big_plan_bytes(int cap);
+cudaError_t launch_big(int d, bool wide, const BigLaunch &L, cudaStream_t stream);
 
 }  // namespace dev
 }  // namespace pmdd
