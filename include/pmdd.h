@@ -211,6 +211,12 @@ void pmdd_server_destroy(pmdd_server *srv);
 const char *pmdd_version(void);
 /* Number of kernels this library has launched in this process (all calls). */
 int64_t pmdd_launch_count(void);
+/* The oversized-destination crossover (candidates from which a destination is filtered
+ * by the GPU-wide pass rather than one sort-filter-skyline block) that the tuning file
+ * at `path` holds for (nobjs, problem_type), or 0 if it holds none.  path NULL: the file
+ * engines read at start-up (PMDD_TUNING_FILE, else the per-user cache written by
+ * pmdd_b200.autotune).  No counterpart in the reference, which has one filter path. */
+int64_t pmdd_tuned_mark_min(const char *path, int32_t nobjs, int32_t problem_type);
 
 #ifdef __cplusplus
 }

@@ -176,6 +176,7 @@ GPU_SYMBOLS = {
     "pmdd_server_destroy": (None, [ctypes.c_void_p]),
     "pmdd_version": (ctypes.c_char_p, []),
     "pmdd_launch_count": (c_i64, []),
+    "pmdd_tuned_mark_min": (c_i64, [ctypes.c_char_p, c_i32, c_i32]),
 }
 
 _host = None

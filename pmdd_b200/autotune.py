@@ -1,0 +1,151 @@
+"""Autotuner for the oversized-destination crossover, cached per (objectives, problem type).
+
+Destinations too large for a shared-memory tile are filtered one of two ways: one
+sort-filter-skyline block each (little work, one SM per destination) or the GPU-wide
+pairwise mark pass (more work, every SM).  The size from which the mark pass pays depends
+on the instance family: a knapsack stream has many mid-sized destinations, a 5-objective
+15-city TSP a few huge ones.  For each requested (objectives, problem type) this tuner
+times a calibration instance of that family under a list of crossover sizes, each in a
+fresh process (the engine reads PMDD_BIG_MARK_MIN at start-up), keeps the fastest, and
+writes the choice to the tuning file the engine reads at start-up:
+
+    {"version": 1, "entries": {"d<objectives>_p<problem type>": {"big_mark_min": n,
+                                "seconds": {"<n>": device seconds, ...}, "instance": "..."}}}
+
+    python -m pmdd_b200.autotune --nobjs 3 5 --ptype 1 3 [--out PATH]
+
+The file is PMDD_TUNING_FILE if set, else $XDG_CACHE_HOME/pmdd_b200/tuning.json or
+~/.cache/pmdd_b200/tuning.json.  Without a file the engine uses 65536 for every family.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+from typing import Callable, Dict, Iterable, Optional, Sequence
+
+from . import instances
+
+CANDIDATE_SIZES = (4096, 16384, 65536, 262144, 1 << 40)
+DEFAULT_MARK_MIN = 65536
+
+
+def tuning_path() -> str:
+    p = os.environ.get("PMDD_TUNING_FILE")
+    if p:
+        return p
+    base = os.environ.get("XDG_CACHE_HOME") or os.path.join(os.path.expanduser("~"), ".cache")
+    return os.path.join(base, "pmdd_b200", "tuning.json")
+
+
+def calibration_instance(nobjs: int, problem_type: int):
+    """(description, text) of the instance a family is tuned on: large enough that
+    some destinations leave the tiles, small enough to run in seconds."""
+    if problem_type == 1:
+        n = {1: 120, 2: 90, 3: 60, 4: 50}.get(nobjs, 30)
+        return f"knapsack n={n} seed 0", instances.knapsack_text(n, nobjs, 0)
+    if problem_type == 2:
+        return "set packing n=100 m=20 seed 0", instances.setpacking_text(100, 20, nobjs, 0)
+    n = {1: 14, 2: 14, 3: 13, 4: 12}.get(nobjs, 11)
+    return f"tsp n={n} seed 0", instances.tsp_text(n, nobjs, 0)
+
+
+_CHILD = r"""
+import json, sys
+sys.path.insert(0, {root!r})
+import pmdd_b200 as P
+dd = P.DecisionDiagram.from_text(open({path!r}).read(), {ptype}, {nobjs})
+best = None
+for _ in range({repeats}):
+    st = {{}}
+    P.enumerate_dd(dd, method={method}, stats=st)
+    best = st["device_elapsed_s"] if best is None else min(best, st["device_elapsed_s"])
+print(json.dumps({{"seconds": best}}))
+"""
+
+
+def time_in_child(path: str, nobjs: int, problem_type: int, method: int, mark_min: int, repeats: int = 3,
+                  timeout: float = 600.0) -> Optional[float]:
+    """Best device time of `repeats` enumerations in a fresh process with the given
+    crossover; None if the run fails or times out."""
+    root = os.path.abspath(os.path.join(os.path.dirname(__file__), ".."))
+    code = _CHILD.format(root=root, path=path, ptype=problem_type, nobjs=nobjs, method=method, repeats=repeats)
+    env = dict(os.environ, PMDD_BIG_MARK_MIN=str(int(mark_min)))
+    try:
+        p = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=timeout)
+    except subprocess.TimeoutExpired:
+        return None
+    if p.returncode != 0:
+        return None
+    try:
+        return float(json.loads(p.stdout.strip().splitlines()[-1])["seconds"])
+    except (ValueError, KeyError, IndexError):
+        return None
+
+
+def choose(times: Dict[int, Optional[float]]) -> int:
+    """Fastest crossover; ties (within 2 %) go to the larger size (fewer GPU-wide
+    passes); no usable timing -> the default."""
+    ok = {k: v for k, v in times.items() if v is not None}
+    if not ok:
+        return DEFAULT_MARK_MIN
+    best = min(ok.values())
+    return max(k for k, v in ok.items() if v <= best * 1.02)
+
+
+def tune(families: Iterable[tuple], sizes: Sequence[int] = CANDIDATE_SIZES, method: int = 1,
+         timer: Optional[Callable[..., Optional[float]]] = None, workdir: Optional[str] = None) -> Dict[str, dict]:
+    """Tunes every (nobjs, problem_type) of `families`; returns the entries to store."""
+    import tempfile
+
+    timer = timer or time_in_child
+    workdir = workdir or tempfile.mkdtemp()
+    out = {}
+    for nobjs, ptype in families:
+        desc, text = calibration_instance(nobjs, ptype)
+        path = os.path.join(workdir, f"cal_d{nobjs}_p{ptype}.dat")
+        with open(path, "w") as f:
+            f.write(text)
+        times = {int(s): timer(path, nobjs, ptype, method, int(s)) for s in sizes}
+        out[f"d{nobjs}_p{ptype}"] = {"big_mark_min": choose(times),
+                                     "seconds": {str(k): v for k, v in times.items()}, "instance": desc}
+    return out
+
+
+def write(entries: Dict[str, dict], path: Optional[str] = None) -> str:
+    """Merges `entries` into the tuning file (other families are kept)."""
+    path = path or tuning_path()
+    data = {"version": 1, "entries": {}}
+    if os.path.exists(path):
+        try:
+            with open(path) as f:
+                old = json.load(f)
+            data["entries"].update(old.get("entries", {}))
+        except (OSError, ValueError):
+            pass
+    data["entries"].update(entries)
+    os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
+    tmp = path + ".tmp"
+    with open(tmp, "w") as f:
+        json.dump(data, f, indent=1)
+    os.replace(tmp, path)
+    return path
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    ap.add_argument("--nobjs", type=int, nargs="+", default=[3])
+    ap.add_argument("--ptype", type=int, nargs="+", default=[1, 2, 3])
+    ap.add_argument("--out", default=None)
+    args = ap.parse_args(argv)
+    entries = tune([(d, p) for d in args.nobjs for p in args.ptype])
+    path = write(entries, args.out)
+    for k, v in entries.items():
+        print(k, v["big_mark_min"], v["seconds"])
+    print("written", path)
+
+
+if __name__ == "__main__":
+    main()

@@ -651,4 +651,10 @@ const char *pmdd_version(void) { return "pmdd_b200 0.1 (sm_100a)"; }
 
 int64_t pmdd_launch_count(void) { return pmdd::g_total_launches.load(); }
 
+int64_t pmdd_tuned_mark_min(const char *path, int32_t nobjs, int32_t problem_type) {
+    const auto table = pmdd::read_tuning(path ? std::string(path) : pmdd::default_tuning_path());
+    auto it = table.find({nobjs, problem_type});
+    return it != table.end() ? it->second : 0;
+}
+
 }  // extern "C"

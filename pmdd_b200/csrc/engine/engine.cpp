@@ -322,13 +322,12 @@ Engine::Engine(int device, int64_t budget_bytes, int max_slots) : device_(device
     const char *ini = std::getenv("PMDD_ARENA_INITIAL");
     if (ini && *ini && std::atoll(ini) > 0) initial = std::atoll(ini);
     if (!arena_.init(static_cast<size_t>(budget), static_cast<size_t>(std::min(initial, budget)), &error_)) return;
-    d_err_ = static_cast<uint32_t *>(arena_.alloc(sizeof(uint32_t)));
-    if (!cuda_ok(cudaMemsetAsync(d_err_, 0, sizeof(uint32_t), stream_), "cudaMemsetAsync")) return;
     if (max_slots_ <= 0) max_slots_ = 1 << 20;
     const char *tr = std::getenv("PMDD_TRACE");
     trace_ = tr != nullptr && tr[0] == '1';
     const char *bm = std::getenv("PMDD_BIG_MARK_MIN");
-    if (bm && *bm && std::atoll(bm) > 0) big_mark_min_ = std::atoll(bm);
+    if (bm && *bm && std::atoll(bm) > 0) big_mark_min_fixed_ = std::atoll(bm);
+    load_tuning();
     // constant initial frontier: one zero point (up to 8 int64 values), offset 0, size 1
     if (!h_init_.reserve(256)) {
         error_ = "cudaMallocHost failed";
@@ -353,6 +352,54 @@ bool Engine::cuda_ok(cudaError_t e, const char *what) {
     error_ = std::string(what) + " failed: " + cudaGetErrorString(e);
     ok_ = false;
     return false;
+}
+
+// The tuning file written by pmdd_b200.autotune: {"entries": {"d<D>_p<P>":
+// {"big_mark_min": <n>, ...}, ...}} (PMDD_TUNING_FILE, else
+// $XDG_CACHE_HOME/pmdd_b200/tuning.json or ~/.cache/pmdd_b200/tuning.json).  Entries
+// that do not parse are ignored; a missing file leaves the defaults.
+std::string default_tuning_path() {
+    if (const char *p = std::getenv("PMDD_TUNING_FILE")) return p;
+    if (const char *x = std::getenv("XDG_CACHE_HOME")) return std::string(x) + "/pmdd_b200/tuning.json";
+    if (const char *h = std::getenv("HOME")) return std::string(h) + "/.cache/pmdd_b200/tuning.json";
+    return std::string();
+}
+
+std::map<std::pair<int, int>, int64_t> read_tuning(const std::string &path) {
+    std::map<std::pair<int, int>, int64_t> out;
+    if (path.empty()) return out;
+    FILE *f = std::fopen(path.c_str(), "rb");
+    if (!f) return out;
+    std::string text;
+    char buf[4096];
+    size_t got;
+    while ((got = std::fread(buf, 1, sizeof(buf), f)) > 0 && text.size() < (1u << 20)) text.append(buf, got);
+    std::fclose(f);
+    size_t pos = 0;
+    while ((pos = text.find("\"d", pos)) != std::string::npos) {
+        int d = 0, p = 0, used = 0;
+        if (std::sscanf(text.c_str() + pos, "\"d%d_p%d\"%n", &d, &p, &used) != 2 || used == 0) {
+            ++pos;
+            continue;
+        }
+        const size_t end = text.find('}', pos);
+        const size_t key = text.find("\"big_mark_min\"", pos);
+        if (key != std::string::npos && key < end) {
+            long long v = 0;
+            if (std::sscanf(text.c_str() + key + 14, " : %lld", &v) == 1 && v > 0 && d >= 1 && d <= 8)
+                out[{d, p}] = v;
+        }
+        pos += used;
+    }
+    return out;
+}
+
+void Engine::load_tuning() { tuned_mark_min_ = read_tuning(default_tuning_path()); }
+
+int64_t Engine::mark_min_for(int d, int problem_type) const {
+    if (big_mark_min_fixed_ > 0) return big_mark_min_fixed_;
+    auto it = tuned_mark_min_.find({d, problem_type});
+    return it != tuned_mark_min_.end() ? it->second : 65536;
 }
 
 void *Engine::scratch(size_t bytes) {
@@ -621,16 +668,6 @@ int Engine::step() {
         exps.push_back(e);
     }
 
-    // survivors written by the tile kernel, one counter per expansion (statistics)
-    unsigned long long *d_tile_surv = nullptr;
-    if (!exps.empty()) {
-        d_tile_surv = static_cast<unsigned long long *>(scratch(sizeof(unsigned long long) * exps.size()));
-        if (!d_tile_surv) {
-            error_ = "engine bookkeeping allocation failed";
-            ok_ = false;
-            return -1;
-        }
-    }
 
     // group by (d, wide) and build descriptors
     std::map<std::pair<int, bool>, std::vector<size_t>> groups;
@@ -712,14 +749,13 @@ int Engine::step() {
                     J.big_surv_idx = reinterpret_cast<int32_t *>(m + 3 * pb + ib);
                     J.big_window = e.big_window;
                     J.big_rows = e.big_rows;
-                    J.big_mark_min = big_mark_min_;
-                    if (s.res.max_item >= big_mark_min_) gl.mark_cap += e.big_rows / big_mark_min_ + 1;
+                    const int64_t mm = mark_min_for(I.d, I.opts.problem_type);
+                    J.big_mark_min = mm;
+                    if (s.res.max_item >= mm) gl.mark_cap += e.big_rows / mm + 1;
                     gl.big_passes = std::max<int64_t>(gl.big_passes, (e.big_total + e.big_window - 1) / e.big_window);
                 }
                 big_bases[pos] = gl.big_rows;
                 gl.big_rows += J.big_rows;
-                J.err = d_err_;
-                J.tile_surv = d_tile_surv + pos;
                 for (int b = 0; b < s.res.num_big; ++b) bigwork.push_back({static_cast<int32_t>(pos - gl.first), b});
                 if (s.res.num_big > 0) gl.max_big = std::max(gl.max_big, s.res.max_item);
                 ordered.push_back(e);
@@ -743,7 +779,6 @@ int Engine::step() {
     std::vector<int64_t> sd_bases;
     std::vector<Instance *> sd_inst;
     std::vector<SdGroup> sdg;
-    int64_t *d_removed = nullptr;
     {
         std::vector<size_t> pick;
         size_t keep_bytes = 0;
@@ -757,14 +792,12 @@ int Engine::step() {
             }
         }
         if (!pick.empty()) {
-            char *mem = static_cast<char *>(scratch(align256(sizeof(int64_t) * pick.size()) + keep_bytes));
-            if (!mem) {
+            char *keep = static_cast<char *>(scratch(keep_bytes));
+            if (!keep) {
                 error_ = "engine bookkeeping allocation failed";
                 ok_ = false;
                 return -1;
             }
-            d_removed = reinterpret_cast<int64_t *>(mem);
-            char *keep = mem + align256(sizeof(int64_t) * pick.size());
             for (size_t k = 0; k < pick.size(); ++k) {
                 const ExpPlan &e = exps[pick[k]];
                 Instance &I = *e.I;
@@ -779,7 +812,7 @@ int Engine::step() {
                 J.size = e.out_size;
                 J.keep = reinterpret_cast<uint8_t *>(keep);
                 keep += align256(static_cast<size_t>(std::max<int64_t>(e.cand, 1)));
-                J.removed = d_removed + k;
+                J.removed = nullptr;  // set once the step's summary block exists
                 J.node_base = I.layer_off[e.nl];
                 J.num_nodes = I.nodes_in(e.nl);
                 if (sdg.empty() || sdg.back().d != I.d || sdg.back().wide != I.wide)
@@ -808,9 +841,25 @@ int Engine::step() {
     std::vector<dev::CountJob> cjobs(counts.size());
     std::vector<int64_t *> new_arc_off(counts.size(), nullptr);
     std::vector<int64_t *> new_big(counts.size(), nullptr);
-    dev::CountResult *d_results = nullptr;
-    if (!counts.empty()) d_results = static_cast<dev::CountResult *>(scratch(sizeof(dev::CountResult) * counts.size()));
-    bool count_alloc_ok = counts.empty() || d_results != nullptr;
+    // The step's summary block: everything the host reads back after the step, in one
+    // device allocation and one copy: count results | tile survivors per expansion |
+    // labels removed by state dominance per job | error word.  All but the count
+    // results start at zero (one memset).
+    const size_t f_ts = sizeof(dev::CountResult) * counts.size();
+    const size_t f_sd = f_ts + sizeof(unsigned long long) * exps.size();
+    const size_t f_err = f_sd + sizeof(int64_t) * sdjobs.size();
+    const size_t f_total = f_err + sizeof(uint64_t);
+    char *d_fixed = static_cast<char *>(scratch(f_total));
+    dev::CountResult *d_results = counts.empty() ? nullptr : reinterpret_cast<dev::CountResult *>(d_fixed);
+    unsigned long long *d_tile_surv = d_fixed ? reinterpret_cast<unsigned long long *>(d_fixed + f_ts) : nullptr;
+    int64_t *d_removed = d_fixed ? reinterpret_cast<int64_t *>(d_fixed + f_sd) : nullptr;
+    uint32_t *d_err_step = d_fixed ? reinterpret_cast<uint32_t *>(d_fixed + f_err) : nullptr;
+    for (size_t k = 0; k < xjobs.size(); ++k) {
+        xjobs[k].tile_surv = d_tile_surv ? d_tile_surv + k : nullptr;
+        xjobs[k].err = d_err_step;
+    }
+    for (size_t k = 0; k < sdjobs.size(); ++k) sdjobs[k].removed = d_removed ? d_removed + k : nullptr;
+    bool count_alloc_ok = d_fixed != nullptr;
     // the expansion's new frontier is what the count reads; resolve per plan below
 
     // ------------------------------------------------------------- staging
@@ -1011,14 +1060,11 @@ int Engine::step() {
 
     // ----------------------------------------------------------- device work
     char *d_stage = stage_bytes ? static_cast<char *>(scratch(stage_bytes)) : nullptr;
-    // summary layout (D2H): count results | coupling ctrs | finishing sizes | error word
-    const size_t s_counts = 0;
-    const size_t s_ctr = align256(s_counts + sizeof(dev::CountResult) * counts.size());
+    // host summary (D2H): the summary block | coupling ctrs | finishing sizes
+    const size_t s_counts = 0, s_ts = f_ts, s_sd = f_sd, s_err = f_err;
+    const size_t s_ctr = align256(f_total);
     const size_t s_fin = align256(s_ctr + sizeof(int64_t) * dev::kCtrCount * ujobs.size());
-    const size_t s_sd = align256(s_fin + sizeof(int32_t) * finishing.size());
-    const size_t s_ts = align256(s_sd + sizeof(int64_t) * sdjobs.size());
-    const size_t s_err = align256(s_ts + sizeof(unsigned long long) * exps.size());
-    const size_t s_total = s_err + sizeof(uint32_t);
+    const size_t s_total = s_fin + sizeof(int32_t) * finishing.size();
     if ((stage_bytes && !d_stage) || !h_summary_.reserve(s_total)) {
         error_ = "engine bookkeeping allocation failed";
         ok_ = false;
@@ -1033,7 +1079,7 @@ int Engine::step() {
         cudaMemcpyAsync(ujobs[k].ctr, d_stage + off_ctrinit + sizeof(int64_t) * dev::kCtrCount * k,
                         sizeof(int64_t) * dev::kCtrCount, cudaMemcpyDeviceToDevice, stream_);
     }
-    if (d_tile_surv) cudaMemsetAsync(d_tile_surv, 0, sizeof(unsigned long long) * exps.size(), stream_);
+    cudaMemsetAsync(d_fixed + f_ts, 0, f_total - f_ts, stream_);
     cudaEventRecord(ev0, stream_);
     for (const GroupLaunch &gl : glaunch) {
         const dev::ExpandJob *dj = reinterpret_cast<const dev::ExpandJob *>(d_stage + off_x) + gl.first;
@@ -1079,7 +1125,6 @@ int Engine::step() {
         }
     }
     if (!sdjobs.empty()) {
-        cudaMemsetAsync(d_removed, 0, sizeof(int64_t) * sdjobs.size(), stream_);
         for (const SdGroup &g : sdg) {
             const dev::StateDomJob *dj = reinterpret_cast<const dev::StateDomJob *>(d_stage + off_sd) + g.first;
             const int64_t *db = reinterpret_cast<const int64_t *>(d_stage + off_sdb) + g.first;
@@ -1129,21 +1174,13 @@ int Engine::step() {
     }
     cudaEventRecord(ev3, stream_);
     char *hsum = static_cast<char *>(h_summary_.p);
-    if (!counts.empty())
-        cudaMemcpyAsync(hsum + s_counts, d_results, sizeof(dev::CountResult) * counts.size(), cudaMemcpyDeviceToHost,
-                        stream_);
+    cudaMemcpyAsync(hsum + s_counts, d_fixed, f_total, cudaMemcpyDeviceToHost, stream_);
     for (size_t k = 0; k < ujobs.size(); ++k)
         cudaMemcpyAsync(hsum + s_ctr + sizeof(int64_t) * dev::kCtrCount * k, ujobs[k].ctr,
                         sizeof(int64_t) * dev::kCtrCount, cudaMemcpyDeviceToHost, stream_);
     for (size_t k = 0; k < finishing.size(); ++k)
         cudaMemcpyAsync(hsum + s_fin + sizeof(int32_t) * k, finishing[k]->td.size, sizeof(int32_t),
                         cudaMemcpyDeviceToHost, stream_);
-    if (!sdjobs.empty())
-        cudaMemcpyAsync(hsum + s_sd, d_removed, sizeof(int64_t) * sdjobs.size(), cudaMemcpyDeviceToHost, stream_);
-    if (d_tile_surv)
-        cudaMemcpyAsync(hsum + s_ts, d_tile_surv, sizeof(unsigned long long) * exps.size(), cudaMemcpyDeviceToHost,
-                        stream_);
-    cudaMemcpyAsync(hsum + s_err, d_err_, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream_);
     for (void *q : to_release) arena_.release(q);
     const cudaError_t se = cudaStreamSynchronize(stream_);
     if (!cuda_ok(se, "engine step")) {
@@ -1185,7 +1222,6 @@ int Engine::step() {
     // ----------------------------------------------------------- host updates
     const uint32_t errw = *reinterpret_cast<uint32_t *>(hsum + s_err);
     if (errw != 0) {
-        cudaMemsetAsync(d_err_, 0, sizeof(uint32_t), stream_);
         for (auto &p : active_)
             if (p->phase != Instance::DONE) fail(*p, PMDD_ERR_INTERNAL, "device-side index check failed");
     }

@@ -134,6 +134,11 @@ int prepare_instance(const pmdd_dd &dd, const pmdd_options &opts, uint64_t id, I
 // at the instance's offsets; the alignment gaps are left as they are).
 void pack_instance(const pmdd_dd &dd, const Instance &inst, unsigned char *dst);
 
+// Tuned oversized-path crossovers, (objectives, problem type) -> big_mark_min, from the
+// tuning file pmdd_b200.autotune writes (see Engine::mark_min_for); empty when absent.
+std::string default_tuning_path();
+std::map<std::pair<int, int>, int64_t> read_tuning(const std::string &path);
+
 // Runs fn(i) for i in [0, n) on up to `threads` host threads (PMDD_HOST_THREADS caps
 // the default, which is the hardware concurrency, at most 32).
 void parallel_for(int64_t n, int threads, const std::function<void(int64_t)> &fn);
@@ -219,13 +224,17 @@ class Engine {
     std::deque<std::unique_ptr<Instance>> finished_;
     std::vector<void *> step_scratch_;
     Pinned h_desc_, h_summary_, h_init_, h_stage_;
-    uint32_t *d_err_ = nullptr;
+
     int64_t launches_ = 0;
     KernelTimes ktimes_;
     bool trace_ = false;  // PMDD_TRACE=1: one stderr line per step
-    // oversized destinations of at least this many candidates are filtered by the
-    // GPU-wide mark/write pass instead of one SFS block (PMDD_BIG_MARK_MIN overrides)
-    int64_t big_mark_min_ = 65536;
+    // Oversized destinations of at least mark_min_for(d, problem type) candidates are
+    // filtered by the GPU-wide mark/write pass instead of one SFS block: PMDD_BIG_MARK_MIN
+    // if set, else the tuned value for (d, problem type) from the tuning file, else 65536.
+    int64_t mark_min_for(int d, int problem_type) const;
+    void load_tuning();
+    int64_t big_mark_min_fixed_ = 0;
+    std::map<std::pair<int, int>, int64_t> tuned_mark_min_;
 };
 
 }  // namespace pmdd

@@ -1,0 +1,104 @@
+"""The crossover autotuner (pmdd_b200/autotune.py) and the engine's reading of its
+tuning file (pmdd_tuned_mark_min, the same parser the engine uses at start-up)."""
+import json
+import os
+
+import pytest
+
+from pmdd_b200 import _native, autotune
+
+
+def test_choose_picks_fastest_and_breaks_ties_upward():
+    assert autotune.choose({4096: 2.0, 65536: 1.0, 1 << 40: 1.5}) == 65536
+    assert autotune.choose({4096: 1.00, 65536: 1.01, 262144: 3.0}) == 65536  # within 2 %: larger size
+    assert autotune.choose({4096: None, 65536: None}) == autotune.DEFAULT_MARK_MIN
+    assert autotune.choose({4096: None, 16384: 0.5}) == 16384
+
+
+def test_tune_with_a_fake_timer(tmp_path):
+    calls = []
+
+    def timer(path, nobjs, ptype, method, mark_min):
+        calls.append((nobjs, ptype, mark_min))
+        assert os.path.exists(path)
+        return 1.0 + abs(mark_min - 16384) / 1e6
+
+    entries = autotune.tune([(3, 1), (5, 3)], sizes=(4096, 16384, 65536), timer=timer, workdir=str(tmp_path))
+    assert set(entries) == {"d3_p1", "d5_p3"}
+    assert all(e["big_mark_min"] == 16384 for e in entries.values())
+    assert len(calls) == 6
+
+
+def test_calibration_instances_build():
+    from pmdd_b200 import DecisionDiagram
+
+    for nobjs, ptype in ((3, 1), (7, 1), (3, 2), (3, 3), (5, 3)):
+        _, text = autotune.calibration_instance(nobjs, ptype)
+        dd = DecisionDiagram.from_text(text, ptype, nobjs)
+        assert dd.view.num_layers >= 2 and dd.view.nobjs == nobjs
+
+
+def test_written_file_is_what_the_engine_reads(tmp_path):
+    path = str(tmp_path / "tuning.json")
+    autotune.write({"d3_p1": {"big_mark_min": 12345, "seconds": {}}, "d5_p3": {"big_mark_min": 777}}, path)
+    autotune.write({"d4_p2": {"big_mark_min": 4242}}, path)  # merges, keeps the others
+    data = json.load(open(path))
+    assert set(data["entries"]) == {"d3_p1", "d5_p3", "d4_p2"}
+    lib = _native.gpu_lib()
+    assert lib.pmdd_tuned_mark_min(path.encode(), 3, 1) == 12345
+    assert lib.pmdd_tuned_mark_min(path.encode(), 5, 3) == 777
+    assert lib.pmdd_tuned_mark_min(path.encode(), 4, 2) == 4242
+    assert lib.pmdd_tuned_mark_min(path.encode(), 3, 2) == 0
+    assert lib.pmdd_tuned_mark_min(str(tmp_path / "missing.json").encode(), 3, 1) == 0
+
+
+def test_tuning_path_follows_the_environment(monkeypatch, tmp_path):
+    monkeypatch.setenv("PMDD_TUNING_FILE", str(tmp_path / "x.json"))
+    assert autotune.tuning_path() == str(tmp_path / "x.json")
+    monkeypatch.delenv("PMDD_TUNING_FILE")
+    monkeypatch.setenv("XDG_CACHE_HOME", str(tmp_path))
+    assert autotune.tuning_path() == os.path.join(str(tmp_path), "pmdd_b200", "tuning.json")
+    lib = _native.gpu_lib()
+    autotune.write({"d2_p1": {"big_mark_min": 99}})
+    assert lib.pmdd_tuned_mark_min(None, 2, 1) == 99
+
+
+TUNED_CHILD = r"""
+import sys, json
+sys.path.insert(0, {root!r})
+import numpy as np
+import oracle
+import pmdd_b200 as P
+from pmdd_b200 import instances
+dd = P.DecisionDiagram.from_text(instances.tsp_text(10, 5, 77), 3, 5)
+st = {{}}
+got = P.enumerate_dd(dd, method=1, stats=st)
+ok = np.array_equal(oracle.sorted_set(np.asarray(got, dtype=np.int64)),
+                    oracle.sorted_set(np.asarray(oracle.enumerate(dd, 1), dtype=np.int64)))
+print(json.dumps({{"ok": bool(ok), "launches": st["gpu_launches"]}}))
+"""
+
+
+@pytest.mark.gpu
+def test_engine_applies_the_tuned_crossover(tmp_path):
+    """A tuning file that sends 5-objective TSP destinations of 1025+ candidates to the
+    GPU-wide pass changes the kernels launched (plan, mark, write), not the frontier."""
+    import subprocess
+    import sys
+
+    from conftest import ROOT
+
+    def run(env_extra):
+        env = dict(os.environ, **env_extra)
+        env.pop("PMDD_BIG_MARK_MIN", None)
+        p = subprocess.run([sys.executable, "-c", TUNED_CHILD.format(root=ROOT)], env=env, capture_output=True,
+                           text=True, timeout=600)
+        assert p.returncode == 0, p.stdout + p.stderr
+        return json.loads(p.stdout.strip().splitlines()[-1])
+
+    path = str(tmp_path / "tuning.json")
+    autotune.write({"d5_p3": {"big_mark_min": 1025}}, path)
+    tuned = run({"PMDD_TUNING_FILE": path})
+    plain = run({"PMDD_TUNING_FILE": str(tmp_path / "none.json")})
+    assert tuned["ok"] and plain["ok"]
+    assert tuned["launches"] > plain["launches"]
