@@ -86,13 +86,16 @@ def time_in_child(path: str, nobjs: int, problem_type: int, method: int, mark_mi
 
 
 def choose(times: Dict[int, Optional[float]]) -> int:
-    """Fastest crossover; ties (within 2 %) go to the larger size (fewer GPU-wide
-    passes); no usable timing -> the default."""
+    """Fastest crossover.  Sizes within 2 % of the fastest tie: the default wins a tie
+    (a calibration run whose destinations never reach the crossover says nothing about
+    it), otherwise the larger size (fewer GPU-wide passes); no usable timing -> the
+    default."""
     ok = {k: v for k, v in times.items() if v is not None}
     if not ok:
         return DEFAULT_MARK_MIN
     best = min(ok.values())
-    return max(k for k, v in ok.items() if v <= best * 1.02)
+    tied = [k for k, v in ok.items() if v <= best * 1.02]
+    return DEFAULT_MARK_MIN if DEFAULT_MARK_MIN in tied else max(tied)
 
 
 def tune(families: Iterable[tuple], sizes: Sequence[int] = CANDIDATE_SIZES, method: int = 1,

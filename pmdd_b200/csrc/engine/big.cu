@@ -344,7 +344,7 @@ __global__ void __launch_bounds__(kWriteThreads) big_write_kernel(const ExpandJo
 
 // Destinations below big_mark_min candidates: one block each.
 template <int D, typename T>
-__global__ void __launch_bounds__(SfsCfg<D, T>::kThreads) big_sfs_kernel(const ExpandJob *__restrict__ jobs,
+__global__ void __launch_bounds__(SfsSmallCfg<D, T>::kThreads) big_sfs_kernel(const ExpandJob *__restrict__ jobs,
                                                                          const BigWork *__restrict__ work,
                                                                          int64_t pass) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -357,15 +357,15 @@ __global__ void __launch_bounds__(SfsCfg<D, T>::kThreads) big_sfs_kernel(const E
     s.I2 = J.big_idx + B.soff;
     s.SV = static_cast<T *>(J.big_surv) + B.soff * D;
     s.SVI = J.big_surv_idx + B.soff;
-    const int32_t kept = sfs_block<D, T>(smem_raw, static_cast<const T *>(J.big_pts) + B.soff * D, B.n, s,
-                                         static_cast<T *>(J.out_pts) + B.c0 * D);
+    const int32_t kept = sfs_block<D, T, SfsSmallCfg<D, T>>(smem_raw, static_cast<const T *>(J.big_pts) + B.soff * D,
+                                                            B.n, s, static_cast<T *>(J.out_pts) + B.c0 * D);
     if (threadIdx.x == 0) J.out_size[B.item] = kept;
 }
 
 template <int D, typename T>
 static cudaError_t launch_big_t(const BigLaunch &L, cudaStream_t stream) {
     if (L.num_work <= 0 || L.total <= 0) return cudaSuccess;
-    using Cfg = SfsCfg<D, T>;
+    using Cfg = SfsSmallCfg<D, T>;
     static bool attr_set = false;
     if (!attr_set) {
         cudaError_t e = cudaFuncSetAttribute(big_sfs_kernel<D, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -20,16 +20,27 @@
 namespace pmdd {
 namespace dev {
 
-template <int D, typename T>
-struct SfsCfg {
-    static constexpr int kThreads = 512;
+template <int D, typename T, int kThreads_, int kMaxBuckets_, int kKeepBytes, int kSurvBytes>
+struct SfsCfgT {
+    static constexpr int kThreads = kThreads_;
     static constexpr int kBucket = 512;        // target points per sum bucket
-    static constexpr int kMaxBuckets = 8192;
-    static constexpr int kKeepCache = 65536 / static_cast<int>(sizeof(PackedPt<D, T>));
-    static constexpr int kSurvCache = 32768 / static_cast<int>(sizeof(PackedPt<D, T>));
+    static constexpr int kMaxBuckets = kMaxBuckets_;
+    static constexpr int kKeepCache = kKeepBytes / static_cast<int>(sizeof(PackedPt<D, T>));
+    static constexpr int kSurvCache = kSurvBytes / static_cast<int>(sizeof(PackedPt<D, T>));
     static constexpr size_t kSmem = sizeof(int32_t) * kMaxBuckets + sizeof(PackedPt<D, T>) * kKeepCache +
                                     (sizeof(PackedPt<D, T>) + sizeof(int32_t) + 1) * kSurvCache + 256;
+    static_assert(kMaxBuckets % kThreads == 0, "bucket scan layout");
 };
+
+// One large block per point set (standalone filter, cutset join): 139 KB of shared
+// memory at d=3, so maxima caches hold 4096 points.
+template <int D, typename T>
+using SfsCfg = SfsCfgT<D, T, 512, 8192, 65536, 32768>;
+
+// Oversized destinations, many side by side: 256 threads and ~60 KB of shared memory at
+// d=3, so three blocks share an SM.
+template <int D, typename T>
+using SfsSmallCfg = SfsCfgT<D, T, 256, 2048, 32768, 16384>;
 
 // Scratch of a point set of n points: P2 and SV hold n points each, I2 and SVI n ints.
 template <typename T>
@@ -49,12 +60,11 @@ __device__ __forceinline__ PackedPt<D, T> load_global_pt(const T *base, int64_t 
 }
 
 // Maxima of P[0..n) (D values per point) into out[0..k); returns k (all threads).
-// Must be called by every thread of a block of SfsCfg<D,T>::kThreads threads with
-// SfsCfg<D,T>::kSmem bytes of dynamic shared memory at smem_raw; n < 2^31.
-template <int D, typename T>
+// Must be called by every thread of a block of Cfg::kThreads threads with Cfg::kSmem
+// bytes of dynamic shared memory at smem_raw; n < 2^31.
+template <int D, typename T, class Cfg = SfsCfg<D, T>>
 __device__ int32_t sfs_block(unsigned char *smem_raw, const T *__restrict__ P, int64_t n, SfsScratch<T> s,
                              T *__restrict__ out) {
-    using Cfg = SfsCfg<D, T>;
     using Pt = PackedPt<D, T>;
     constexpr int NT = Cfg::kThreads, NW = NT / 32, KS = Cfg::kKeepCache, SC = Cfg::kSurvCache;
     Pt *kc = reinterpret_cast<Pt *>(smem_raw);                  // [KS]
