@@ -62,6 +62,8 @@ def dd_bytes(dd):
     n = (v.num_layers + 1) + (v.num_nodes + 1) + 2 * v.num_arcs + v.num_weights * v.nobjs
     if v.min_weight:
         n += v.num_nodes
+    if v.node_state:
+        n += 2 * v.num_nodes * v.state_words
     return 4 * n
 
 

@@ -61,6 +61,12 @@ enum pmdd_status {
  * min_weight (optional, may be NULL): knapsack used-capacity lower bound per node,
  * required only for state_dominance > 0 with problem_type 1 (the reference's
  * Node::min_weight, src/pmdd/bdd/knapsack_bdd.cpp:123-150).
+ *
+ * node_state (optional, may be NULL): set-packing state per node, state_words 64-bit
+ * words each, bit v of word v/64 set iff vertex v may still be chosen below the node
+ * (the reference's Node::setpack_state, src/pmdd/bdd/indepset_bdd.cpp:79-135);
+ * required only for state_dominance > 0 with problem_type 2.  state_words is 0 when
+ * node_state is NULL.
  */
 typedef struct pmdd_dd {
     int32_t nobjs;        /* objectives per point, 1..8 */
@@ -74,13 +80,18 @@ typedef struct pmdd_dd {
     const int32_t *arc_weight;      /* [num_arcs] row index into weights */
     const int32_t *weights;         /* [num_weights*nobjs] */
     const int32_t *min_weight;      /* [num_nodes] or NULL */
+    const uint64_t *node_state;     /* [num_nodes*state_words] or NULL */
+    int32_t state_words;
+    int32_t reserved;               /* must be 0 */
 } pmdd_dd;
 
 /* ------------------------------------------------------------------- options */
 typedef struct pmdd_options {
     int32_t method;           /* 1 = top-down, 3 = dynamic layer cutset (coupled) */
     int32_t problem_type;     /* 1 knapsack, 2 set packing, 3 TSP */
-    int32_t state_dominance;  /* > 0: knapsack label pruning (method 1, problem 1) */
+    int32_t state_dominance;  /* > 0: label pruning between nodes of a top-down layer
+                                 (problem 1 by min_weight, problem 2 by state subsets;
+                                 methods 1 and 3; ignored for problem 3) */
     int32_t maximization;     /* must be 1 (the reference's main always maximises) */
     int64_t max_cand;         /* candidate points per expansion pass (--max-cand, 20M) */
     int64_t max_prod;         /* pair products per coupling pass (--max-prod, 625K) */

@@ -46,7 +46,8 @@ def lib():
         for name in ("oracle_topdown",):
             getattr(_lib, name).argtypes = [ctypes.c_void_p, ctypes.c_int, P(P(ctypes.c_int32)), P(ctypes.c_int64),
                                             P(OracleStats)]
-        _lib.oracle_coupled.argtypes = [ctypes.c_void_p, P(P(ctypes.c_int32)), P(ctypes.c_int64), P(OracleStats)]
+        _lib.oracle_coupled.argtypes = [ctypes.c_void_p, ctypes.c_int, P(P(ctypes.c_int32)), P(ctypes.c_int64),
+                                        P(OracleStats)]
         _lib.oracle_bottomup.argtypes = [ctypes.c_void_p, P(P(ctypes.c_int32)), P(ctypes.c_int64)]
         _lib.oracle_nd_keep.argtypes = [P(ctypes.c_int32), ctypes.c_int64, ctypes.c_int, P(ctypes.c_uint8)]
         _lib.oracle_free.argtypes = [ctypes.c_void_p]
@@ -76,7 +77,8 @@ def enumerate(dd, method: int = 1, state_dominance: int = 0, stats: dict | None 
     elif method == 2:
         rc = lib().oracle_bottomup(ctypes.addressof(view), ctypes.byref(out), ctypes.byref(n))
     elif method == 3:
-        rc = lib().oracle_coupled(ctypes.addressof(view), ctypes.byref(out), ctypes.byref(n), ctypes.byref(st))
+        rc = lib().oracle_coupled(ctypes.addressof(view), state_dominance, ctypes.byref(out), ctypes.byref(n),
+                                  ctypes.byref(st))
     else:
         raise ValueError("method must be 1, 2 or 3")
     if rc != 0:
@@ -130,3 +132,46 @@ def run_ref(path: str, problem_type: int, method: int, nobjs: int, threads: int 
             stats = json.loads(f.readline())
     pts = np.array(rows, dtype=np.int64).reshape(-1, nobjs)
     return {"frontier": pts, "stdout": p.stdout.splitlines(), "stats": stats}
+
+
+def write_flat_dd(dd, path: str) -> None:
+    """Writes a pmdd_b200.DecisionDiagram in the file layout oracle/ref_harness.cpp reads."""
+    v = dd.view
+    a = dd.arrays()
+    minw = a["min_weight"]
+    st = a["node_state"]
+    hdr = np.array([0x46444450, v.nobjs, v.num_layers, v.num_nodes, v.num_arcs, v.num_weights,
+                    1 if minw is not None else 0, v.state_words if st is not None else 0], dtype="<i4")
+    with open(path, "wb") as f:
+        f.write(hdr.tobytes())
+        for k in ("layer_offsets", "in_arc_offsets", "arc_src", "arc_weight", "weights"):
+            f.write(np.ascontiguousarray(a[k], dtype="<i4").tobytes())
+        if minw is not None:
+            f.write(np.ascontiguousarray(minw, dtype="<i4").tobytes())
+        if st is not None:
+            f.write(np.ascontiguousarray(st, dtype="<u8").tobytes())
+
+
+def harness_binary(nobjs: int) -> str:
+    return os.path.join(REF_DIR, f"ref_harness_nobjs{nobjs}")
+
+
+def have_harness(nobjs: int) -> bool:
+    return os.path.exists(harness_binary(nobjs))
+
+
+def run_harness(dd, problem_type: int, method: int, state_dominance: int = 0, timeout: float = 600.0) -> dict:
+    """The reference's CPU enumeration (methods 1 and 3, with its state-dominance passes)
+    run on this DD in this project's node numbering; returns its counters and frontier."""
+    nobjs = dd.view.nobjs
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "dd.bin")
+        write_flat_dd(dd, path)
+        cmd = [harness_binary(nobjs), path, str(problem_type), str(method), str(state_dominance)]
+        p = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout)
+    if p.returncode != 0:
+        raise RuntimeError(f"reference harness failed: {' '.join(cmd)}\n{p.stdout}\n{p.stderr}")
+    lines = p.stdout.splitlines()
+    stats = json.loads(lines[0])
+    rows = [list(map(int, line.split(","))) for line in lines[1:] if line.strip()]
+    return {"frontier": np.array(rows, dtype=np.int64).reshape(-1, nobjs), "stats": stats}

@@ -25,6 +25,10 @@
  *                       ParetoFrontier::convolute (pareto_frontier.hpp:353-365)
  *   knapsack state dominance
  *                       filter_dominance_knapsack_cpu  src/pmdd/enum/cpu/dominance.cpp:24-86
+ *   set-packing state dominance
+ *                       filter_dominance_setpacking_cpu  src/pmdd/enum/cpu/dominance.cpp:88-173
+ *                       (applied on top-down layers by methods 1 and 3,
+ *                       src/pmdd/enum/cpu/enum.cpp:43-49 and :275-285)
  *   oracle_nd_keep      the GPU filter's keep rule dominates_or_tie_before
  *                       src/pmdd/enum/gpu/dominance_utils.cuh:10-23 (first duplicate kept)
  *
@@ -227,6 +231,108 @@ static int64_t knapsack_state_dominance(const pmdd_dd *dd, int l, front_t *fr) {
     return removed;
 }
 
+/* Drops the labels of node n1 that a label of node n2 weakly dominates (>= on every
+ * objective); returns how many. */
+static int64_t drop_dominated_labels(front_t *fr, int32_t n1, int32_t n2, int d) {
+    int64_t w = 0, dropped = 0;
+    for (int64_t s1 = 0; s1 < fr[n1].n; ++s1) {
+        const int32_t *x = fr[n1].pts + s1 * d;
+        int dom = 0;
+        for (int64_t s2 = 0; s2 < fr[n2].n && !dom; ++s2) {
+            const int32_t *y = fr[n2].pts + s2 * d;
+            dom = 1;
+            for (int o = 0; o < d && dom; ++o) dom = (y[o] >= x[o]);
+        }
+        if (dom) {
+            ++dropped;
+            continue;
+        }
+        if (w != s1) memcpy(fr[n1].pts + w * d, x, sizeof(int32_t) * d);
+        ++w;
+    }
+    fr[n1].n = w;
+    return dropped;
+}
+
+static int lowest_vertex(const uint64_t *s, int W) {
+    for (int w = 0; w < W; ++w)
+        if (s[w]) return w * 64 + __builtin_ctzll(s[w]);
+    return -1;
+}
+
+/* filter_dominance_setpacking_cpu (src/pmdd/enum/cpu/dominance.cpp:88-173) on layer l:
+ * the layer's nodes (labels or not) are bucketed by state size, buckets 0 ..
+ * num_layers-2, each in layer order.  For a bucket b1 (b1 < num_layers-2) holding two or
+ * more nodes, only the next non-empty bucket b2 is searched: each node of b1 takes the
+ * first node of b2 that has the same lowest vertex, is not its single-parent sibling
+ * through a different arc type, and whose state contains the node's state, and loses
+ * the labels that a label of that node weakly dominates.  A node is only compared with
+ * nodes of larger buckets, which are pruned later, so every comparison sees the labels
+ * as they were before the pass. */
+static int64_t setpacking_state_dominance(const pmdd_dd *dd, int l, front_t *fr) {
+    const int d = dd->nobjs, W = dd->state_words, nb = dd->num_layers - 1;
+    const int32_t b = dd->layer_offsets[l], e = dd->layer_offsets[l + 1];
+    const int32_t cnt = e - b;
+    if (cnt <= 1 || dd->node_state == NULL || W <= 0) return 0;
+    int32_t *bucket = (int32_t *)malloc((size_t)cnt * sizeof(int32_t));
+    int32_t *start = (int32_t *)calloc((size_t)nb + 2, sizeof(int32_t));
+    int32_t *list = (int32_t *)malloc((size_t)cnt * sizeof(int32_t));
+    for (int32_t i = 0; i < cnt; ++i) {
+        const uint64_t *s = dd->node_state + (size_t)(b + i) * W;
+        int pc = 0;
+        for (int w = 0; w < W; ++w) pc += __builtin_popcountll(s[w]);
+        bucket[i] = pc < nb ? pc : nb; /* sizes >= nb take no part */
+        start[bucket[i] + 1]++;
+    }
+    for (int k = 0; k <= nb; ++k) start[k + 1] += start[k];
+    {
+        int32_t *fill = (int32_t *)malloc(((size_t)nb + 1) * sizeof(int32_t));
+        memcpy(fill, start, ((size_t)nb + 1) * sizeof(int32_t));
+        for (int32_t i = 0; i < cnt; ++i) list[fill[bucket[i]]++] = i; /* layer order within a bucket */
+        free(fill);
+    }
+    int64_t removed = 0;
+    for (int b1 = 0; b1 + 1 < nb; ++b1) {
+        if (start[b1 + 1] - start[b1] <= 1) continue;
+        int b2 = b1 + 1;
+        while (b2 < nb && start[b2 + 1] == start[b2]) ++b2;
+        if (b2 >= nb) continue;
+        for (int32_t p = start[b1]; p < start[b1 + 1]; ++p) {
+            const int32_t n1 = b + list[p];
+            const uint64_t *s1 = dd->node_state + (size_t)n1 * W;
+            const int32_t a1 = dd->in_arc_offsets[n1 + 1] - dd->in_arc_offsets[n1] == 1 ? dd->in_arc_offsets[n1] : -1;
+            for (int32_t q = start[b2]; q < start[b2 + 1]; ++q) {
+                const int32_t n2 = b + list[q];
+                const uint64_t *s2 = dd->node_state + (size_t)n2 * W;
+                if (lowest_vertex(s1, W) != lowest_vertex(s2, W)) continue;
+                const int32_t a2 =
+                    dd->in_arc_offsets[n2 + 1] - dd->in_arc_offsets[n2] == 1 ? dd->in_arc_offsets[n2] : -1;
+                if (a1 >= 0 && a2 >= 0 && dd->arc_src[a1] == dd->arc_src[a2] &&
+                    (dd->arc_weight[a1] != 0) != (dd->arc_weight[a2] != 0))
+                    continue;
+                int subset = 1;
+                for (int w = 0; w < W && subset; ++w) subset = (s1[w] & ~s2[w]) == 0;
+                if (!subset) continue;
+                removed += drop_dominated_labels(fr, n1, n2, d);
+                break;
+            }
+        }
+    }
+    free(bucket);
+    free(start);
+    free(list);
+    return removed;
+}
+
+/* filter_dominance_cpu (src/pmdd/enum/cpu/dominance.cpp:12-22) dispatches on the problem
+ * type; here the DD says which: knapsack BDDs carry min_weight, set-packing BDDs their
+ * node states, TSP MDDs neither (no state dominance, as in the reference). */
+static int64_t layer_state_dominance(const pmdd_dd *dd, int l, front_t *fr) {
+    if (dd->min_weight != NULL) return knapsack_state_dominance(dd, l, fr);
+    if (dd->node_state != NULL) return setpacking_state_dominance(dd, l, fr);
+    return 0;
+}
+
 static int validate(const pmdd_dd *dd) {
     if (!dd || dd->nobjs < 1 || dd->nobjs > 8 || dd->num_layers < 2) return PMDD_ERR_INVALID;
     if (dd->layer_offsets[1] != 1 || dd->layer_offsets[dd->num_layers] - dd->layer_offsets[dd->num_layers - 1] != 1)
@@ -275,7 +381,7 @@ int oracle_topdown(const pmdd_dd *dd, int state_dominance, int32_t **out, int64_
             }
         }
         if (state_dominance > 0) {
-            const int64_t r = knapsack_state_dominance(dd, l, fr);
+            const int64_t r = layer_state_dominance(dd, l, fr);
             if (st) st->dominance_filtered_total += r;
         }
         for (int32_t v = dd->layer_offsets[l]; v < dd->layer_offsets[l + 1]; ++v)
@@ -333,7 +439,7 @@ int oracle_bottomup(const pmdd_dd *dd, int32_t **out, int64_t *n_out) {
  * truncated per node as src/pmdd/enum/cpu/couple.cpp:15-48 does.  At the meeting
  * layer every node's top-down and bottom-up frontiers are convoluted into one
  * running frontier. */
-int oracle_coupled(const pmdd_dd *dd, int32_t **out, int64_t *n_out, oracle_stats *st) {
+int oracle_coupled(const pmdd_dd *dd, int state_dominance, int32_t **out, int64_t *n_out, oracle_stats *st) {
     int rc = validate(dd);
     if (rc) return rc;
     const int d = dd->nobjs;
@@ -368,8 +474,15 @@ int oracle_coupled(const pmdd_dd *dd, int32_t **out, int64_t *n_out, oracle_stat
                         return PMDD_ERR_OOM;
                 }
                 val_td += (int64_t)td[v].n * (oc.off[v + 1] - oc.off[v]);
-                if (st) st->survivors_total += td[v].n;
             }
+            /* state dominance after the layer value, before the survivor count
+             * (src/pmdd/enum/cpu/enum.cpp:266-285) */
+            if (state_dominance > 0) {
+                const int64_t r = layer_state_dominance(dd, l, td);
+                if (st) st->dominance_filtered_total += r;
+            }
+            for (int32_t v = dd->layer_offsets[l]; v < dd->layer_offsets[l + 1]; ++v)
+                if (st) st->survivors_total += td[v].n;
             for (int32_t u = dd->layer_offsets[l - 1]; u < dd->layer_offsets[l]; ++u) front_free(&td[u]);
         } else {
             --layer_bu;
@@ -405,6 +518,8 @@ int oracle_coupled(const pmdd_dd *dd, int32_t **out, int64_t *n_out, oracle_stat
                 return PMDD_ERR_OOM;
     }
     (void)sum_points;
+    /* the joined frontier counts as survivors too (src/pmdd/enum/cpu/enum.cpp:393-395) */
+    if (st) st->survivors_total += res.n;
     rc = take_result(&res, d, out, n_out);
     front_free(&res);
     for (int32_t v = 0; v < N; ++v) {

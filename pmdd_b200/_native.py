@@ -33,6 +33,9 @@ class PmddDD(ctypes.Structure):
         ("arc_weight", P_i32),
         ("weights", P_i32),
         ("min_weight", P_i32),
+        ("node_state", ctypes.POINTER(ctypes.c_uint64)),
+        ("state_words", c_i32),
+        ("reserved", c_i32),
     ]
 
 

@@ -484,6 +484,7 @@ pmdd_resident *pmdd_resident_upload(const pmdd_dd *dds, int32_t count, int32_t d
         I->blob.shrink_to_fit();
         I->blob_src = nullptr;
         std::vector<int32_t>().swap(I->sd_order);
+        std::vector<int32_t>().swap(I->sd_next);
     }
     return R.release();
 }
@@ -536,8 +537,14 @@ int pmdd_resident_enumerate(pmdd_resident *R, const pmdd_options *opts, pmdd_fro
         I->d_arc_w = T.d_arc_w;
         I->d_weights = T.d_weights;
         I->has_sd_order = T.has_sd_order;
+        I->sd_kind = T.sd_kind;
+        I->state_words = T.state_words;
         I->off_sdord = T.off_sdord;
+        I->off_sdnext = T.off_sdnext;
+        I->off_state = T.off_state;
         I->d_sd_order = T.d_sd_order;
+        I->d_sd_next = T.d_sd_next;
+        I->d_state = T.d_state;
         I->d_out_off = T.d_out_off;
         I->d_out_head = T.d_out_head;
         I->d_out_w = T.d_out_w;

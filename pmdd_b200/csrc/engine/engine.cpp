@@ -165,6 +165,49 @@ void pack_instance(const pmdd_dd &dd, const Instance &I, unsigned char *dst) {
     std::memcpy(dst + I.off_weights, dd.weights, sizeof(int32_t) * K * I.d);
     if (dd.min_weight) std::memcpy(dst + I.off_minw, dd.min_weight, sizeof(int32_t) * N);
     if (I.has_sd_order) std::memcpy(dst + I.off_sdord, I.sd_order.data(), sizeof(int32_t) * N);
+    if (I.sd_kind == 2) {
+        std::memcpy(dst + I.off_sdnext, I.sd_next.data(), sizeof(int32_t) * 2 * N);
+        std::memcpy(dst + I.off_state, dd.node_state, sizeof(uint64_t) * N * static_cast<size_t>(I.state_words));
+    }
+}
+
+// Set-packing state-dominance layout (src/pmdd/enum/cpu/dominance.cpp:88-173): per
+// layer, nodes bucketed by state size (bucket b < num_layers-1), ordered by (size, id);
+// a node whose bucket holds two or more nodes takes its partner from the next non-empty
+// bucket only.  Fills I->sd_order and I->sd_next.
+static void setpacking_sd_layout(const pmdd_dd &dd, Instance *I) {
+    const int32_t N = dd.num_nodes, W = dd.state_words, nb = dd.num_layers - 1;
+    I->sd_order.assign(N, 0);
+    I->sd_next.assign(2 * static_cast<size_t>(N), 0);
+    std::vector<int32_t> pc, first(nb + 1);
+    for (int l = 0; l < dd.num_layers; ++l) {
+        const int32_t b = dd.layer_offsets[l], e = dd.layer_offsets[l + 1], cnt = e - b;
+        pc.assign(cnt, 0);
+        for (int32_t i = 0; i < cnt; ++i) {
+            const uint64_t *s = dd.node_state + static_cast<size_t>(b + i) * W;
+            for (int32_t w = 0; w < W; ++w) pc[i] += __builtin_popcountll(s[w]);
+        }
+        int32_t *ord = I->sd_order.data() + b;
+        for (int32_t i = 0; i < cnt; ++i) ord[i] = i;
+        std::stable_sort(ord, ord + cnt, [&pc](int32_t x, int32_t y) { return pc[x] < pc[y]; });
+        // first[k] = first order position with size >= k (sizes >= nb take no part)
+        int32_t p = 0;
+        for (int32_t k = 0; k <= nb; ++k) {
+            while (p < cnt && pc[ord[p]] < k) ++p;
+            first[k] = p;
+        }
+        int32_t *nx = I->sd_next.data() + 2 * static_cast<size_t>(b);
+        for (int32_t k = 0; k + 1 < nb; ++k) {
+            if (first[k + 1] - first[k] < 2) continue;
+            int32_t k2 = k + 1;
+            while (k2 < nb && first[k2 + 1] == first[k2]) ++k2;
+            if (k2 >= nb) continue;
+            for (int32_t q = first[k]; q < first[k + 1]; ++q) {
+                nx[2 * q] = first[k2];
+                nx[2 * q + 1] = first[k2 + 1];
+            }
+        }
+    }
 }
 
 int prepare_instance(const pmdd_dd &dd, const pmdd_options &o, uint64_t id, Instance *I, std::string *err,
@@ -238,9 +281,20 @@ int prepare_instance(const pmdd_dd &dd, const pmdd_options &o, uint64_t id, Inst
     const bool has_minw = dd.min_weight != nullptr;
     I->off_minw = has_minw ? off : 0;
     if (has_minw) off = align256(off + sizeof(int32_t) * static_cast<size_t>(N));
-    I->has_sd_order = has_minw && (with_out_csr || (o.state_dominance > 0 && o.problem_type == 1 && o.method == 1));
-    I->off_sdord = 0;
-    if (I->has_sd_order) {
+    const bool has_state = dd.node_state != nullptr && dd.state_words > 0;
+    if (dd.node_state != nullptr && (dd.state_words <= 0 || dd.state_words > (1 << 20)))
+        return bad("state_words out of range");
+    // state-dominance data: by the requested problem type, or by what the DD carries for
+    // resident sets (which serve any options)
+    int sd_kind = 0;
+    if (o.problem_type == 1 && has_minw) sd_kind = 1;
+    else if (o.problem_type == 2 && has_state) sd_kind = 2;
+    else if (with_out_csr) sd_kind = has_minw ? 1 : (has_state ? 2 : 0);
+    I->sd_kind = (with_out_csr || o.state_dominance > 0) ? sd_kind : 0;
+    I->has_sd_order = I->sd_kind != 0;
+    I->off_sdord = I->off_sdnext = I->off_state = 0;
+    I->state_words = 0;
+    if (I->sd_kind == 1) {
         I->off_sdord = off;
         off = align256(off + sizeof(int32_t) * static_cast<size_t>(N));
         I->sd_order.resize(N);
@@ -251,6 +305,15 @@ int prepare_instance(const pmdd_dd &dd, const pmdd_options &o, uint64_t id, Inst
             const int32_t *mw = dd.min_weight + b;
             std::stable_sort(ord, ord + (e - b), [mw](int32_t x, int32_t y) { return mw[x] > mw[y]; });
         }
+    } else if (I->sd_kind == 2) {
+        I->state_words = dd.state_words;
+        I->off_sdord = off;
+        off = align256(off + sizeof(int32_t) * static_cast<size_t>(N));
+        I->off_sdnext = off;
+        off = align256(off + sizeof(int32_t) * 2 * static_cast<size_t>(N));
+        I->off_state = off;
+        off = align256(off + sizeof(uint64_t) * static_cast<size_t>(N) * static_cast<size_t>(dd.state_words));
+        setpacking_sd_layout(dd, I);
     }
     I->blob_bytes = off;
     if (pack) {
@@ -497,6 +560,8 @@ bool Engine::upload_dd(Instance &I) {
     I.d_arc_w = reinterpret_cast<const int32_t *>(I.dd + I.off_w);
     I.d_weights = reinterpret_cast<const int32_t *>(I.dd + I.off_weights);
     I.d_sd_order = I.has_sd_order ? reinterpret_cast<const int32_t *>(I.dd + I.off_sdord) : nullptr;
+    I.d_sd_next = I.sd_kind == 2 ? reinterpret_cast<const int32_t *>(I.dd + I.off_sdnext) : nullptr;
+    I.d_state = I.sd_kind == 2 ? reinterpret_cast<const uint64_t *>(I.dd + I.off_state) : nullptr;
     if (I.with_out_csr) {
         size_t off = I.blob_bytes;
         I.d_out_off = reinterpret_cast<int32_t *>(I.dd + off);
@@ -767,8 +832,9 @@ int Engine::step() {
         exps.swap(ordered);
     }
 
-    // knapsack state dominance on the layers that method-1 knapsack requests asking for it
-    // expand this step (jobs follow the expansion order, so (d, wide) groups stay contiguous)
+    // state dominance on the top-down layers that knapsack and set-packing requests asking
+    // for it expand this step, in both methods (jobs follow the expansion order, so
+    // (d, wide) groups stay contiguous)
     struct SdGroup {
         int d;
         bool wide;
@@ -785,7 +851,7 @@ int Engine::step() {
         for (size_t i = 0; i < exps.size(); ++i) {
             const ExpPlan &e = exps[i];
             const Instance &I = *e.I;
-            if (e.td && I.opts.method == 1 && I.opts.problem_type == 1 && I.opts.state_dominance > 0 &&
+            if (e.td && I.opts.state_dominance > 0 && I.sd_kind != 0 && I.sd_kind == I.opts.problem_type &&
                 I.d_sd_order != nullptr && I.nodes_in(e.nl) > 1) {
                 pick.push_back(i);
                 keep_bytes += align256(static_cast<size_t>(std::max<int64_t>(e.cand, 1)));
@@ -804,6 +870,10 @@ int Engine::step() {
                 dev::StateDomJob J;
                 std::memset(&J, 0, sizeof(J));
                 J.order = I.d_sd_order + I.layer_off[e.nl];
+                J.kind = I.sd_kind;
+                J.next = I.sd_kind == 2 ? I.d_sd_next + 2 * static_cast<size_t>(I.layer_off[e.nl]) : nullptr;
+                J.state = I.d_state;
+                J.state_words = I.state_words;
                 J.in_off = I.d_in_off;
                 J.arc_src = I.d_arc_src;
                 J.arc_w = I.d_arc_w;

@@ -84,12 +84,21 @@ struct Instance {
     std::vector<unsigned char> blob;    // packed DD arrays, uploaded at admission
     const unsigned char *blob_src = nullptr;  // packed arrays in the engine's pinned staging (instead of blob)
     size_t off_layer = 0, off_in = 0, off_src = 0, off_w = 0, off_weights = 0, off_minw = 0, blob_bytes = 0;
-    // knapsack state dominance: per layer, the layer-local node ids by min_weight
-    // descending (ties by id); packed into the blob at off_sdord when present
+    // state dominance (sd_kind 1: knapsack, 2: set packing; 0: none).  sd_order holds, per
+    // layer, the layer-local node ids by min_weight descending (kind 1) or by state size
+    // ascending (kind 2), ties by id; packed into the blob at off_sdord when present.
+    // Kind 2 also packs sd_next (per order position: the order range [begin, end) of the
+    // next non-empty state-size bucket, empty when the node takes no partner) at
+    // off_sdnext and the DD's node states (state_words words per node) at off_state.
     std::vector<int32_t> sd_order;
-    size_t off_sdord = 0;
+    std::vector<int32_t> sd_next;
+    size_t off_sdord = 0, off_sdnext = 0, off_state = 0;
+    int32_t state_words = 0;
+    int sd_kind = 0;
     bool has_sd_order = false;
     const int32_t *d_sd_order = nullptr;
+    const int32_t *d_sd_next = nullptr;
+    const uint64_t *d_state = nullptr;
     size_t dev_bytes = 0;               // blob + out-arc CSR
     // device DD
     unsigned char *dd = nullptr;
@@ -123,9 +132,9 @@ struct Instance {
 
 // Validates a flat DD and lays it out in an Instance (host side only).  The device copy
 // gets the bottom-up CSR when the method needs it or `with_out_csr` asks for it, and the
-// state-dominance node order when the DD has min_weight and either the options ask for
-// knapsack state dominance (method 1, problem type 1) or `with_out_csr` is set (resident
-// sets, which serve any options).  With
+// state-dominance data when the DD carries it (min_weight for knapsack, node_state for
+// set packing) and either the options ask for state dominance or `with_out_csr` is set
+// (resident sets, which serve any options).  With
 // `pack` the arrays are also copied into inst->blob; without it the caller packs them
 // later with pack_instance (e.g. straight into pinned staging memory).
 int prepare_instance(const pmdd_dd &dd, const pmdd_options &opts, uint64_t id, Instance *inst, std::string *err,

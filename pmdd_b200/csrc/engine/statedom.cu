@@ -1,5 +1,6 @@
-// Knapsack state dominance: one warp per node of every job's layer, in two launches
-// (mark against the labels as they were, then compact each node's slot in place).
+// State dominance (knapsack and set packing): one warp per node of every job's layer, in
+// two launches (mark against the labels as they were, then compact each node's slot in
+// place).
 #include <algorithm>
 
 #include "scan.cuh"
@@ -30,6 +31,13 @@ __device__ __forceinline__ int32_t single_in_arc(const StateDomJob &J, int32_t l
     return J.in_off[v + 1] - a == 1 ? a : -1;
 }
 
+// Lowest vertex of a set-packing state, or -1 for the empty state.
+__device__ __forceinline__ int first_vertex(const uint64_t *s, int W) {
+    for (int w = 0; w < W; ++w)
+        if (s[w] != 0) return w * 64 + __ffsll(static_cast<long long>(s[w])) - 1;
+    return -1;
+}
+
 template <int D, typename T>
 __global__ void __launch_bounds__(kSdThreads) sd_mark_kernel(const StateDomJob *jobs, const int64_t *node_bases,
                                                              int num_jobs, int64_t total) {
@@ -43,22 +51,6 @@ __global__ void __launch_bounds__(kSdThreads) sd_mark_kernel(const StateDomJob *
         const int32_t n1 = J.order[pos];
         const int32_t s1 = J.size[n1];
         if (s1 == 0) continue;
-        // the next two positions of the order whose node holds labels
-        int32_t part0 = -1, part1 = -1;
-        int found = 0;
-        for (int32_t p = pos + 1; p < J.num_nodes && found < 2; p += 32) {
-            const int32_t q = p + lane;
-            const bool act = q < J.num_nodes && J.size[J.order[q]] > 0;
-            unsigned m = __ballot_sync(kFull, act);
-            while (m != 0 && found < 2) {
-                const int b = __ffs(m) - 1;
-                m &= m - 1;
-                const int32_t node = J.order[p + b];
-                if (found == 0) part0 = node;
-                else part1 = node;
-                ++found;
-            }
-        }
         // siblings under one single parent (through different arc types) are not compared
         const int32_t a1 = single_in_arc(J, n1);
         auto skipped = [&](int32_t n2) -> bool {
@@ -66,8 +58,45 @@ __global__ void __launch_bounds__(kSdThreads) sd_mark_kernel(const StateDomJob *
             const int32_t a2 = single_in_arc(J, n2);
             return a2 >= 0 && J.arc_src[a1] == J.arc_src[a2] && ((J.arc_w[a1] != 0) != (J.arc_w[a2] != 0));
         };
-        if (skipped(part0)) part0 = -1;
-        if (skipped(part1)) part1 = -1;
+        int32_t part0 = -1, part1 = -1;
+        if (J.kind == 2) {
+            // first node of the partner bucket with the same lowest vertex, not a
+            // single-parent sibling, whose state contains n1's
+            const int32_t qb = J.next[2 * pos], qe = J.next[2 * pos + 1];
+            const int W = J.state_words;
+            const uint64_t *st1 = J.state + static_cast<int64_t>(J.node_base + n1) * W;
+            const int ff1 = first_vertex(st1, W);
+            for (int32_t p = qb; p < qe && part0 < 0; p += 32) {
+                const int32_t q = p + lane;
+                bool ok = false;
+                if (q < qe) {
+                    const int32_t n2 = J.order[q];
+                    const uint64_t *st2 = J.state + static_cast<int64_t>(J.node_base + n2) * W;
+                    ok = first_vertex(st2, W) == ff1 && !skipped(n2);
+                    for (int w = 0; w < W && ok; ++w) ok = (st1[w] & ~st2[w]) == 0;
+                }
+                const unsigned m = __ballot_sync(kFull, ok);
+                if (m != 0) part0 = J.order[p + __ffs(m) - 1];
+            }
+        } else {
+            // the next two positions of the order whose node holds labels
+            int found = 0;
+            for (int32_t p = pos + 1; p < J.num_nodes && found < 2; p += 32) {
+                const int32_t q = p + lane;
+                const bool act = q < J.num_nodes && J.size[J.order[q]] > 0;
+                unsigned m = __ballot_sync(kFull, act);
+                while (m != 0 && found < 2) {
+                    const int b = __ffs(m) - 1;
+                    m &= m - 1;
+                    const int32_t node = J.order[p + b];
+                    if (found == 0) part0 = node;
+                    else part1 = node;
+                    ++found;
+                }
+            }
+            if (skipped(part0)) part0 = -1;
+            if (skipped(part1)) part1 = -1;
+        }
         const T *P = static_cast<const T *>(J.pts);
         const int64_t o1 = J.off[n1];
         for (int32_t kb = 0; kb < s1; kb += 32) {

@@ -30,6 +30,8 @@ pmdd_dd FlatDD::view() const {
     v.arc_weight = arc_weight.data();
     v.weights = weights.data();
     v.min_weight = min_weight.empty() ? nullptr : min_weight.data();
+    v.node_state = node_state.empty() ? nullptr : node_state.data();
+    v.state_words = node_state.empty() ? 0 : state_words;
     return v;
 }
 
@@ -370,7 +372,9 @@ FlatDD build_indepset_bdd(const SetPackingData &sp, int nobjs) {
     for (int v = 0; v < n; ++v) active[v] = v;
     std::vector<int> counter(n, 0);
     std::vector<int> var_layer(n, -1);
+    std::vector<uint64_t> node_state;  // the states of every layer, in node order
     for (int l = 1; l <= n; ++l) {
+        for (const Bits &s : states) node_state.insert(node_state.end(), s.begin(), s.end());
         // min-in-state: vertex appearing in the fewest current states; ties go to the
         // first such entry of the active list, which shrinks by swap-with-last.
         for (int v : active) counter[v] = 0;
@@ -419,12 +423,15 @@ FlatDD build_indepset_bdd(const SetPackingData &sp, int nobjs) {
         states.swap(next);
     }
     if (L[n].size() != 1) throw std::runtime_error("independent-set BDD did not close to a single terminal");
+    node_state.insert(node_state.end(), states[0].begin(), states[0].end());
     std::vector<std::vector<int>> one_w(n, std::vector<int>(nobjs, 0));
     for (int l = 0; l < n; ++l)
         for (int o = 0; o < nobjs; ++o) one_w[l][o] = sp.objs[o][var_layer[l]];
     FlatDD f = flatten_bdd(L, one_w, nobjs);
     f.problem_type = 2;
     f.info.problem_type = 2;
+    f.node_state.swap(node_state);
+    f.state_words = W;
     int64_t w, nn;
     layer_shape(L, &w, &nn);
     f.info.original_width = f.info.reduced_width = w;

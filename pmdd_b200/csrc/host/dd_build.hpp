@@ -21,6 +21,8 @@ struct FlatDD {
     std::vector<int32_t> arc_weight;      // A
     std::vector<int32_t> weights;         // K*d
     std::vector<int32_t> min_weight;      // N (knapsack only)
+    std::vector<uint64_t> node_state;     // N*state_words (set packing only)
+    int32_t state_words = 0;
     pmdd_dd_info info{};
 
     int32_t num_layers() const { return static_cast<int32_t>(layer_offsets.size()) - 1; }

@@ -93,6 +93,8 @@ class DecisionDiagram:
             "arc_weight": arr(v.arc_weight, v.num_arcs),
             "weights": arr(v.weights, v.num_weights * v.nobjs).reshape(v.num_weights, v.nobjs),
             "min_weight": arr(v.min_weight, v.num_nodes) if v.min_weight else None,
+            "node_state": (np.ctypeslib.as_array(v.node_state, shape=(v.num_nodes, v.state_words)).copy()
+                           if v.node_state and v.state_words > 0 else None),
         }
 
     def close(self):

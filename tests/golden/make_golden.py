@@ -8,7 +8,11 @@ committed, so the tests never need them):
 
 For every fixture instance this writes
     <name>.dat           the instance (reference text format)
-    <name>.json          the reference run's structure stats and solution counts
+    <name>.json          the reference run's structure stats and solution counts, and for
+                         knapsack and set packing the counters of the reference's CPU
+                         enumeration run on this project's DD numbering ("same_numbering",
+                         methods 1 and 3 with and without state dominance; needs
+                         `make -C oracle harness`)
     <name>.m<k>.csv      the reference frontier for method k, sorted ascending
 Instances are seeded synthetic ones from pmdd_b200.instances plus a few files of
 the reference's own data/ directory (named ref_*).  The 5-objective 15-city TSP files
@@ -106,6 +110,22 @@ def record(name, path, problem_type, nobjs, methods):
             "work_frontier_survivors_total": s["work"]["work_frontier_survivors_total"],
             "dominance_filtered_total": s["dominance"]["dominance_filtered_total"],
         }
+    if problem_type in (1, 2) and oracle.have_harness(nobjs):
+        # the reference's CPU enumeration on this project's DD numbering (oracle/ref_harness.cpp):
+        # counters of methods 1 and 3 with and without state dominance, comparable one to one
+        from pmdd_b200 import DecisionDiagram
+
+        dd = DecisionDiagram.from_file(path, problem_type, nobjs)
+        runs = {}
+        for m in (1, 3):
+            for sd in (0, 1):
+                r = oracle.run_harness(dd, problem_type, m, sd)
+                ref_m = str(m) if str(m) in out["methods"] else None
+                if ref_m is not None:
+                    assert oracle.sorted_set(r["frontier"]).tolist() == oracle.sorted_set(
+                        oracle.run_ref(path, problem_type, m, nobjs)["frontier"]).tolist()
+                runs[f"m{m}_sd{sd}"] = r["stats"]
+        out["same_numbering"] = runs
     with open(os.path.join(HERE, f"{name}.json"), "w") as f:
         json.dump(out, f, indent=1)
     print(name, {m: out["methods"][m]["num_solutions"] for m in out["methods"]})

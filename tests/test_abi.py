@@ -45,8 +45,8 @@ def test_python_bindings_cover_headers():
 
 
 def test_struct_sizes_match_c_layout():
-    # pmdd_dd: 5 int32 + pad + 6 pointers; pmdd_options: 4 int32 + 2 int64 + 2 int32
-    assert ctypes.sizeof(_native.PmddDD) == 5 * 4 + 4 + 6 * 8
+    # pmdd_dd: 5 int32 + pad + 7 pointers + 2 int32; pmdd_options: 4 int32 + 2 int64 + 2 int32
+    assert ctypes.sizeof(_native.PmddDD) == 5 * 4 + 4 + 7 * 8 + 2 * 4
     assert ctypes.sizeof(_native.PmddOptions) == 40
     assert ctypes.sizeof(_native.PmddFrontier) == 24
 

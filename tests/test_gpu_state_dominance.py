@@ -1,10 +1,16 @@
-"""Knapsack state dominance on the GPU (method 1, problem type 1, state_dominance > 0).
+"""State dominance on the GPU (state_dominance > 0; knapsack and set packing; methods 1
+and 3).
 
-The reference prunes, after every top-down layer, the labels of a node that a label of
-one of the next two nodes in min_weight order weakly dominates
-(src/pmdd/enum/gpu/topdown.cu:256-521).  The frontier does not change; the labels
-removed, the candidates of later layers and the survivors do.  Bar: the frontier and all
-three counts equal to the reference run (golden fixtures) and to the oracle.
+After every top-down layer the reference prunes the labels of a node that a label of a
+partner node weakly dominates: for knapsack one of the next two nodes in min_weight
+order (src/pmdd/enum/gpu/topdown.cu:256-521, src/pmdd/enum/cpu/dominance.cpp:24-86), for
+set packing the first node of the next non-empty state-size bucket whose state contains
+the node's (src/pmdd/enum/cpu/dominance.cpp:88-173); its CPU coupled method does the same
+on the top-down side (src/pmdd/enum/cpu/enum.cpp:275-285).  The frontier does not
+change; the labels removed, the candidates of later layers and the survivors do.  Bar:
+the frontier and the counts equal to the reference's runs (golden fixtures: the
+reference binary for knapsack method 1, the reference's enumeration on the same DD
+numbering for everything else) and to the oracle.
 """
 import itertools
 
@@ -80,13 +86,95 @@ def test_state_dominance_in_a_batch_and_resident():
         res.close()
 
 
-@pytest.mark.parametrize("ptype,method", [(1, 3), (2, 1), (3, 1)])
-def test_state_dominance_is_a_no_op_elsewhere(ptype, method):
-    """Like the reference's GPU path: only method 1 on knapsack prunes states."""
-    text = {1: instances.knapsack_text(20, 3, 7), 2: instances.setpacking_text(40, 12, 3, 7),
-            3: instances.tsp_text(7, 3, 7)}[ptype]
-    dd = P.DecisionDiagram.from_text(text, ptype, 3)
+@pytest.mark.parametrize("method", (1, 3))
+def test_state_dominance_is_a_no_op_for_tsp(method):
+    """Problem type 3 has no state dominance, as in the reference (dominance.cpp:12-22)."""
+    dd = P.DecisionDiagram.from_text(instances.tsp_text(7, 3, 7), 3, 3)
     st = {}
     got = P.enumerate_dd(dd, method=method, state_dominance=1, stats=st)
     assert same_set(got, oracle.enumerate(dd, method))
     assert st["dominance_filtered_total"] == 0
+
+
+NUMBERED = [c for c in golden_cases() if "same_numbering" in c]
+
+
+@pytest.mark.parametrize("rec", NUMBERED, ids=[c["name"] for c in NUMBERED])
+def test_same_numbering_state_dominance(rec):
+    """Methods 1 and 3 with state dominance against the reference's enumeration on the
+    same DD numbering.  Method 3 picks its cutset by the GPU driver's rule, so its label
+    count is compared where the cutset layer is the CPU run's."""
+    dd = P.DecisionDiagram.from_file(rec["dat"], rec["problem_type"], rec["nobjs"])
+    want_pts = golden_frontier(rec, 1 if "1" in rec["methods"] else 3)
+    for m in (1, 3):
+        want = rec["same_numbering"][f"m{m}_sd1"]
+        st = {}
+        got = P.enumerate_dd(dd, method=m, state_dominance=1, stats=st)
+        assert same_set(got, want_pts), m
+        if m == 1:
+            assert st["dominance_filtered_total"] == want["dominance_filtered_total"]
+            assert st["work_candidates_total"] == want["work_candidates_total"]
+            assert st["work_frontier_survivors_total"] == want["work_frontier_survivors_total"]
+        elif st["layer_coupling"] == want["layer_coupling"]:
+            assert st["dominance_filtered_total"] == want["dominance_filtered_total"]
+
+
+def test_same_numbering_method3_cases_compare_counts():
+    """Enough method-3 fixtures share the CPU run's cutset layer for the count check above
+    to bite, with labels actually removed."""
+    hits = 0
+    for rec in NUMBERED:
+        want = rec["same_numbering"]["m3_sd1"]
+        if want["dominance_filtered_total"] == 0:
+            continue
+        dd = P.DecisionDiagram.from_file(rec["dat"], rec["problem_type"], rec["nobjs"])
+        st = {}
+        P.enumerate_dd(dd, method=3, state_dominance=1, stats=st)
+        if st["layer_coupling"] == want["layer_coupling"]:
+            assert st["dominance_filtered_total"] == want["dominance_filtered_total"], rec["name"]
+            hits += 1
+    assert hits >= 3, hits
+
+
+SP_SEEDED = [(d, n, m, instances.setpacking_text(n, max(4, n // 5), d, 700 + 7 * n + d)) for d, n, m in
+             itertools.product((2, 3, 5), (12, 40, 90), (10,))]
+
+
+@pytest.mark.parametrize("case", SP_SEEDED, ids=[f"sp{d}_n{n}" for d, n, _, _ in SP_SEEDED])
+def test_seeded_setpacking_state_dominance_against_oracle(case):
+    d, n, _, text = case
+    dd = P.DecisionDiagram.from_text(text, 2, d)
+    for method in (1, 3):
+        st, ost = {}, {}
+        got = P.enumerate_dd(dd, method=method, state_dominance=1, stats=st)
+        want = oracle.enumerate(dd, method, state_dominance=1, stats=ost)
+        assert same_set(got, want), method
+        if method == 1 or st["layer_coupling"] == ost["layer_coupling"]:
+            assert st["dominance_filtered_total"] == ost["dominance_filtered_total"], method
+        if method == 1:
+            assert st["work_candidates_total"] == ost["candidates_total"]
+            assert st["work_frontier_survivors_total"] == ost["survivors_total"]
+
+
+def test_setpacking_state_dominance_in_a_batch_and_resident():
+    dds = [P.DecisionDiagram.from_text(instances.setpacking_text(30 + i % 50, 12, 3, 1300 + i), 2, 3)
+           for i in range(24)]
+    want = []
+    for dd in dds:
+        ost = {}
+        want.append((oracle.enumerate(dd, 1, state_dominance=1, stats=ost), ost["dominance_filtered_total"]))
+    assert sum(r for _, r in want) > 0
+    st = {}
+    got = P.enumerate_batch(dds, method=1, state_dominance=1, stats=st)
+    for g, (w, _) in zip(got, want):
+        assert same_set(g, w)
+    assert st["dominance_filtered_total"] == sum(r for _, r in want)
+    res = P.ResidentSet(dds)
+    try:
+        st2 = {}
+        got2 = res.enumerate(method=1, state_dominance=1, stats=st2)
+        for g, (w, _) in zip(got2, want):
+            assert same_set(g, w)
+        assert st2["dominance_filtered_total"] == st["dominance_filtered_total"]
+    finally:
+        res.close()

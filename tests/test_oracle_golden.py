@@ -61,6 +61,35 @@ def test_oracle_knapsack_state_dominance_keeps_frontier(rec):
     assert st["survivors_total"] == want["work_frontier_survivors_total"]
 
 
+NUMBERED = [c for c in CASES if "same_numbering" in c]
+
+
+@pytest.mark.parametrize("rec", NUMBERED, ids=[c["name"] for c in NUMBERED])
+def test_oracle_counters_match_reference_on_same_numbering(rec):
+    """Every counter of methods 1 and 3, with and without state dominance (knapsack and
+    set packing), equals the reference's CPU enumeration run on the same DD numbering."""
+    dd = DecisionDiagram.from_file(rec["dat"], rec["problem_type"], rec["nobjs"])
+    for key, want in rec["same_numbering"].items():
+        m, sd = int(key[1]), int(key[-1])
+        st = {}
+        got = oracle.enumerate(dd, m, state_dominance=sd, stats=st)
+        assert len(got) == want["num_solutions"], key
+        assert np.array_equal(oracle.sorted_set(got), golden_frontier(rec, m if str(m) in rec["methods"] else 1)), key
+        assert st["dominance_filtered_total"] == want["dominance_filtered_total"], key
+        assert st["candidates_total"] == want["work_candidates_total"], key
+        assert st["survivors_total"] == want["work_frontier_survivors_total"], key
+        if m == 3:
+            assert st["layer_coupling"] == want["layer_coupling"], key
+            assert st["join_products_total"] == want["work_join_products_total"], key
+
+
+def test_same_numbering_fixtures_exercise_set_packing_state_dominance():
+    pruned = [c["name"] for c in NUMBERED
+              if c["problem_type"] == 2 and c["same_numbering"]["m1_sd1"]["dominance_filtered_total"] > 0
+              and c["same_numbering"]["m3_sd1"]["dominance_filtered_total"] > 0]
+    assert len(pruned) >= 3, pruned
+
+
 def test_nd_keep_rule_against_bruteforce():
     rng = np.random.default_rng(7)
     for trial in range(30):
