@@ -25,6 +25,7 @@ import argparse
 import concurrent.futures as cf
 import json
 import os
+import shutil
 import statistics
 import subprocess
 import sys
@@ -214,7 +215,12 @@ def single_instances(P, instances, device, with_ref):
 # --------------------------------------------------------------- served loop
 def served_loop(rate, n_req, seed, P, instances):
     """Poisson arrivals at `rate` req/s; KP (n~U{20..60}) / SP (n~U{60..100}) method 1 and
-    TSP (n~U{9..13}, method 3); latency = finish - arrival on the host clock."""
+    TSP (n~U{9..13}, method 3); latency = finish - arrival on the host clock.  Every
+    result's frontier CSV.gz and stats record are handed to the asynchronous writer as it
+    is polled (the reference's per-request output); the writer's tail after the last
+    result is reported beside the latencies."""
+    from pmdd_b200.writer import FrontierWriter
+
     rng = np.random.default_rng(seed)
     specs = []
     for i in range(n_req):
@@ -230,6 +236,8 @@ def served_loop(rate, n_req, seed, P, instances):
     gaps = rng.exponential(1.0 / rate, size=n_req)
     arrivals = np.cumsum(gaps)
     srv = P.Server()
+    outdir = tempfile.mkdtemp(prefix="pmdd_served_")
+    writer = FrontierWriter()
     t0 = time.perf_counter()
     t0_mono = time.monotonic()
     nxt = 0
@@ -254,11 +262,21 @@ def served_loop(rate, n_req, seed, P, instances):
             # finish_s is the engine's steady clock; arrival is relative to t0
             lat.append((r.finish_s - (t0_mono + arrivals[r.req_id])) * 1e3)
             finished += 1
+            rec = json.dumps({"request": int(r.req_id), "problem_type": specs[r.req_id][0],
+                              "method": specs[r.req_id][2], "num_solutions": int(len(r.frontier))})
+            writer.submit(r.frontier, os.path.join(outdir, f"r{r.req_id}.frontier.csv.gz"),
+                          os.path.join(outdir, "stats.jsonl"), rec)
     wall = time.perf_counter() - t0
     srv.close()
+    tw = time.perf_counter()
+    written = writer.flush()
+    tail_ms = (time.perf_counter() - tw) * 1e3
+    writer.close()
+    shutil.rmtree(outdir, ignore_errors=True)
     lat = np.array(lat)
     return {"rate_rps": rate, "requests": n_req, "p50_ms": float(np.percentile(lat, 50)),
-            "p99_ms": float(np.percentile(lat, 99)), "solves_per_s": n_req / wall}
+            "p99_ms": float(np.percentile(lat, 99)), "solves_per_s": n_req / wall,
+            "outputs_written": written, "writer_tail_ms": tail_ms}
 
 
 # ------------------------------------------------------------------- main

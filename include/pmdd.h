@@ -41,7 +41,8 @@ enum pmdd_status {
     PMDD_ERR_INTERNAL = 6,       /* device-side consistency check failed */
     PMDD_ERR_CANCELLED = 7,      /* request cancelled before completion */
     PMDD_ERR_NO_DEVICE = 8,      /* no CUDA device / extension not usable */
-    PMDD_ERR_RANGE = 9           /* objective sums exceed the supported integer range */
+    PMDD_ERR_RANGE = 9,          /* objective sums exceed the supported integer range */
+    PMDD_ERR_IO = 10             /* an output file could not be written (pmdd_host.h writers) */
 };
 
 /* ------------------------------------------------------------ the flat DD format

@@ -71,6 +71,38 @@ void pmdd_host_dd_free(pmdd_host_dd *h);
  * src/pmdd/enum/pareto_frontier.hpp:418-433). */
 void pmdd_sort_points_lex_ascending(int32_t *points, int64_t num_points, int32_t nobjs);
 
+/* ------------------------------------------------------------------ output writers
+ * The frontier CSV.gz of the reference (write_frontier_gzip_csv,
+ * src/pmdd/util/output_utils.cpp:87-152): one point per line, objectives as decimal
+ * integers separated by ',', '\n' line ends, gzip-compressed (here by zlib in process
+ * instead of a `gzip -c` child per file; the decompressed bytes are the reference's).
+ * `points` holds num_points*nobjs values of elem_bytes (4: int32, 8: int64) bytes, as in
+ * pmdd_frontier; with `sort` they are written ascending lexicographically, as the
+ * reference's main sorts before writing (src/pmdd/main.cpp:267).  The caller's array is
+ * not modified.  Returns PMDD_OK, PMDD_ERR_INVALID or PMDD_ERR_IO (text in err). */
+int pmdd_write_frontier_csv_gz(const void *points, int64_t num_points, int32_t nobjs, int32_t elem_bytes,
+                               int32_t sort, const char *path, char *err, size_t errlen);
+
+/* Asynchronous writer: a pool of `threads` writer threads (<= 0: up to 4) fed by a queue,
+ * so that a serving loop hands each result over and goes on.  No counterpart in the
+ * reference, which writes from the enumerating thread. */
+typedef struct pmdd_writer pmdd_writer;
+pmdd_writer *pmdd_writer_create(int32_t threads, char *err, size_t errlen);
+/* Queues one result: the frontier (copied now; sorted, then written to csv_gz_path as
+ * above) and/or one JSONL record (a single line without '\n', appended to jsonl_path as
+ * the reference's write_stats_jsonl appends, output_utils.cpp:154-300).  Either path may
+ * be NULL or empty, not both.  Returns PMDD_OK or PMDD_ERR_INVALID; never blocks on I/O. */
+int pmdd_writer_submit(pmdd_writer *w, const void *points, int64_t num_points, int32_t nobjs, int32_t elem_bytes,
+                       const char *csv_gz_path, const char *jsonl_path, const char *jsonl_record);
+/* Results queued or being written. */
+int64_t pmdd_writer_pending(pmdd_writer *w);
+/* Blocks until everything queued so far is written.  Returns the number of results
+ * that failed since the last flush (first failure's text in err) and, in *written, the
+ * number written. */
+int64_t pmdd_writer_flush(pmdd_writer *w, int64_t *written, char *err, size_t errlen);
+/* Writes what is queued, then stops the threads and frees the writer. */
+void pmdd_writer_destroy(pmdd_writer *w);
+
 #ifdef __cplusplus
 }
 #endif

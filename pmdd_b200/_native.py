@@ -130,6 +130,7 @@ STATUS_NAMES = {
     7: "CANCELLED",
     8: "NO_DEVICE",
     9: "RANGE",
+    10: "IO",
 }
 
 HOST_SYMBOLS = {
@@ -140,6 +141,14 @@ HOST_SYMBOLS = {
     "pmdd_host_dd_layer_sizes": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(c_i64), c_i32]),
     "pmdd_host_dd_free": (None, [ctypes.c_void_p]),
     "pmdd_sort_points_lex_ascending": (None, [P_i32, c_i64, c_i32]),
+    "pmdd_write_frontier_csv_gz": (ctypes.c_int, [ctypes.c_void_p, c_i64, c_i32, c_i32, c_i32, ctypes.c_char_p,
+                                                  ctypes.c_char_p, ctypes.c_size_t]),
+    "pmdd_writer_create": (ctypes.c_void_p, [c_i32, ctypes.c_char_p, ctypes.c_size_t]),
+    "pmdd_writer_submit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, c_i64, c_i32, c_i32, ctypes.c_char_p,
+                                          ctypes.c_char_p, ctypes.c_char_p]),
+    "pmdd_writer_pending": (c_i64, [ctypes.c_void_p]),
+    "pmdd_writer_flush": (c_i64, [ctypes.c_void_p, ctypes.POINTER(c_i64), ctypes.c_char_p, ctypes.c_size_t]),
+    "pmdd_writer_destroy": (None, [ctypes.c_void_p]),
 }
 
 GPU_SYMBOLS = {

@@ -3,15 +3,14 @@
 // Same positional arguments, options, defaults and messages as the reference CLI
 // (src/pmdd/util/cli_parser.cpp:181-488), the same three stdout lines
 // (src/pmdd/util/output_utils.cpp:302-374), the same gzip'd frontier CSV
-// (output_utils.cpp:87-152; ascending lexicographic order, "%d" values joined by ',')
+// (output_utils.cpp:87-152; ascending lexicographic order, "%d" values joined by ',',
+// written by pmdd_write_frontier_csv_gz of the host library)
 // and the same stats JSONL record (output_utils.cpp:154-300, schema_version 1).
 // The number of objectives comes from the program name (multiobj_nobjs3 -> 3), as the
 // reference's compile-time NOBJS does; PMDD_NOBJS overrides it.
 //
 // This binary drives the B200 engine; it has no CPU enumeration.  `--backend cpu`
 // (the reference's default) is rejected with a message naming --backend gpu.
-#include <zlib.h>
-
 #include <cctype>
 #include <cerrno>
 #include <chrono>
@@ -261,36 +260,6 @@ std::string json_escape(const std::string &v) {
     return s;
 }
 
-bool write_frontier_gz(const std::vector<int32_t> &pts, int d, const std::string &path, std::string *error) {
-    gzFile f = gzopen(path.c_str(), "wb");
-    if (!f) {
-        *error = "could not open output";
-        return false;
-    }
-    std::string line;
-    char num[24];
-    const size_t n = d > 0 ? pts.size() / d : 0;
-    for (size_t i = 0; i < n; ++i) {
-        line.clear();
-        for (int o = 0; o < d; ++o) {
-            if (o) line += ',';
-            std::snprintf(num, sizeof(num), "%d", pts[i * d + o]);
-            line += num;
-        }
-        line += '\n';
-        if (gzwrite(f, line.data(), static_cast<unsigned>(line.size())) != static_cast<int>(line.size())) {
-            gzclose(f);
-            *error = "failed while writing compressed frontier";
-            return false;
-        }
-    }
-    if (gzclose(f) != Z_OK) {
-        *error = "failed while writing compressed frontier";
-        return false;
-    }
-    return true;
-}
-
 struct RunTimes {
     double cpu_compile_s = 0, cpu_enumeration_s = 0, wall_compile_s = 0, wall_enumeration_s = 0;
 };
@@ -438,8 +407,9 @@ int main(int argc, char **argv) {
     pmdd_frontier_free(&fr);
     pmdd_sort_points_lex_ascending(pts.data(), num_solutions, nobjs);
     if (o.save_frontier) {
-        std::string e;
-        if (!write_frontier_gz(pts, nobjs, o.frontier_out_path, &e)) {
+        char e[256] = {0};
+        if (pmdd_write_frontier_csv_gz(pts.data(), num_solutions, nobjs, 4, 0, o.frontier_out_path.c_str(), e,
+                                       sizeof(e)) != PMDD_OK) {
             std::cout << "Error - failed to save frontier to '" << o.frontier_out_path << "': " << e << std::endl;
             return 1;
         }
