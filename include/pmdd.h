@@ -187,6 +187,37 @@ int pmdd_resident_enumerate(pmdd_resident *res, const pmdd_options *opts, pmdd_f
 int64_t pmdd_resident_bytes(const pmdd_resident *res);
 void pmdd_resident_free(pmdd_resident *res);
 
+/* 0/1 knapsack instance, one constraint (the reference's KnapsackInstance,
+ * src/pmdd/instances/knapsack_instance.cpp:17-47, with n_cons = 1). */
+typedef struct pmdd_knapsack {
+    int32_t n;                 /* items, >= 1 */
+    int32_t nobjs;             /* objectives used, 1..8 */
+    const int32_t *profits;    /* [nobjs][n], objective-major as in the file */
+    const int32_t *weights;    /* [n], >= 0 */
+    int32_t capacity;          /* 0 .. 2^24 */
+    int32_t reserved;          /* must be 0 */
+} pmdd_knapsack;
+
+/* Builds the exact knapsack BDDs of `count` instances on the device -- the DD the host
+ * constructor makes (pmdd_build_from_text, problem type 1: the reference's
+ * KnapsackBDDConstructor::generate_exact, two BDDAlg::reduce passes and
+ * update_node_weights, src/pmdd/bdd/knapsack_bdd.cpp:10-150, src/pmdd/main.cpp:120-153),
+ * array for array -- and keeps them resident like pmdd_resident_upload: only the item
+ * weights and profits cross the bus.  No counterpart in the reference, which builds its
+ * DDs on the CPU. */
+pmdd_resident *pmdd_resident_build_knapsack(const pmdd_knapsack *instances, int32_t count, int32_t device, char *err,
+                                            size_t errlen);
+
+/* Shape of DD i of a resident set: shape = {nobjs, num_layers, num_nodes, num_arcs,
+ * num_weights}; widths = {original width, original nodes, reduced width, reduced nodes}
+ * for device-built DDs, -1 otherwise (either pointer may be NULL). */
+int pmdd_resident_dd_shape(const pmdd_resident *res, int32_t i, int32_t *shape, int64_t *widths);
+/* Copies DD i's arrays (pmdd_dd layout, sized by pmdd_resident_dd_shape) to the host;
+ * min_weight may be NULL (it is filled only for DDs that carry it). */
+int pmdd_resident_dd_copy(pmdd_resident *res, int32_t i, int32_t *layer_offsets, int32_t *in_arc_offsets,
+                          int32_t *arc_src, int32_t *arc_weight, int32_t *weights, int32_t *min_weight, char *err,
+                          size_t errlen);
+
 /* ---------------------------------------------------------------- serving
  * A device-resident request loop with continuous batching: submitted requests are
  * admitted as slots and HBM budget free up; every admitted request advances one

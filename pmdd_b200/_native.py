@@ -39,6 +39,17 @@ class PmddDD(ctypes.Structure):
     ]
 
 
+class PmddKnapsack(ctypes.Structure):
+    _fields_ = [
+        ("n", c_i32),
+        ("nobjs", c_i32),
+        ("profits", P_i32),
+        ("weights", P_i32),
+        ("capacity", c_i32),
+        ("reserved", c_i32),
+    ]
+
+
 class PmddOptions(ctypes.Structure):
     _fields_ = [
         ("method", c_i32),
@@ -177,6 +188,11 @@ GPU_SYMBOLS = {
          ctypes.POINTER(PmddStats), ctypes.c_char_p, ctypes.c_size_t],
     ),
     "pmdd_resident_bytes": (c_i64, [ctypes.c_void_p]),
+    "pmdd_resident_build_knapsack": (ctypes.c_void_p, [ctypes.POINTER(PmddKnapsack), c_i32, c_i32, ctypes.c_char_p,
+                                                       ctypes.c_size_t]),
+    "pmdd_resident_dd_shape": (ctypes.c_int, [ctypes.c_void_p, c_i32, P_i32, ctypes.POINTER(c_i64)]),
+    "pmdd_resident_dd_copy": (ctypes.c_int, [ctypes.c_void_p, c_i32, P_i32, P_i32, P_i32, P_i32, P_i32, P_i32,
+                                             ctypes.c_char_p, ctypes.c_size_t]),
     "pmdd_resident_free": (None, [ctypes.c_void_p]),
     "pmdd_server_create": (ctypes.c_void_p, [c_i32, c_i64, c_i32, ctypes.c_char_p, ctypes.c_size_t]),
     "pmdd_server_submit": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(PmddDD), ctypes.POINTER(PmddOptions),

@@ -1,5 +1,8 @@
 // extern "C" boundary of libpmdd_gpu.so (declared in include/pmdd.h).
+#include <algorithm>
+#include <array>
 #include <atomic>
+#include <climits>
 #include <cstdlib>
 #include <cstring>
 #include <functional>
@@ -10,6 +13,7 @@
 #include <unordered_map>
 
 #include "engine.hpp"
+#include "kpbuild.cuh"
 #include "pareto.cuh"
 #include "pmdd.h"
 
@@ -441,6 +445,7 @@ struct pmdd_resident {
     uint64_t generation = 0;
     int64_t bytes = 0;
     std::vector<std::unique_ptr<pmdd::Instance>> tmpl;  // prepared requests whose DD stays on the device
+    std::vector<std::array<int64_t, 4>> widths;          // device-built DDs: original / reduced width and nodes
 };
 
 pmdd_resident *pmdd_resident_upload(const pmdd_dd *dds, int32_t count, int32_t device, char *err, size_t errlen) {
@@ -578,6 +583,240 @@ void pmdd_resident_free(pmdd_resident *R) {
             for (auto &I : R->tmpl) slot.engine->release_dd(*I);
     }
     delete R;
+}
+
+// ------------------------------------------------- knapsack BDDs built on the device
+namespace {
+constexpr int32_t kBuildMaxItems = 4096;
+constexpr int32_t kBuildMaxCap = 1 << 24;
+constexpr int64_t kBuildScratchBytes = static_cast<int64_t>(2) << 30;  // per chunk of instances
+}  // namespace
+
+pmdd_resident *pmdd_resident_build_knapsack(const pmdd_knapsack *ks, int32_t count, int32_t device, char *err,
+                                            size_t errlen) {
+    if (count < 0 || (count > 0 && !ks)) {
+        write_err(err, errlen, "invalid knapsack set");
+        return nullptr;
+    }
+    for (int32_t i = 0; i < count; ++i) {
+        const pmdd_knapsack &k = ks[i];
+        std::string why;
+        if (k.n < 1 || k.n > kBuildMaxItems) why = "n must be in 1..4096";
+        else if (k.nobjs < 1 || k.nobjs > 8) why = "nobjs must be in 1..8";
+        else if (!k.profits || !k.weights) why = "profits / weights pointer is NULL";
+        else if (k.capacity < 0 || k.capacity > kBuildMaxCap) why = "capacity must be in 0..2^24";
+        else
+            for (int32_t j = 0; j < k.n && why.empty(); ++j)
+                if (k.weights[j] < 0) why = "weights must be >= 0";
+        if (!why.empty()) {
+            write_err(err, errlen, "instance " + std::to_string(i) + ": " + why);
+            return nullptr;
+        }
+    }
+    std::unique_ptr<pmdd_resident> R(new pmdd_resident);
+    R->device = device;
+    DeviceSlot &slot = slot_for(device);
+    std::lock_guard<std::mutex> lk(slot.mu);
+    std::string msg;
+    if (ensure_engine(device, slot, &msg) != PMDD_OK) {
+        write_err(err, errlen, msg);
+        return nullptr;
+    }
+    R->generation = slot.generation;
+    pmdd::Engine &E = *slot.engine;
+    cudaStream_t st = E.stream();
+    std::vector<void *> temps;
+    auto give_up = [&](const std::string &why) -> pmdd_resident * {
+        cudaStreamSynchronize(st);
+        for (void *p : temps) E.release(p);
+        for (auto &I : R->tmpl)
+            if (I->dd) E.release_dd(*I);
+        write_err(err, errlen, why);
+        return nullptr;
+    };
+    auto dev_alloc = [&](size_t bytes) -> void * {
+        void *p = E.alloc(std::max<size_t>(bytes, 256));
+        if (p) temps.push_back(p);
+        return p;
+    };
+    // item weights and profits of every instance, one upload
+    std::vector<size_t> in_off(count + 1, 0);
+    for (int32_t i = 0; i < count; ++i) in_off[i + 1] = in_off[i] + static_cast<size_t>(ks[i].n) * (1 + ks[i].nobjs);
+    std::vector<int32_t> hin(std::max<size_t>(in_off[count], 1));
+    for (int32_t i = 0; i < count; ++i) {
+        std::memcpy(&hin[in_off[i]], ks[i].weights, sizeof(int32_t) * ks[i].n);
+        std::memcpy(&hin[in_off[i] + ks[i].n], ks[i].profits, sizeof(int32_t) * ks[i].n * ks[i].nobjs);
+    }
+    int32_t *d_in = static_cast<int32_t *>(dev_alloc(sizeof(int32_t) * hin.size()));
+    if (!d_in) return give_up("knapsack inputs do not fit the device memory budget");
+    if (cudaMemcpyAsync(d_in, hin.data(), sizeof(int32_t) * hin.size(), cudaMemcpyHostToDevice, st) != cudaSuccess)
+        return give_up("knapsack input upload failed");
+    auto scratch_bytes = [&](int32_t i) { return sizeof(int32_t) * pmdd::dev::kp_scratch_ints(ks[i].n, ks[i].capacity); };
+    for (int32_t i0 = 0; i0 < count;) {
+        int32_t i1 = i0;
+        int64_t acc = 0;
+        while (i1 < count && (i1 == i0 || acc + static_cast<int64_t>(scratch_bytes(i1)) <= kBuildScratchBytes)) {
+            acc += static_cast<int64_t>(scratch_bytes(i1)) + 256;
+            ++i1;
+        }
+        const int32_t m = i1 - i0;
+        std::vector<size_t> hdr_off(m + 1, 0), scr_off(m + 1, 0);
+        int max_layers = 0;
+        for (int32_t k = 0; k < m; ++k) {
+            const pmdd_knapsack &q = ks[i0 + k];
+            hdr_off[k + 1] = hdr_off[k] + 3 * (static_cast<size_t>(q.n) + 1) + 1;
+            scr_off[k + 1] = scr_off[k] + (scratch_bytes(i0 + k) + 255) / 256 * 64;  // ints, 256-byte aligned
+            max_layers = std::max(max_layers, q.n + 1);
+        }
+        int32_t *d_scr = static_cast<int32_t *>(dev_alloc(sizeof(int32_t) * scr_off[m]));
+        int32_t *d_hdr = static_cast<int32_t *>(dev_alloc(sizeof(int32_t) * hdr_off[m]));
+        auto *d_jobs = static_cast<pmdd::dev::KpBuildJob *>(dev_alloc(sizeof(pmdd::dev::KpBuildJob) * m));
+        if (!d_scr || !d_hdr || !d_jobs) return give_up("knapsack build scratch does not fit the device memory budget");
+        std::vector<pmdd::dev::KpBuildJob> jobs(m);
+        for (int32_t k = 0; k < m; ++k) {
+            const pmdd_knapsack &q = ks[i0 + k];
+            pmdd::dev::KpBuildJob &J = jobs[k];
+            std::memset(&J, 0, sizeof(J));
+            const int64_t S = static_cast<int64_t>(q.capacity) + 1, Lc = q.n + 1;
+            J.n = q.n;
+            J.cap = q.capacity;
+            J.nobjs = q.nobjs;
+            J.w = d_in + in_off[i0 + k];
+            J.profit = d_in + in_off[i0 + k] + q.n;
+            int32_t *base = d_scr + scr_off[k];
+            J.idx = base;
+            J.cls_new = base + Lc * S;
+            J.cls_c0 = base + 2 * Lc * S;
+            J.cls_c1 = base + 3 * Lc * S;
+            J.tmp = base + 4 * Lc * S;
+            int32_t *h = d_hdr + hdr_off[k];
+            J.width = h;
+            J.classes = h + Lc;
+            J.arcs_into = h + 2 * Lc;
+            J.err = h + 3 * Lc;
+        }
+        std::vector<int32_t> hhdr(hdr_off[m]);
+        if (cudaMemcpyAsync(d_jobs, jobs.data(), sizeof(jobs[0]) * m, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+            pmdd::dev::launch_kp_reduce(d_jobs, m, st) != cudaSuccess ||
+            cudaMemcpyAsync(hhdr.data(), d_hdr, sizeof(int32_t) * hhdr.size(), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess)
+            return give_up(std::string("knapsack build failed: ") + cudaGetErrorString(cudaGetLastError()));
+        E.count_launches(1);
+        for (int32_t k = 0; k < m; ++k) {
+            const pmdd_knapsack &q = ks[i0 + k];
+            const int32_t Lc = q.n + 1;
+            const int32_t *h = hhdr.data() + hdr_off[k];
+            if (h[3 * Lc] != 0) return give_up("knapsack build: inconsistent layer counts (internal)");
+            std::vector<int32_t> layer_off(Lc + 1, 0), arc_at(Lc + 1, 0);
+            int64_t ow = 0, on = 0, rw = 0, rn = 0;
+            // header: width[Lc] | classes[Lc] | arcs_into[Lc] | err
+            for (int32_t l = 0; l < Lc; ++l) {
+                layer_off[l + 1] = layer_off[l] + h[Lc + l];
+                arc_at[l + 1] = arc_at[l] + h[2 * Lc + l];
+                ow = std::max<int64_t>(ow, h[l]);
+                on += h[l];
+                rw = std::max<int64_t>(rw, h[Lc + l]);
+                rn += h[Lc + l];
+            }
+            // bound on |path sums| as prepare_instance computes it: a layer with a 1-arc adds
+            // its largest |profit|
+            int64_t bound = 0;
+            for (int32_t l = 0; l < q.n; ++l) {
+                if (q.weights[l] > q.capacity) continue;
+                int64_t mx = 0;
+                for (int o = 0; o < q.nobjs; ++o) mx = std::max<int64_t>(mx, std::llabs(static_cast<int64_t>(q.profits[o * q.n + l])));
+                bound += mx;
+            }
+            std::unique_ptr<pmdd::Instance> I(new pmdd::Instance);
+            pmdd_options_default(&I->opts);
+            I->opts.problem_type = 1;
+            I->id = static_cast<uint64_t>(i0 + k);
+            pmdd::layout_built_knapsack(I.get(), q.nobjs, bound > static_cast<int64_t>(INT32_MAX), layer_off, arc_at,
+                                        q.n + 1);
+            I->dd = static_cast<unsigned char *>(E.alloc(I->dev_bytes));
+            if (!I->dd) return give_up("built DD set does not fit the device memory budget");
+            pmdd::dev::KpBuildJob &J = jobs[k];
+            J.layer_offsets = reinterpret_cast<int32_t *>(I->dd + I->off_layer);
+            J.in_arc_offsets = reinterpret_cast<int32_t *>(I->dd + I->off_in);
+            J.arc_src = reinterpret_cast<int32_t *>(I->dd + I->off_src);
+            J.arc_weight = reinterpret_cast<int32_t *>(I->dd + I->off_w);
+            J.weights = reinterpret_cast<int32_t *>(I->dd + I->off_weights);
+            J.min_weight = reinterpret_cast<int32_t *>(I->dd + I->off_minw);
+            J.sd_order = reinterpret_cast<int32_t *>(I->dd + I->off_sdord);
+            R->bytes += static_cast<int64_t>(I->dev_bytes);
+            R->tmpl.push_back(std::move(I));
+            R->widths.push_back({ow, on, rw, rn});
+        }
+        if (cudaMemcpyAsync(d_jobs, jobs.data(), sizeof(jobs[0]) * m, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+            pmdd::dev::launch_kp_flatten(d_jobs, m, max_layers, st) != cudaSuccess)
+            return give_up(std::string("knapsack flatten failed: ") + cudaGetErrorString(cudaGetLastError()));
+        E.count_launches(1);
+        for (int32_t k = 0; k < m; ++k)
+            if (!E.bind_dd(*R->tmpl[i0 + k])) return give_up(E.ok() ? "out-arc CSR failed" : E.error());
+        if (cudaMemcpyAsync(hhdr.data(), d_hdr, sizeof(int32_t) * hhdr.size(), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess)
+            return give_up(std::string("knapsack build failed: ") + cudaGetErrorString(cudaGetLastError()));
+        for (int32_t k = 0; k < m; ++k)
+            if (hhdr[hdr_off[k] + 3 * (ks[i0 + k].n + 1)] != 0)
+                return give_up("knapsack build: min_weight order check failed (internal)");
+        E.release(d_scr);
+        E.release(d_hdr);
+        E.release(d_jobs);
+        temps.erase(std::remove_if(temps.begin(), temps.end(),
+                                   [&](void *p) { return p == d_scr || p == d_hdr || p == d_jobs; }),
+                    temps.end());
+        i0 = i1;
+    }
+    cudaStreamSynchronize(st);
+    for (void *p : temps) E.release(p);
+    return R.release();
+}
+
+int pmdd_resident_dd_shape(const pmdd_resident *R, int32_t i, int32_t *shape, int64_t *widths) {
+    if (!R || i < 0 || i >= static_cast<int32_t>(R->tmpl.size())) return PMDD_ERR_INVALID;
+    const pmdd::Instance &T = *R->tmpl[i];
+    if (shape) {
+        shape[0] = T.d;
+        shape[1] = T.L;
+        shape[2] = T.N;
+        shape[3] = T.A;
+        shape[4] = T.K;
+    }
+    if (widths)
+        for (int k = 0; k < 4; ++k) widths[k] = i < static_cast<int32_t>(R->widths.size()) ? R->widths[i][k] : -1;
+    return PMDD_OK;
+}
+
+int pmdd_resident_dd_copy(pmdd_resident *R, int32_t i, int32_t *layer_offsets, int32_t *in_arc_offsets,
+                          int32_t *arc_src, int32_t *arc_weight, int32_t *weights, int32_t *min_weight, char *err,
+                          size_t errlen) {
+    if (!R || i < 0 || i >= static_cast<int32_t>(R->tmpl.size()) || !layer_offsets || !in_arc_offsets ||
+        !weights || ((!arc_src || !arc_weight) && R->tmpl[i]->A > 0)) {
+        write_err(err, errlen, "invalid resident DD copy");
+        return PMDD_ERR_INVALID;
+    }
+    DeviceSlot &slot = slot_for(R->device);
+    std::lock_guard<std::mutex> lk(slot.mu);
+    if (!slot.engine || !slot.engine->ok() || slot.generation != R->generation) {
+        write_err(err, errlen, "resident DD set was invalidated by an engine restart");
+        return PMDD_ERR_CUDA;
+    }
+    const pmdd::Instance &T = *R->tmpl[i];
+    cudaStream_t st = slot.engine->stream();
+    auto get = [&](void *dst, size_t off, size_t bytes) {
+        return bytes == 0 || cudaMemcpyAsync(dst, T.dd + off, bytes, cudaMemcpyDeviceToHost, st) == cudaSuccess;
+    };
+    bool ok = get(layer_offsets, T.off_layer, sizeof(int32_t) * (static_cast<size_t>(T.L) + 1)) &&
+              get(in_arc_offsets, T.off_in, sizeof(int32_t) * (static_cast<size_t>(T.N) + 1)) &&
+              get(arc_src, T.off_src, sizeof(int32_t) * static_cast<size_t>(T.A)) &&
+              get(arc_weight, T.off_w, sizeof(int32_t) * static_cast<size_t>(T.A)) &&
+              get(weights, T.off_weights, sizeof(int32_t) * static_cast<size_t>(T.K) * T.d);
+    if (ok && min_weight && T.sd_kind == 1) ok = get(min_weight, T.off_minw, sizeof(int32_t) * static_cast<size_t>(T.N));
+    if (!ok || cudaStreamSynchronize(st) != cudaSuccess) {
+        write_err(err, errlen, std::string("CUDA error: ") + cudaGetErrorString(cudaGetLastError()));
+        return PMDD_ERR_CUDA;
+    }
+    return PMDD_OK;
 }
 
 // ------------------------------------------------------------------ serving

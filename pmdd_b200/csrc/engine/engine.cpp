@@ -337,6 +337,49 @@ int prepare_instance(const pmdd_dd &dd, const pmdd_options &o, uint64_t id, Inst
     return PMDD_OK;
 }
 
+void layout_built_knapsack(Instance *I, int d, bool wide, const std::vector<int32_t> &layer_off,
+                           const std::vector<int32_t> &arc_at_layer, int32_t K) {
+    const int32_t L = static_cast<int32_t>(layer_off.size()) - 1;
+    const int32_t N = layer_off.back(), A = arc_at_layer.back();
+    I->d = d;
+    I->wide = wide;
+    I->L = L;
+    I->N = N;
+    I->A = A;
+    I->K = K;
+    I->layer_off = layer_off;
+    I->arc_at_layer = arc_at_layer;
+    size_t off = 0;
+    I->off_layer = off;
+    off = align256(off + sizeof(int32_t) * (static_cast<size_t>(L) + 1));
+    I->off_in = off;
+    off = align256(off + sizeof(int32_t) * (static_cast<size_t>(N) + 1));
+    I->off_src = off;
+    off = align256(off + sizeof(int32_t) * static_cast<size_t>(A));
+    I->off_w = off;
+    off = align256(off + sizeof(int32_t) * static_cast<size_t>(A));
+    I->off_weights = off;
+    off = align256(off + sizeof(int32_t) * static_cast<size_t>(K) * d);
+    I->off_minw = off;
+    off = align256(off + sizeof(int32_t) * static_cast<size_t>(N));
+    I->sd_kind = 1;
+    I->has_sd_order = true;
+    I->off_sdord = off;
+    off = align256(off + sizeof(int32_t) * static_cast<size_t>(N));
+    I->blob_bytes = off;
+    I->with_out_csr = true;
+    size_t dev = off;
+    dev = align256(dev + sizeof(int32_t) * (static_cast<size_t>(N) + 1));
+    dev = align256(dev + sizeof(int32_t) * static_cast<size_t>(A));
+    dev = align256(dev + sizeof(int32_t) * static_cast<size_t>(A));
+    dev = align256(dev + sizeof(int32_t) * static_cast<size_t>(N));
+    I->dev_bytes = dev;
+    int64_t widest_arcs = 0;
+    for (int l = 0; l < L; ++l) widest_arcs = std::max<int64_t>(widest_arcs, arc_at_layer[l + 1] - arc_at_layer[l]);
+    I->est_bytes = static_cast<int64_t>(dev) + 8 * widest_arcs * static_cast<int64_t>(d * I->elem() + 16);
+    I->submit_s = now_s();
+}
+
 // ------------------------------------------------------------------ Engine
 Engine::Engine(int device, int64_t budget_bytes, int max_slots) : device_(device), max_slots_(max_slots) {
     const double init_t0 = now_s();
@@ -555,6 +598,10 @@ bool Engine::upload_dd(Instance &I) {
     if (!I.dd) return false;
     if (!cuda_ok(cudaMemcpyAsync(I.dd, I.blob_src ? I.blob_src : I.blob.data(), I.blob_bytes, cudaMemcpyHostToDevice, stream_), "DD upload"))
         return false;
+    return bind_dd(I);
+}
+
+bool Engine::bind_dd(Instance &I) {
     I.d_in_off = reinterpret_cast<const int32_t *>(I.dd + I.off_in);
     I.d_arc_src = reinterpret_cast<const int32_t *>(I.dd + I.off_src);
     I.d_arc_w = reinterpret_cast<const int32_t *>(I.dd + I.off_w);

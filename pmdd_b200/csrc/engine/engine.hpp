@@ -143,6 +143,13 @@ int prepare_instance(const pmdd_dd &dd, const pmdd_options &opts, uint64_t id, I
 // at the instance's offsets; the alignment gaps are left as they are).
 void pack_instance(const pmdd_dd &dd, const Instance &inst, unsigned char *dst);
 
+// Host metadata and blob layout of a knapsack BDD built on the device (kpbuild.cu): layer
+// offsets and the incoming-arc offsets at layer starts (both L+1), K weight rows; the
+// blob holds the pmdd_dd arrays, min_weight and the min_weight order, then the
+// bottom-up CSR.
+void layout_built_knapsack(Instance *I, int d, bool wide, const std::vector<int32_t> &layer_off,
+                           const std::vector<int32_t> &arc_at_layer, int32_t K);
+
 // Tuned oversized-path crossovers, (objectives, problem type) -> big_mark_min, from the
 // tuning file pmdd_b200.autotune writes (see Engine::mark_min_for); empty when absent.
 std::string default_tuning_path();
@@ -188,6 +195,9 @@ class Engine {
     // Device copy of a prepared request's DD (with the bottom-up CSR) that stays in
     // the arena until release_dd(); requests then share it via external_dd.
     bool upload_dd(Instance &I);
+    // Device pointers of a DD whose arrays are in I.dd (uploaded or built on the device),
+    // and its bottom-up CSR when the instance carries one.
+    bool bind_dd(Instance &I);
     void release_dd(Instance &I);
     // Pinned host memory for packing DD uploads (grow-only, kept across calls); nullptr
     // when it cannot be had.  Contents must stay untouched until the uploads that read

@@ -134,15 +134,70 @@ class ResidentSet:
             raise CudaEnumerationError(3, err.value.decode(errors="replace"))
         self._lib = lib
         self.device = device
+        self.count = n
+        self.problem_type = self.dds[0].problem_type if self.dds else 1
+
+    @classmethod
+    def from_knapsack(cls, instances: Iterable, device: int = 0) -> "ResidentSet":
+        """Knapsack BDDs built on the device (pmdd_resident_build_knapsack) from
+        (profits (nobjs, n), weights (n,), capacity) triples; only those arrays cross the bus."""
+        items = [(np.ascontiguousarray(p, dtype=np.int32), np.ascontiguousarray(w, dtype=np.int32), int(c))
+                 for p, w, c in instances]
+        n = len(items)
+        specs = (_native.PmddKnapsack * max(n, 1))()
+        P32 = ctypes.POINTER(ctypes.c_int32)
+        for i, (p, w, c) in enumerate(items):
+            if p.ndim != 2 or w.ndim != 1 or p.shape[1] != w.shape[0]:
+                raise ValueError(f"instance {i}: profits must be (nobjs, n) and weights (n,)")
+            specs[i] = _native.PmddKnapsack(w.shape[0], p.shape[0], p.ctypes.data_as(P32), w.ctypes.data_as(P32), c, 0)
+        lib = _native.gpu_lib()
+        err = ctypes.create_string_buffer(512)
+        self = cls.__new__(cls)
+        self.dds = []
+        self._lib = lib
+        self.device = device
+        self.count = n
+        self.problem_type = 1
+        self._h = lib.pmdd_resident_build_knapsack(specs, n, device, err, len(err))
+        if not self._h:
+            raise CudaEnumerationError(1, err.value.decode(errors="replace"))
+        return self
 
     @property
     def device_bytes(self) -> int:
         return self._lib.pmdd_resident_bytes(self._h)
 
+    def dd_info(self, i: int) -> dict:
+        shape = (ctypes.c_int32 * 5)()
+        widths = (ctypes.c_int64 * 4)()
+        if self._lib.pmdd_resident_dd_shape(self._h, i, shape, widths) != _native.PMDD_OK:
+            raise IndexError(i)
+        return {"nobjs": shape[0], "num_layers": shape[1], "num_nodes": shape[2], "num_arcs": shape[3],
+                "num_weights": shape[4], "original_width": widths[0], "original_num_nodes": widths[1],
+                "reduced_width": widths[2], "reduced_num_nodes": widths[3]}
+
+    def dd_arrays(self, i: int) -> dict:
+        """Host copy of DD i's flat arrays (same keys as DecisionDiagram.arrays)."""
+        info = self.dd_info(i)
+        d, L, N, A, K = (info[k] for k in ("nobjs", "num_layers", "num_nodes", "num_arcs", "num_weights"))
+        out = {"layer_offsets": np.zeros(L + 1, np.int32), "in_arc_offsets": np.zeros(N + 1, np.int32),
+               "arc_src": np.zeros(max(A, 1), np.int32), "arc_weight": np.zeros(max(A, 1), np.int32),
+               "weights": np.zeros((K, d), np.int32), "min_weight": np.zeros(N, np.int32)}
+        P32 = ctypes.POINTER(ctypes.c_int32)
+        err = ctypes.create_string_buffer(512)
+        rc = self._lib.pmdd_resident_dd_copy(self._h, i, *(out[k].ctypes.data_as(P32) for k in
+                                                           ("layer_offsets", "in_arc_offsets", "arc_src",
+                                                            "arc_weight", "weights", "min_weight")), err, len(err))
+        if rc != _native.PMDD_OK:
+            raise CudaEnumerationError(rc, err.value.decode(errors="replace"))
+        out["arc_src"] = out["arc_src"][:A]
+        out["arc_weight"] = out["arc_weight"][:A]
+        return out
+
     def enumerate(self, method: int = 1, state_dominance: int = 0, max_cand: int = DEFAULT_MAX_CAND,
                   max_prod: int = DEFAULT_MAX_PROD, stats: Optional[dict] = None, keep: bool = True) -> list:
-        n = len(self.dds)
-        ptype = self.dds[0].problem_type if self.dds else 1
+        n = self.count
+        ptype = self.problem_type
         o = _options(method, ptype, state_dominance, True, max_cand, max_prod, self.device)
         outs = (_native.PmddFrontier * max(n, 1))()
         status = (ctypes.c_int32 * max(n, 1))()

@@ -15,11 +15,16 @@ from __future__ import annotations
 import numpy as np
 
 
-def knapsack_text(n: int, nobjs: int, seed: int) -> str:
+def knapsack_arrays(n: int, nobjs: int, seed: int):
+    """(profits (nobjs, n), weights (n,), capacity) of the instance knapsack_text writes."""
     rng = np.random.default_rng(seed)
-    profits = rng.integers(1, 1001, size=(nobjs, n))
-    weights = rng.integers(1, 1001, size=n)
-    cap = int(weights.sum()) // 2
+    profits = rng.integers(1, 1001, size=(nobjs, n)).astype(np.int32)
+    weights = rng.integers(1, 1001, size=n).astype(np.int32)
+    return profits, weights, int(weights.sum()) // 2
+
+
+def knapsack_text(n: int, nobjs: int, seed: int) -> str:
+    profits, weights, cap = knapsack_arrays(n, nobjs, seed)
     lines = [f"{n} 1 {nobjs}"]
     lines += [" ".join(str(int(x)) for x in row) for row in profits]
     lines.append(" ".join(str(int(x)) for x in weights) + f" {cap}")
