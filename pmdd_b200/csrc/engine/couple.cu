@@ -4,10 +4,16 @@
 //    src/pmdd/enum/gpu/couple.cu:340-498 / src/pmdd/enum/cpu/enum.cpp:333-398, done in
 //    rounds without ever materialising all products.  A seed round builds a first
 //    running frontier from a few extreme products per cutset node; each product round
-//    streams the remaining products against the running frontier F held in shared
-//    memory (per-node and per-row ideal-point bounds discard whole groups of products
-//    first), appends survivors behind F, and re-filters F + survivors with the
-//    sort-filter-skyline block routine of sfs.cuh.
+//    streams the remaining products against the whole running frontier F (its first
+//    points from shared memory, the rest from L2; per-node and per-row ideal-point bounds
+//    discard whole groups of products first) and appends the survivors S behind F.  As
+//    no survivor is weakly dominated by a point of F, the next running frontier is
+//    {f in F : no s in S dominates f} + the maxima of S: F + S are bucketed by
+//    decreasing objective sum (a dominator's sum is never smaller), one GPU-wide mark
+//    pass sweeps tiles of F + S against the survivors up to the end of each point's
+//    bucket, staged in shared memory, and a compaction writes the next F in bucket
+//    order.  The product round uses that order: a product stops sweeping F once the
+//    buckets left cannot reach its sum.
 #include "couple.cuh"
 #include "sfs.cuh"
 
@@ -208,12 +214,40 @@ __global__ void __launch_bounds__(kCoupleThreads) couple_seed_kernel(const Coupl
     }
 }
 
-// Is a single point weakly dominated by any staged frontier point?  (lanes split F)
+// Order of the running frontier: F is in decreasing sum-bucket order under (mx, width,
+// nb), so every point from position j on has a sum <= top(F_j).  width 0: no order.
+struct FOrder {
+    int64_t mx, width, nb;
+    template <int D, typename T>
+    __device__ __forceinline__ int64_t top(const T *q) const {
+        if (width <= 0) return INT64_MAX;
+        const int64_t sm = point_sum<D, T>(q);
+        if (sm > mx) return INT64_MAX;
+        const int64_t b = (mx - sm) / width;
+        return mx - (b < nb ? b : nb - 1) * width;
+    }
+};
+
+// Is a single point weakly dominated by a point of F?  Lanes split F: the staged points
+// in shared memory first, then the rest of F in global memory; the sweep ends where the
+// remaining buckets cannot reach the point's sum.
 template <int D, typename T>
-__device__ __forceinline__ bool warp_point_dominated(const PackedPt<D, T> *fs, int nf, const T (&p)[D], int lane) {
+__device__ __forceinline__ bool warp_point_dominated(const PackedPt<D, T> *fs, int nf, const T *F, int64_t fn,
+                                                     const FOrder &ord, const T (&p)[D], int lane) {
+    const int64_t ps = point_sum<D, T>(p);
     bool hit = false;
-    for (int j = lane; j < nf && !hit; j += 32) hit = ge_all<D, T>(fs[j], p);
-    return __any_sync(0xffffffffu, hit);
+    for (int j = lane; j < nf && !hit; j += 32) {
+        if (ord.top<D, T>(fs[j].v) < ps) break;
+        hit = ge_all<D, T>(fs[j], p);
+    }
+    if (__any_sync(0xffffffffu, hit)) return true;
+    for (int64_t j0 = nf; j0 < fn; j0 += 32) {
+        if (ord.top<D, T>(F + j0 * D) < ps) break;  // warp-uniform
+        const int64_t j = j0 + lane;
+        if (j < fn) hit = ge_all<D, T>(load_global_pt<D, T>(F, j), p);
+        if (__any_sync(0xffffffffu, hit)) return true;
+    }
+    return false;
 }
 
 template <int D, typename T>
@@ -226,6 +260,7 @@ __global__ void __launch_bounds__(kCoupleThreads) couple_prune_kernel(const Coup
     const T *bu = static_cast<const T *>(J.bu_pts);
     const int64_t fn = J.ctr[kCtrF];
     const int nf = static_cast<int>(fn < kCoupleFS ? fn : kCoupleFS);
+    const FOrder ord{J.ctr[kCtrFMax], J.ctr[kCtrFWidth], J.ctr[kCtrFBuckets]};
     for (int k = threadIdx.x; k < nf; k += blockDim.x) {
         PackedPt<D, T> q;
 #pragma unroll
@@ -271,7 +306,7 @@ __global__ void __launch_bounds__(kCoupleThreads) couple_prune_kernel(const Coup
         T ub[D];
 #pragma unroll
         for (int o = 0; o < D; ++o) ub[o] = mt[o] + mb[o];
-        if (warp_point_dominated<D, T>(fs, nf, ub, lane)) continue;
+        if (warp_point_dominated<D, T>(fs, nf, U, fn, ord, ub, lane)) continue;
         bool overflowed = false;
         for (int t = 0; t < nt && !overflowed; ++t) {
             T tp[D], rub[D];
@@ -280,7 +315,7 @@ __global__ void __launch_bounds__(kCoupleThreads) couple_prune_kernel(const Coup
                 tp[o] = tdv[static_cast<int64_t>(t) * D + o];
                 rub[o] = tp[o] + mb[o];
             }
-            if (warp_point_dominated<D, T>(fs, nf, rub, lane)) continue;
+            if (warp_point_dominated<D, T>(fs, nf, U, fn, ord, rub, lane)) continue;
             for (int b0 = 0; b0 < nb; b0 += 32) {
                 const int b = b0 + lane;
                 const bool valid = b < nb;
@@ -288,15 +323,30 @@ __global__ void __launch_bounds__(kCoupleThreads) couple_prune_kernel(const Coup
 #pragma unroll
                 for (int o = 0; o < D; ++o) p[o] = valid ? tp[o] + buv[static_cast<int64_t>(b) * D + o] : T(0);
                 bool dom = !valid;
+                // `done`: no point of F from here on can reach this product's sum
+                bool done = false;
+                const int64_t ps = point_sum<D, T>(p);
                 // warp-uniform sweep of the staged frontier
                 int j = 0, it = 0;
                 for (; j + 4 <= nf; j += 4) {
 #pragma unroll
                     for (int u = 0; u < 4; ++u) dom |= ge_all<D, T>(fs[j + u], p);
-                    if ((++it & 7) == 0 && __all_sync(0xffffffffu, dom)) break;
+                    if ((++it & 7) == 0) {
+                        if (j + 4 < nf) done |= ord.top<D, T>(fs[j + 4].v) < ps;
+                        if (__all_sync(0xffffffffu, dom || done)) break;
+                    }
                 }
-                if (!__all_sync(0xffffffffu, dom))
+                if (!__all_sync(0xffffffffu, dom || done))
                     for (; j < nf; ++j) dom |= ge_all<D, T>(fs[j], p);
+                // the rest of F from global memory (warp-uniform, broadcast loads)
+                if (fn > nf && !__all_sync(0xffffffffu, dom || done))
+                    for (int64_t g = nf; g < fn; ++g) {
+                        dom |= ge_all<D, T>(load_global_pt<D, T>(U, g), p);
+                        if ((g & 31) == 31) {
+                            if (g + 1 < fn) done |= ord.top<D, T>(U + (g + 1) * D) < ps;
+                            if (__all_sync(0xffffffffu, dom || done)) break;
+                        }
+                    }
                 if (valid) ++evaluated;
                 if (!append_points<D, T>(J, U, fn, !dom, p, v, lane)) {
                     overflowed = true;
@@ -309,26 +359,246 @@ __global__ void __launch_bounds__(kCoupleThreads) couple_prune_kernel(const Coup
     if (lane == 0 && evaluated) atomicAdd(reinterpret_cast<unsigned long long *>(&J.ctr[kCtrEvaluated]), evaluated);
 }
 
-// F + survivors -> next running frontier in U_alt (one block per job), and the round's
-// bookkeeping.
+// Points of U at the start of a refilter: F = [0, fn) then this round's survivors S,
+// clamped to what was written.
+__device__ __forceinline__ void couple_extent(const CoupleJob &J, int64_t *fn, int64_t *n) {
+    *fn = J.ctr[kCtrF];
+    int64_t m = *fn + J.ctr[kCtrB];
+    if (m > J.ctr[kCtrValidEnd]) m = J.ctr[kCtrValidEnd];
+    if (m > J.ucap) m = J.ucap;
+    *n = m;
+}
+
+constexpr int kMarkThreads = 256;
+constexpr int kMarkStage = 2048;  // survivors staged in shared memory at a time
+
+// Sum bucket of a point (bucket 0 holds the largest sums): -1 above the top bucket.
+__device__ __forceinline__ int64_t sum_bucket(int64_t sum, int64_t mx, int64_t width, int64_t nb) {
+    if (sum > mx) return -1;
+    const int64_t b = (mx - sum) / width;
+    return b < nb ? b : nb - 1;
+}
+
+// Largest sum a point in the same bucket as `sum` can have (INT64_MAX without an order).
+__device__ __forceinline__ int64_t bucket_top(int64_t sum, int64_t mx, int64_t width, int64_t nb) {
+    if (width <= 0) return INT64_MAX;
+    const int64_t b = sum_bucket(sum, mx, width, nb);
+    return b < 0 ? INT64_MAX : mx - b * width;
+}
+
+// Refilter step 1 (one block per job): the sum range of F + S, the bucket count and
+// width, and zeroed bucket counts (all points and survivors apart).
 template <int D, typename T>
-__global__ void __launch_bounds__(SfsCfg<D, T>::kThreads) couple_sfs_kernel(const CoupleJob *__restrict__ jobs,
-                                                                            int seed) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+__global__ void __launch_bounds__(1024) couple_bucket_prep_kernel(const CoupleJob *__restrict__ jobs) {
+    __shared__ int64_t red_min[32], red_max[32];
     const CoupleJob &J = jobs[blockIdx.x];
-    const int64_t fn = J.ctr[kCtrF];
-    int64_t n = fn + J.ctr[kCtrB];
-    if (n > J.ctr[kCtrValidEnd]) n = J.ctr[kCtrValidEnd];
-    if (n > J.ucap) n = J.ucap;
-    SfsScratch<T> s;
-    s.P2 = static_cast<T *>(J.sc_pts2);
-    s.I2 = J.sc_idx;
-    s.SV = static_cast<T *>(J.sc_surv);
-    s.SVI = J.sc_sidx;
-    const int32_t kept = sfs_block<D, T>(smem_raw, static_cast<const T *>(J.U), n, s, static_cast<T *>(J.U_alt));
+    const T *U = static_cast<const T *>(J.U);
+    int64_t fn, n;
+    couple_extent(J, &fn, &n);
+    int64_t mn = INT64_MAX, mx = INT64_MIN;
+    for (int64_t i = threadIdx.x; i < n; i += 1024) {
+        const int64_t sm = point_sum<D, T>(U + i * D);
+        mn = min(mn, sm);
+        mx = max(mx, sm);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        mn = min(mn, static_cast<int64_t>(__shfl_xor_sync(0xffffffffu, mn, o)));
+        mx = max(mx, static_cast<int64_t>(__shfl_xor_sync(0xffffffffu, mx, o)));
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) {
+        red_min[warp] = mn;
+        red_max[warp] = mx;
+    }
+    __syncthreads();
+    int64_t nb = n / 64;
+    nb = nb < 1 ? 1 : (nb > kMaxBuckets ? kMaxBuckets : nb);
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < 32; ++w) {
+            mn = min(mn, red_min[w]);
+            mx = max(mx, red_max[w]);
+        }
+        if (n <= 0) {
+            mn = 0;
+            mx = 0;
+        }
+        J.ctr[kCtrSumMax] = mx;
+        J.ctr[kCtrWidth] = (mx - mn) / nb + 1;
+        J.ctr[kCtrBuckets] = nb;
+    }
+    for (int64_t b = threadIdx.x; b <= nb; b += 1024) {
+        J.sc_hist[b] = 0;
+        J.sc_hist[kMaxBuckets + 1 + b] = 0;
+    }
+}
+
+// Refilter step 2 (grid): points per bucket, all of F + S and survivors alone.
+template <int D, typename T>
+__global__ void __launch_bounds__(kMarkThreads) couple_bucket_count_kernel(const CoupleJob *__restrict__ jobs) {
+    const CoupleJob &J = jobs[blockIdx.y];
+    const T *U = static_cast<const T *>(J.U);
+    int64_t fn, n;
+    couple_extent(J, &fn, &n);
+    const int64_t mx = J.ctr[kCtrSumMax], width = J.ctr[kCtrWidth], nb = J.ctr[kCtrBuckets];
+    int32_t *hc = J.sc_hist, *hs = J.sc_hist + kMaxBuckets + 1;
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * kMarkThreads + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * kMarkThreads) {
+        const int64_t b = max(static_cast<int64_t>(0), sum_bucket(point_sum<D, T>(U + i * D), mx, width, nb));
+        atomicAdd(&hc[b], 1);
+        if (i >= fn) atomicAdd(&hs[b], 1);
+    }
+}
+
+// Refilter step 3 (one block per job): bucket counts -> bucket starts, both arrays.
+__global__ void __launch_bounds__(1024) couple_bucket_scan_kernel(const CoupleJob *__restrict__ jobs) {
+    __shared__ int32_t warp_buf[32];
+    __shared__ int32_t total;
+    const CoupleJob &J = jobs[blockIdx.x];
+    const int64_t nb = J.ctr[kCtrBuckets];
+    const int64_t chunk = (nb + 1023) / 1024;
+    const int64_t b0 = threadIdx.x * chunk, b1 = min(nb, b0 + chunk);
+    for (int h = 0; h < 2; ++h) {
+        int32_t *a = J.sc_hist + h * (kMaxBuckets + 1);
+        int32_t sum = 0;
+        for (int64_t b = b0; b < b1; ++b) sum += a[b];
+        int32_t run = block_exclusive_scan<int32_t, 1024>(sum, warp_buf, &total);
+        for (int64_t b = b0; b < b1; ++b) {
+            const int32_t c = a[b];
+            a[b] = run;
+            run += c;
+        }
+    }
+}
+
+// Refilter step 4 (grid): F + S into sc_pts2 in bucket order with a byte per point saying
+// whether it is a survivor, and the survivors alone into sc_surv in bucket order with their
+// sc_pts2 positions (order inside a bucket arbitrary).  Afterwards the histograms hold
+// the bucket ends.
+template <int D, typename T>
+__global__ void __launch_bounds__(kMarkThreads) couple_bucket_scatter_kernel(const CoupleJob *__restrict__ jobs) {
+    const CoupleJob &J = jobs[blockIdx.y];
+    const T *U = static_cast<const T *>(J.U);
+    T *C = static_cast<T *>(J.sc_pts2);
+    T *Sp = static_cast<T *>(J.sc_surv);
+    int64_t fn, n;
+    couple_extent(J, &fn, &n);
+    const int64_t mx = J.ctr[kCtrSumMax], width = J.ctr[kCtrWidth], nb = J.ctr[kCtrBuckets];
+    int32_t *hc = J.sc_hist, *hs = J.sc_hist + kMaxBuckets + 1;
+    uint8_t *origin = reinterpret_cast<uint8_t *>(J.sc_idx) + J.ucap;
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * kMarkThreads + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * kMarkThreads) {
+        const int64_t b = max(static_cast<int64_t>(0), sum_bucket(point_sum<D, T>(U + i * D), mx, width, nb));
+        const int64_t pos = atomicAdd(&hc[b], 1);
+#pragma unroll
+        for (int o = 0; o < D; ++o) C[pos * D + o] = U[i * D + o];
+        origin[pos] = i >= fn ? 1 : 0;
+        if (i >= fn) {
+            const int64_t sp = atomicAdd(&hs[b], 1);
+#pragma unroll
+            for (int o = 0; o < D; ++o) Sp[sp * D + o] = U[i * D + o];
+            J.sc_sidx[sp] = static_cast<int32_t>(pos);
+        }
+    }
+}
+
+// Refilter step 5: a keep byte for every point of F + S (in bucket order, sc_idx).  A
+// point of F is dropped when a survivor is >= on every objective (no survivor equals a
+// point of F: the product round drops products weakly dominated by F); a survivor is
+// dropped when another survivor is >= and differs, or equals it and comes first.  A
+// dominator's sum is never smaller, so it sits in the point's bucket or an earlier one:
+// each point sweeps the survivors up to the end of its own bucket.  Tiles of 256 points,
+// persistent over gridDim.x blocks per job; a tile stops once all its points are dropped.
+template <int D, typename T>
+__global__ void __launch_bounds__(kMarkThreads) couple_mark_kernel(const CoupleJob *__restrict__ jobs) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    PackedPt<D, T> *sp = reinterpret_cast<PackedPt<D, T> *>(smem_raw);                   // [kMarkStage]
+    int32_t *spos = reinterpret_cast<int32_t *>(smem_raw + sizeof(PackedPt<D, T>) * kMarkStage);  // [kMarkStage]
+    __shared__ int32_t tile_end;
+    const CoupleJob &J = jobs[blockIdx.y];
+    const T *C = static_cast<const T *>(J.sc_pts2);
+    const T *Sp = static_cast<const T *>(J.sc_surv);
+    int64_t fn, n;
+    couple_extent(J, &fn, &n);
+    const int64_t mx = J.ctr[kCtrSumMax], width = J.ctr[kCtrWidth], nb = J.ctr[kCtrBuckets];
+    const int32_t *ends = J.sc_hist + kMaxBuckets + 1;  // survivor bucket ends
+    uint8_t *keep = reinterpret_cast<uint8_t *>(J.sc_idx);
+    const uint8_t *origin = keep + J.ucap;
+    for (int64_t t0 = static_cast<int64_t>(blockIdx.x) * kMarkThreads; t0 < n;
+         t0 += static_cast<int64_t>(gridDim.x) * kMarkThreads) {
+        const int64_t i = t0 + threadIdx.x;
+        const bool valid = i < n;
+        const bool in_s = valid && origin[i] != 0;
+        T p[D];
+#pragma unroll
+        for (int o = 0; o < D; ++o) p[o] = valid ? C[i * D + o] : T(0);
+        int32_t my_end = 0;
+        if (valid && n > fn) my_end = ends[max(static_cast<int64_t>(0), sum_bucket(point_sum<D, T>(p), mx, width, nb))];
+        if (threadIdx.x == 0) tile_end = 0;
+        __syncthreads();
+        atomicMax(&tile_end, my_end);
+        bool dom = !valid;
+        __syncthreads();
+        const int64_t limit = tile_end;
+        for (int64_t c0 = 0; c0 < limit; c0 += kMarkStage) {
+            if (__syncthreads_and(dom || c0 >= my_end)) break;
+            const int cn = static_cast<int>(limit - c0 < kMarkStage ? limit - c0 : static_cast<int64_t>(kMarkStage));
+            for (int k = threadIdx.x; k < cn; k += kMarkThreads) {
+                sp[k] = load_global_pt<D, T>(Sp, c0 + k);
+                spos[k] = J.sc_sidx[c0 + k];
+            }
+            __syncthreads();
+            if (!dom) {
+                const int64_t rem = my_end - c0;
+                const int kn = static_cast<int>(rem < cn ? (rem > 0 ? rem : 0) : cn);
+                for (int k = 0; k < kn; ++k) {
+                    if (!ge_all<D, T>(sp[k], p)) continue;
+                    if (!in_s || (spos[k] != i && (!eq_all<D, T>(sp[k], p) || spos[k] < i))) {
+                        dom = true;
+                        break;
+                    }
+                }
+            }
+        }
+        __syncthreads();  // the stage and tile_end are rewritten by the next tile
+        if (valid) keep[i] = dom ? 0 : 1;
+    }
+}
+
+// Refilter step 6: compacts the kept points into U_alt in bucket order -- the next
+// running frontier, ordered by decreasing sum bucket under the parameters it records --
+// and does the round's bookkeeping.  One block per job.
+template <int D, typename T>
+__global__ void __launch_bounds__(1024) couple_compact_kernel(const CoupleJob *__restrict__ jobs, int seed) {
+    __shared__ int64_t warp_buf[32];
+    __shared__ int64_t total;
+    const CoupleJob &J = jobs[blockIdx.x];
+    const T *C = static_cast<const T *>(J.sc_pts2);
+    T *out = static_cast<T *>(J.U_alt);
+    int64_t fn, n;
+    couple_extent(J, &fn, &n);
+    const uint8_t *keep = reinterpret_cast<const uint8_t *>(J.sc_idx);
+    constexpr int ITEMS = 8;
+    int64_t base = 0;
+    for (int64_t c0 = 0; c0 < n; c0 += 1024 * ITEMS) {
+        const int64_t b = c0 + static_cast<int64_t>(threadIdx.x) * ITEMS;
+        int64_t mine = 0;
+#pragma unroll
+        for (int k = 0; k < ITEMS; ++k) mine += (b + k < n && keep[b + k]) ? 1 : 0;
+        int64_t pos = base + block_exclusive_scan<int64_t, 1024>(mine, warp_buf, &total);
+#pragma unroll
+        for (int k = 0; k < ITEMS; ++k) {
+            if (b + k < n && keep[b + k]) {
+#pragma unroll
+                for (int o = 0; o < D; ++o) out[pos * D + o] = C[(b + k) * D + o];
+                ++pos;
+            }
+        }
+        base += total;
+        __syncthreads();
+    }
     if (threadIdx.x == 0) {
         const int64_t resume = J.ctr[kCtrResume];
-        J.ctr[kCtrF] = kept;
+        J.ctr[kCtrF] = base;
         J.ctr[kCtrB] = 0;
         if (seed) {
             J.ctr[kCtrCursor] = 0;
@@ -339,6 +609,9 @@ __global__ void __launch_bounds__(SfsCfg<D, T>::kThreads) couple_sfs_kernel(cons
         }
         J.ctr[kCtrResume] = J.num_nodes;
         J.ctr[kCtrValidEnd] = J.ucap;
+        J.ctr[kCtrFMax] = J.ctr[kCtrSumMax];
+        J.ctr[kCtrFWidth] = J.ctr[kCtrWidth];
+        J.ctr[kCtrFBuckets] = J.ctr[kCtrBuckets];
     }
 }
 
@@ -346,20 +619,26 @@ template <int D, typename T>
 static cudaError_t launch_couple_round_t(const CoupleJob *jobs, int num_jobs, int blocks_per_job, bool seed,
                                         cudaStream_t stream) {
     const size_t smem = static_cast<size_t>(kCoupleFS) * sizeof(PackedPt<D, T>);
-    using Cfg = SfsCfg<D, T>;
+    const size_t mark_smem = static_cast<size_t>(kMarkStage) * (sizeof(PackedPt<D, T>) + sizeof(int32_t));
     static bool attr_set = false;
     if (!attr_set) {
         cudaError_t e = cudaFuncSetAttribute(couple_prune_kernel<D, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              static_cast<int>(smem));
         if (e != cudaSuccess) return e;
-        e = cudaFuncSetAttribute(couple_sfs_kernel<D, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(Cfg::kSmem));
+        e = cudaFuncSetAttribute(couple_mark_kernel<D, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(mark_smem));
         if (e != cudaSuccess) return e;
         attr_set = true;
     }
     if (seed) couple_seed_kernel<D, T><<<dim3(blocks_per_job, num_jobs), kCoupleThreads, 0, stream>>>(jobs);
     else couple_prune_kernel<D, T><<<dim3(blocks_per_job, num_jobs), kCoupleThreads, smem, stream>>>(jobs);
-    couple_sfs_kernel<D, T><<<num_jobs, Cfg::kThreads, Cfg::kSmem, stream>>>(jobs, seed ? 1 : 0);
+    const dim3 grid(blocks_per_job, num_jobs);
+    couple_bucket_prep_kernel<D, T><<<num_jobs, 1024, 0, stream>>>(jobs);
+    couple_bucket_count_kernel<D, T><<<grid, kMarkThreads, 0, stream>>>(jobs);
+    couple_bucket_scan_kernel<<<num_jobs, 1024, 0, stream>>>(jobs);
+    couple_bucket_scatter_kernel<D, T><<<grid, kMarkThreads, 0, stream>>>(jobs);
+    couple_mark_kernel<D, T><<<grid, kMarkThreads, mark_smem, stream>>>(jobs);
+    couple_compact_kernel<D, T><<<num_jobs, 1024, 0, stream>>>(jobs, seed ? 1 : 0);
     return cudaGetLastError();
 }
 

@@ -538,7 +538,7 @@ void Engine::release_instance(Instance &I) {
     arena_.release(I.cu_ctr);
     I.dd = nullptr;
     I.cu_mem = I.cu_U = I.cu_U_alt = I.cu_p2 = I.cu_sv = nullptr;
-    I.cu_i2 = I.cu_si = nullptr;
+    I.cu_i2 = I.cu_si = I.cu_hist = nullptr;
     I.cu_ctr = nullptr;
     I.blob.clear();
     I.blob.shrink_to_fit();
@@ -585,6 +585,7 @@ bool Engine::carve_couple(Instance &I, int64_t ucap) {
     I.cu_sv = m + 3 * pts;
     I.cu_i2 = reinterpret_cast<int32_t *>(m + 4 * pts);
     I.cu_si = reinterpret_cast<int32_t *>(m + 4 * pts + idx);
+    I.cu_hist = reinterpret_cast<int32_t *>(m + 4 * pts + 2 * idx);
     if (old_U && I.result_n > 0)  // carry the running frontier over (growth)
         cudaMemcpyAsync(I.cu_U, old_U, static_cast<size_t>(I.result_n) * I.d * I.elem(), cudaMemcpyDeviceToDevice,
                         stream_);
@@ -1161,6 +1162,7 @@ int Engine::step() {
         J.sc_surv = I->cu_sv;
         J.sc_idx = I->cu_i2;
         J.sc_sidx = I->cu_si;
+        J.sc_hist = I->cu_hist;
         J.ctr = I->cu_ctr;
         // the next running frontier lands in U_alt: swap now (host view)
         std::swap(I->cu_U, I->cu_U_alt);
@@ -1284,7 +1286,7 @@ int Engine::step() {
                                                       per, std::get<2>(g.first), stream_),
                              "coupling round"))
                     return -1;
-                launches_ += 2;
+                launches_ += 7;
                 i = j + 1;
             }
         }

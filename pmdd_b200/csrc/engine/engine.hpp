@@ -111,7 +111,7 @@ struct Instance {
     void *cu_U = nullptr;               // current running frontier (+ this round's survivors)
     void *cu_U_alt = nullptr;           // receives the next running frontier
     void *cu_p2 = nullptr, *cu_sv = nullptr;
-    int32_t *cu_i2 = nullptr, *cu_si = nullptr;
+    int32_t *cu_i2 = nullptr, *cu_si = nullptr, *cu_hist = nullptr;
     int64_t *cu_ctr = nullptr;
     int64_t cu_ucap = 0;
     int couple_rounds = 0;
