@@ -58,6 +58,16 @@ def build_dds(specs, threads=16):
         return list(ex.map(one, specs))
 
 
+def kp_arrays_from_text(text):
+    """(profits (d, n), weights (n,), capacity) of a one-constraint knapsack instance text."""
+    tok = list(map(int, text.split()))
+    n, m, d = tok[0], tok[1], tok[2]
+    assert m == 1
+    prof = np.array(tok[3:3 + d * n], dtype=np.int32).reshape(d, n)
+    w = np.array(tok[3 + d * n:3 + d * n + n], dtype=np.int32)
+    return prof, w, tok[3 + d * n + n]
+
+
 def dd_bytes(dd):
     v = dd.view
     n = (v.num_layers + 1) + (v.num_nodes + 1) + 2 * v.num_arcs + v.num_weights * v.nobjs
@@ -500,6 +510,30 @@ def main():
                                   "filter_achieved_gbs": af, "filter_frac_of_peak": af / peak,
                                   "filter_kernel_s": tf, "filter_algorithmic_bytes": int(bf)}
         r1.close()
+        # the knapsack half of the stream with DD construction inside the timed region:
+        # built on the device from the instance arrays and enumerated from there, against
+        # the host constructors (16 threads) + upload + enumeration
+        kp_texts = [t for p_, t, _ in specs if p_ == 1]
+        kp_arr = [kp_arrays_from_text(t) for t in kp_texts]
+        P.ResidentSet.from_knapsack(kp_arr[:2], device=device).close()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        rb = P.ResidentSet.from_knapsack(kp_arr, device=device)
+        t_build = time.perf_counter() - t0
+        n_b = rb.enumerate(method=1, keep=False)
+        t_dev = time.perf_counter() - t0
+        rb.close()
+        t0 = time.perf_counter()
+        kdds = build_dds([(1, t, "") for t in kp_texts])
+        t_hb = time.perf_counter() - t0
+        outs_h = P.enumerate_batch(kdds, method=1)
+        t_host = time.perf_counter() - t0
+        del kdds
+        line["knapsack_with_construction"] = {
+            "instances": len(kp_texts), "unit": "solves/s",
+            "device_built": len(kp_texts) / t_dev, "device_build_s": t_build,
+            "host_built": len(kp_texts) / t_host, "host_build_s": t_hb, "host_build_threads": 16,
+            "same_frontier_sizes": list(n_b) == [len(o) for o in outs_h]}
         # reference CPU baseline on the box's cores
         if world == 1:
             cores = os.cpu_count() or 1
