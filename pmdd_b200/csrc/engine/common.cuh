@@ -8,11 +8,14 @@ namespace pmdd {
 namespace dev {
 
 // Fused expand+filter tiles: a tile owns every destination whose candidate range
-// starts inside its window of kTileWindow candidates; destinations of at most
+// starts inside its window of at most kTileWindow candidates; destinations of at most
 // kSmallMax candidates are filtered in shared memory, larger ones take the
-// global-memory ("big") path.  A tile therefore holds < 2*kTileWindow candidates.
+// global-memory ("big") path.  A tile therefore holds < 2*kTileWindow candidates.  The
+// window shrinks (to kTileWindowMin) for steps with few candidates, so that a small
+// step still spreads over the SMs.
 constexpr int kTileThreads = 512;
 constexpr int kTileWindow = 1024;
+constexpr int kTileWindowMin = 128;
 constexpr int kSmallMax = 1024;
 constexpr int kTileCap = 2 * kTileWindow;
 // Per-pass staging caps, sized so that a tile's shared memory (about 70 KB at d=3) lets
@@ -56,6 +59,7 @@ struct ExpandJob {
     int64_t total_cand;
     int64_t tile_base;             // first global tile index of this job
     int64_t num_tiles;
+    int64_t tile_window;           // candidates per tile window (kTileWindowMin..kTileWindow)
     int32_t *tile_first;           // [num_tiles+1]: first destination of each tile (tile_plan_kernel)
     const int64_t *big_list;       // (local item, scratch offset) pairs
     int32_t num_big;

@@ -740,6 +740,19 @@ int Engine::step() {
     std::vector<ExpPlan> exps;
     int64_t blocked_need = -1;
     Instance *blocked = nullptr;
+    // tile window of this step: full windows when the step has candidates for a few waves
+    // of tiles over the SMs, smaller ones (more tiles) when it has not
+    int64_t step_cand = 0;
+    for (auto &p : active_) {
+        const Instance &I = *p;
+        if (I.phase != Instance::RUNNING) continue;
+        const bool is_td = I.opts.method != 3 || I.td.score <= I.bu.score;
+        const Side &s = is_td ? I.td : I.bu;
+        if (s.counted) step_cand += s.res.total;
+    }
+    const int64_t want_tiles = static_cast<int64_t>(sms_) * 6;
+    const int64_t window = std::max<int64_t>(dev::kTileWindowMin, std::min<int64_t>(dev::kTileWindow,
+                                                                                     step_cand / want_tiles));
     for (auto &p : active_) {
         Instance &I = *p;
         if (I.phase != Instance::RUNNING) continue;
@@ -755,7 +768,7 @@ int Engine::step() {
         e.out_pts = arena_.alloc(pts_bytes);
         e.out_off = static_cast<int64_t *>(arena_.alloc(sizeof(int64_t) * V));
         // sizes of the new frontier, followed by the tile plan of this expansion
-        const int64_t ntiles = std::max<int64_t>(1, (C + dev::kTileWindow - 1) / dev::kTileWindow);
+        const int64_t ntiles = std::max<int64_t>(1, (C + window - 1) / window);
         e.out_size = static_cast<int32_t *>(arena_.alloc(sizeof(int32_t) * (V + ntiles + 1)));
         bool okay = e.out_pts && e.out_off && e.out_size;
         if (okay && s.res.num_big > 0) {
@@ -842,7 +855,8 @@ int Engine::step() {
                 J.out_off = e.out_off;
                 J.out_size = e.out_size;
                 J.total_cand = s.res.total;
-                J.num_tiles = std::max<int64_t>(1, (s.res.total + dev::kTileWindow - 1) / dev::kTileWindow);
+                J.tile_window = window;
+                J.num_tiles = std::max<int64_t>(1, (s.res.total + window - 1) / window);
                 J.tile_first = e.out_size + J.num_items;
                 J.tile_base = gl.tiles;
                 tile_bases[pos] = gl.tiles;

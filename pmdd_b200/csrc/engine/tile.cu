@@ -1,7 +1,8 @@
 // Fused expand + dominance filter over candidate tiles (the per-layer hot kernel).
 //
 // A tile owns every destination assigned to it by tile_plan_kernel (those whose
-// candidate range starts inside the tile's window of kTileWindow candidates);
+// candidate range starts inside the tile's window of J.tile_window <= kTileWindow
+// candidates);
 // destinations with at most kSmallMax candidates are handled here entirely in shared
 // memory, larger ones only get their slot offset (the oversized path in big.cu filters
 // them).  A tile therefore holds < kTileCap points.
@@ -77,7 +78,7 @@ __global__ void tile_plan_kernel(const ExpandJob *__restrict__ jobs, const int64
         const int64_t T = J.num_tiles;
         auto tile_of = [&](int32_t k) -> int64_t {
             const int64_t s = item_start(J.item_arc_off, J.arc_cand_off, J.item_base, J.arc_base, k);
-            const int64_t t = s / kTileWindow;
+            const int64_t t = s / J.tile_window;
             return t < T - 1 ? t : T - 1;
         };
         const int64_t ti = tile_of(i);
