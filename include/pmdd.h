@@ -208,6 +208,22 @@ typedef struct pmdd_knapsack {
 pmdd_resident *pmdd_resident_build_knapsack(const pmdd_knapsack *instances, int32_t count, int32_t device, char *err,
                                             size_t errlen);
 
+/* TSP instance: n cities, one cost matrix per objective (the reference's TSPInstance,
+ * src/pmdd/instances/tsp_instance.cpp:11-39; arc weights are the negated costs). */
+typedef struct pmdd_tsp {
+    int32_t n;                 /* cities, 2..20 */
+    int32_t nobjs;             /* objectives used, 1..8 */
+    const int32_t *cost;       /* [nobjs][n][n], row-major per objective */
+} pmdd_tsp;
+
+/* TSP MDDs on the device: every MDD of n cities has the same layers, nodes and arcs (all
+ * (visited set, last city) states are reachable; src/pmdd/mdd/tsp_mdd.cpp:21-196), so the
+ * engine builds that structure once per n on the GPU and keeps it, and each instance
+ * adds only its weight table.  The DDs equal the host constructor's (problem type 3)
+ * array for array.  No counterpart in the reference. */
+pmdd_resident *pmdd_resident_build_tsp(const pmdd_tsp *instances, int32_t count, int32_t device, char *err,
+                                       size_t errlen);
+
 /* Shape of DD i of a resident set: shape = {nobjs, num_layers, num_nodes, num_arcs,
  * num_weights}; widths = {original width, original nodes, reduced width, reduced nodes}
  * for device-built DDs, -1 otherwise (either pointer may be NULL). */
@@ -240,6 +256,9 @@ pmdd_server *pmdd_server_create(int32_t device, int64_t budget_bytes, int32_t ma
 /* Copies the DD; the caller's buffers may be reused immediately. */
 int pmdd_server_submit(pmdd_server *srv, const pmdd_dd *dd, const pmdd_options *opts,
                        uint64_t req_id);
+/* Submits a TSP request by its cost matrices: the server uses its shared n-city MDD
+ * structure (built on the device on first use) and uploads only the weight table. */
+int pmdd_server_submit_tsp(pmdd_server *srv, const pmdd_tsp *inst, const pmdd_options *opts, uint64_t req_id);
 /* Runs engine steps until at least one request completes or nothing is pending;
  * returns the number of results now waiting. */
 int pmdd_server_run(pmdd_server *srv, int32_t max_steps);

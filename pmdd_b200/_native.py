@@ -50,6 +50,14 @@ class PmddKnapsack(ctypes.Structure):
     ]
 
 
+class PmddTsp(ctypes.Structure):
+    _fields_ = [
+        ("n", c_i32),
+        ("nobjs", c_i32),
+        ("cost", P_i32),
+    ]
+
+
 class PmddOptions(ctypes.Structure):
     _fields_ = [
         ("method", c_i32),
@@ -190,6 +198,10 @@ GPU_SYMBOLS = {
     "pmdd_resident_bytes": (c_i64, [ctypes.c_void_p]),
     "pmdd_resident_build_knapsack": (ctypes.c_void_p, [ctypes.POINTER(PmddKnapsack), c_i32, c_i32, ctypes.c_char_p,
                                                        ctypes.c_size_t]),
+    "pmdd_resident_build_tsp": (ctypes.c_void_p, [ctypes.POINTER(PmddTsp), c_i32, c_i32, ctypes.c_char_p,
+                                                  ctypes.c_size_t]),
+    "pmdd_server_submit_tsp": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(PmddTsp), ctypes.POINTER(PmddOptions),
+                                              ctypes.c_uint64]),
     "pmdd_resident_dd_shape": (ctypes.c_int, [ctypes.c_void_p, c_i32, P_i32, ctypes.POINTER(c_i64)]),
     "pmdd_resident_dd_copy": (ctypes.c_int, [ctypes.c_void_p, c_i32, P_i32, P_i32, P_i32, P_i32, P_i32, P_i32,
                                              ctypes.c_char_p, ctypes.c_size_t]),

@@ -14,6 +14,7 @@
 
 #include "engine.hpp"
 #include "kpbuild.cuh"
+#include "tspbuild.cuh"
 #include "pareto.cuh"
 #include "pmdd.h"
 
@@ -555,6 +556,7 @@ int pmdd_resident_enumerate(pmdd_resident *R, const pmdd_options *opts, pmdd_fro
         I->d_out_w = T.d_out_w;
         I->d_cursor = T.d_cursor;
         I->external_dd = true;
+        I->tsp = T.tsp;
         I->with_out_csr = T.with_out_csr;
         I->est_bytes = std::max<int64_t>(0, T.est_bytes - static_cast<int64_t>(T.dev_bytes));
         I->submit_s = pmdd::now_s();
@@ -772,6 +774,60 @@ pmdd_resident *pmdd_resident_build_knapsack(const pmdd_knapsack *ks, int32_t cou
     return R.release();
 }
 
+pmdd_resident *pmdd_resident_build_tsp(const pmdd_tsp *ts, int32_t count, int32_t device, char *err, size_t errlen) {
+    if (count < 0 || (count > 0 && !ts)) {
+        write_err(err, errlen, "invalid TSP set");
+        return nullptr;
+    }
+    for (int32_t i = 0; i < count; ++i) {
+        std::string why;
+        if (ts[i].n < pmdd::dev::kTspMinCities || ts[i].n > pmdd::dev::kTspMaxCities) why = "n must be in 2..20";
+        else if (ts[i].nobjs < 1 || ts[i].nobjs > 8) why = "nobjs must be in 1..8";
+        else if (!ts[i].cost) why = "cost pointer is NULL";
+        if (!why.empty()) {
+            write_err(err, errlen, "instance " + std::to_string(i) + ": " + why);
+            return nullptr;
+        }
+    }
+    std::unique_ptr<pmdd_resident> R(new pmdd_resident);
+    R->device = device;
+    DeviceSlot &slot = slot_for(device);
+    std::lock_guard<std::mutex> lk(slot.mu);
+    std::string msg;
+    if (ensure_engine(device, slot, &msg) != PMDD_OK) {
+        write_err(err, errlen, msg);
+        return nullptr;
+    }
+    R->generation = slot.generation;
+    pmdd::Engine &E = *slot.engine;
+    pmdd_options o;
+    pmdd_options_default(&o);
+    o.problem_type = 3;
+    for (int32_t i = 0; i < count; ++i) {
+        const pmdd::TspStructure *S = E.tsp_structure(ts[i].n, &msg);
+        std::unique_ptr<pmdd::Instance> I(new pmdd::Instance);
+        if (S) pmdd::prepare_tsp_instance(*S, ts[i].nobjs, ts[i].cost, o, static_cast<uint64_t>(i), I.get());
+        if (!S || !E.upload_dd(*I)) {
+            if (I->dd) E.release_dd(*I);
+            for (auto &T : R->tmpl) E.release_dd(*T);
+            write_err(err, errlen, S ? "TSP set does not fit the device memory budget" : msg);
+            return nullptr;
+        }
+        R->bytes += static_cast<int64_t>(I->dev_bytes);
+        R->tmpl.push_back(std::move(I));
+    }
+    if (cudaStreamSynchronize(E.stream()) != cudaSuccess) {
+        for (auto &T : R->tmpl) E.release_dd(*T);
+        write_err(err, errlen, "TSP weight upload failed");
+        return nullptr;
+    }
+    for (auto &I : R->tmpl) {
+        I->blob.clear();
+        I->blob.shrink_to_fit();
+    }
+    return R.release();
+}
+
 int pmdd_resident_dd_shape(const pmdd_resident *R, int32_t i, int32_t *shape, int64_t *widths) {
     if (!R || i < 0 || i >= static_cast<int32_t>(R->tmpl.size())) return PMDD_ERR_INVALID;
     const pmdd::Instance &T = *R->tmpl[i];
@@ -803,15 +859,16 @@ int pmdd_resident_dd_copy(pmdd_resident *R, int32_t i, int32_t *layer_offsets, i
     }
     const pmdd::Instance &T = *R->tmpl[i];
     cudaStream_t st = slot.engine->stream();
-    auto get = [&](void *dst, size_t off, size_t bytes) {
-        return bytes == 0 || cudaMemcpyAsync(dst, T.dd + off, bytes, cudaMemcpyDeviceToHost, st) == cudaSuccess;
+    auto get = [&](void *dst, const void *src, size_t bytes) {
+        return bytes == 0 || cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st) == cudaSuccess;
     };
-    bool ok = get(layer_offsets, T.off_layer, sizeof(int32_t) * (static_cast<size_t>(T.L) + 1)) &&
-              get(in_arc_offsets, T.off_in, sizeof(int32_t) * (static_cast<size_t>(T.N) + 1)) &&
-              get(arc_src, T.off_src, sizeof(int32_t) * static_cast<size_t>(T.A)) &&
-              get(arc_weight, T.off_w, sizeof(int32_t) * static_cast<size_t>(T.A)) &&
-              get(weights, T.off_weights, sizeof(int32_t) * static_cast<size_t>(T.K) * T.d);
-    if (ok && min_weight && T.sd_kind == 1) ok = get(min_weight, T.off_minw, sizeof(int32_t) * static_cast<size_t>(T.N));
+    std::memcpy(layer_offsets, T.layer_off.data(), sizeof(int32_t) * (static_cast<size_t>(T.L) + 1));
+    bool ok = get(in_arc_offsets, T.d_in_off, sizeof(int32_t) * (static_cast<size_t>(T.N) + 1)) &&
+              get(arc_src, T.d_arc_src, sizeof(int32_t) * static_cast<size_t>(T.A)) &&
+              get(arc_weight, T.d_arc_w, sizeof(int32_t) * static_cast<size_t>(T.A)) &&
+              get(weights, T.d_weights, sizeof(int32_t) * static_cast<size_t>(T.K) * T.d);
+    if (ok && min_weight && T.sd_kind == 1)
+        ok = get(min_weight, T.dd + T.off_minw, sizeof(int32_t) * static_cast<size_t>(T.N));
     if (!ok || cudaStreamSynchronize(st) != cudaSuccess) {
         write_err(err, errlen, std::string("CUDA error: ") + cudaGetErrorString(cudaGetLastError()));
         return PMDD_ERR_CUDA;
@@ -852,6 +909,33 @@ int pmdd_server_submit(pmdd_server *srv, const pmdd_dd *dd, const pmdd_options *
         srv->engine->finished().push_back(std::move(I));
         return rc;
     }
+    srv->engine->submit(std::move(I));
+    srv->submitted++;
+    return PMDD_OK;
+}
+
+int pmdd_server_submit_tsp(pmdd_server *srv, const pmdd_tsp *t, const pmdd_options *opts, uint64_t req_id) {
+    if (!srv || !t || !t->cost || t->n < pmdd::dev::kTspMinCities || t->n > pmdd::dev::kTspMaxCities ||
+        t->nobjs < 1 || t->nobjs > 8)
+        return PMDD_ERR_INVALID;
+    pmdd_options o;
+    if (opts) o = *opts;
+    else pmdd_options_default(&o);
+    o.problem_type = 3;
+    if ((o.method != 1 && o.method != 3) || o.maximization == 0) return PMDD_ERR_INVALID;
+    std::string msg;
+    const pmdd::TspStructure *S = srv->engine->tsp_structure(t->n, &msg);
+    std::unique_ptr<pmdd::Instance> I(new pmdd::Instance);
+    if (!S) {
+        I->id = req_id;
+        I->status = PMDD_ERR_OOM;
+        I->error = msg;
+        I->phase = pmdd::Instance::DONE;
+        I->finish_s = pmdd::now_s();
+        srv->engine->finished().push_back(std::move(I));
+        return PMDD_ERR_OOM;
+    }
+    pmdd::prepare_tsp_instance(*S, t->nobjs, t->cost, o, req_id, I.get());
     srv->engine->submit(std::move(I));
     srv->submitted++;
     return PMDD_OK;

@@ -13,6 +13,7 @@
 // layer's candidate count and the bottom-up score is 1.5x (truncated) the next
 // bottom-up layer's candidate count; both start at 0.
 #include "engine.hpp"
+#include "tspbuild.cuh"
 
 #include <algorithm>
 #include <atomic>
@@ -337,6 +338,118 @@ int prepare_instance(const pmdd_dd &dd, const pmdd_options &o, uint64_t id, Inst
     return PMDD_OK;
 }
 
+void prepare_tsp_instance(const TspStructure &S, int nobjs, const int32_t *cost, const pmdd_options &opts,
+                          uint64_t id, Instance *I) {
+    const int n = S.n, d = nobjs;
+    const int32_t L = n + 2, K = 1 + n * n;
+    I->id = id;
+    I->opts = opts;
+    I->d = d;
+    I->L = L;
+    I->N = S.N;
+    I->A = S.A;
+    I->K = K;
+    I->layer_off = S.layer_off;
+    I->arc_at_layer = S.arc_at;
+    I->tsp = &S;
+    I->off_weights = 0;
+    I->blob.assign(sizeof(int32_t) * static_cast<size_t>(K) * d, 0);
+    int32_t *w = reinterpret_cast<int32_t *>(I->blob.data());
+    const size_t nn = static_cast<size_t>(n) * n;
+    for (size_t ij = 0; ij < nn; ++ij)
+        for (int o = 0; o < d; ++o) w[(1 + ij) * d + o] = -cost[o * nn + ij];
+    // |path sum| bound, layer by layer as prepare_instance takes it: the arcs into layer 2
+    // use rows (0, v), layers 3..n rows (u, v) with u, v >= 1, the terminal rows (u, 0)
+    auto rmax = [&](int i, int j) {
+        int64_t m = 0;
+        for (int o = 0; o < d; ++o) m = std::max<int64_t>(m, std::llabs(static_cast<int64_t>(cost[o * nn + i * n + j])));
+        return m;
+    };
+    int64_t m2 = 0, m3 = 0, mt = 0;
+    for (int v = 1; v < n; ++v) m2 = std::max(m2, rmax(0, v));
+    for (int u = 1; u < n; ++u)
+        for (int v = 1; v < n; ++v)
+            if (u != v) m3 = std::max(m3, rmax(u, v));
+    for (int u = 1; u < n; ++u) mt = std::max(mt, rmax(u, 0));
+    const int64_t bound = m2 + static_cast<int64_t>(std::max(0, n - 2)) * m3 + mt;
+    I->wide = bound > static_cast<int64_t>(INT32_MAX);
+    I->blob_bytes = I->blob.size();
+    I->dev_bytes = align256(I->blob_bytes);
+    I->with_out_csr = true;
+    I->sd_kind = 0;
+    I->has_sd_order = false;
+    int64_t widest_arcs = 0;
+    for (int l = 0; l < L; ++l) widest_arcs = std::max<int64_t>(widest_arcs, S.arc_at[l + 1] - S.arc_at[l]);
+    I->est_bytes = static_cast<int64_t>(I->dev_bytes) + 8 * widest_arcs * static_cast<int64_t>(d * I->elem() + 16);
+    I->submit_s = now_s();
+}
+
+const TspStructure *Engine::tsp_structure(int n, std::string *err) {
+    auto it = tsp_cache_.find(n);
+    if (it != tsp_cache_.end()) return it->second.get();
+    if (n < dev::kTspMinCities || n > dev::kTspMaxCities) {
+        *err = "TSP structure: n must be in 2..20";
+        return nullptr;
+    }
+    std::unique_ptr<TspStructure> S(new TspStructure);
+    const dev::TspShape shape = dev::tsp_shape(n);
+    S->n = n;
+    S->layer_off = shape.layer_off;
+    S->arc_at = shape.arc_at;
+    S->N = shape.layer_off.back();
+    S->A = shape.arc_at.back();
+    const size_t L1 = shape.layer_off.size(), N = static_cast<size_t>(S->N), A = static_cast<size_t>(S->A);
+    size_t off = 0;
+    auto take = [&](size_t ints) {
+        const size_t o = off;
+        off = align256(off + sizeof(int32_t) * ints);
+        return o;
+    };
+    const size_t o_lo = take(L1), o_in = take(N + 1), o_src = take(A), o_w = take(A), o_oo = take(N + 1),
+                 o_oh = take(A), o_ow = take(A), o_cur = take(N), o_err = take(1);
+    S->mem = static_cast<unsigned char *>(arena_.alloc(off));
+    void *scratch = arena_.alloc(dev::tsp_scratch_bytes(n));
+    if (!S->mem || !scratch) {
+        arena_.release(S->mem);
+        arena_.release(scratch);
+        *err = "TSP structure does not fit the device memory budget";
+        return nullptr;
+    }
+    int32_t *base = reinterpret_cast<int32_t *>(S->mem);
+    auto at = [&](size_t o) { return reinterpret_cast<int32_t *>(S->mem + o); };
+    int32_t *d_err = at(o_err);
+    int32_t h_err = 0;
+    (void)base;
+    bool ok = cuda_ok(cudaMemsetAsync(d_err, 0, sizeof(int32_t), stream_), "TSP structure");
+    int64_t nl = 0;
+    ok = ok && cuda_ok(dev::launch_tsp_structure(n, shape, at(o_lo), at(o_in), at(o_src), at(o_w), scratch, d_err,
+                                                 sms_, stream_, &nl),
+                       "TSP structure");
+    S->in_off = at(o_in);
+    S->arc_src = at(o_src);
+    S->arc_w = at(o_w);
+    S->out_off = at(o_oo);
+    S->out_head = at(o_oh);
+    S->out_w = at(o_ow);
+    S->cursor = at(o_cur);
+    ok = ok && cuda_ok(dev::launch_build_out_csr(S->in_off, S->arc_src, S->arc_w, S->N, S->A, S->out_off, S->cursor,
+                                                 S->out_head, S->out_w, stream_),
+                       "TSP out-arc CSR");
+    ok = ok && cuda_ok(cudaMemcpyAsync(&h_err, d_err, sizeof(int32_t), cudaMemcpyDeviceToHost, stream_), "TSP check") &&
+         cuda_ok(cudaStreamSynchronize(stream_), "TSP structure");
+    launches_ += nl + 3;
+    g_total_launches += nl + 3;
+    arena_.release(scratch);
+    if (!ok || h_err != 0) {
+        arena_.release(S->mem);
+        *err = ok ? "TSP structure: layer sizes differ from the combinatorial count (internal)" : error_;
+        return nullptr;
+    }
+    const TspStructure *r = S.get();
+    tsp_cache_[n] = std::move(S);
+    return r;
+}
+
 void layout_built_knapsack(Instance *I, int d, bool wide, const std::vector<int32_t> &layer_off,
                            const std::vector<int32_t> &arc_at_layer, int32_t K) {
     const int32_t L = static_cast<int32_t>(layer_off.size()) - 1;
@@ -603,6 +716,21 @@ bool Engine::upload_dd(Instance &I) {
 }
 
 bool Engine::bind_dd(Instance &I) {
+    if (I.tsp) {  // shared structure: only the weight table is the instance's own
+        const TspStructure &S = *I.tsp;
+        I.d_in_off = S.in_off;
+        I.d_arc_src = S.arc_src;
+        I.d_arc_w = S.arc_w;
+        I.d_weights = reinterpret_cast<const int32_t *>(I.dd);
+        I.d_sd_order = nullptr;
+        I.d_sd_next = nullptr;
+        I.d_state = nullptr;
+        I.d_out_off = S.out_off;
+        I.d_out_head = S.out_head;
+        I.d_out_w = S.out_w;
+        I.d_cursor = S.cursor;
+        return true;
+    }
     I.d_in_off = reinterpret_cast<const int32_t *>(I.dd + I.off_in);
     I.d_arc_src = reinterpret_cast<const int32_t *>(I.dd + I.off_src);
     I.d_arc_w = reinterpret_cast<const int32_t *>(I.dd + I.off_w);

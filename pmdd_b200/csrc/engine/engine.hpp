@@ -72,6 +72,17 @@ struct Side {
     int64_t score = 0;
 };
 
+// The shared part of every TSP MDD of n cities (tspbuild.cuh): all arrays but the
+// weight table, with the bottom-up CSR, in one device block owned by the engine.
+struct TspStructure {
+    int n = 0;
+    unsigned char *mem = nullptr;
+    std::vector<int32_t> layer_off, arc_at;  // host copies, L+1 each
+    int32_t N = 0, A = 0;
+    const int32_t *in_off = nullptr, *arc_src = nullptr, *arc_w = nullptr;
+    int32_t *out_off = nullptr, *out_head = nullptr, *out_w = nullptr, *cursor = nullptr;
+};
+
 struct Instance {
     enum Phase { QUEUED, RUNNING, COUPLING, DONE };
     uint64_t id = 0;
@@ -124,6 +135,7 @@ struct Instance {
     double submit_s = 0, admit_s = 0, finish_s = 0;
     int64_t est_bytes = 0;              // admission estimate
     bool external_dd = false;           // DD already resident (owned by a pmdd_resident set)
+    const TspStructure *tsp = nullptr;  // TSP MDD: structure shared, I.dd holds the weight table only
     bool with_out_csr = false;          // device copy carries the bottom-up CSR
 
     size_t elem() const { return wide ? 8 : 4; }
@@ -149,6 +161,12 @@ void pack_instance(const pmdd_dd &dd, const Instance &inst, unsigned char *dst);
 // bottom-up CSR.
 void layout_built_knapsack(Instance *I, int d, bool wide, const std::vector<int32_t> &layer_off,
                            const std::vector<int32_t> &arc_at_layer, int32_t K);
+
+// A TSP request over a shared structure: host metadata and the blob, which is the weight
+// table alone (row 0 zero, row 1 + i*n + j = -cost[o][i][j]; `cost` is [nobjs][n][n]).
+// The path-sum bound follows prepare_instance's rule layer by layer.
+void prepare_tsp_instance(const TspStructure &S, int nobjs, const int32_t *cost, const pmdd_options &opts,
+                          uint64_t id, Instance *I);
 
 // Tuned oversized-path crossovers, (objectives, problem type) -> big_mark_min, from the
 // tuning file pmdd_b200.autotune writes (see Engine::mark_min_for); empty when absent.
@@ -198,6 +216,9 @@ class Engine {
     // Device pointers of a DD whose arrays are in I.dd (uploaded or built on the device),
     // and its bottom-up CSR when the instance carries one.
     bool bind_dd(Instance &I);
+    // The structure of n-city TSP MDDs on this engine's device, built on first use and
+    // kept for the engine's life; nullptr (with *err) if it cannot be built.
+    const TspStructure *tsp_structure(int n, std::string *err);
     void release_dd(Instance &I);
     // Pinned host memory for packing DD uploads (grow-only, kept across calls); nullptr
     // when it cannot be had.  Contents must stay untouched until the uploads that read
@@ -237,6 +258,7 @@ class Engine {
     int max_slots_ = 0;
     cudaStream_t stream_ = nullptr;
     cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};  // per-step phase timing, reused
+    std::map<int, std::unique_ptr<TspStructure>> tsp_cache_;
     Arena arena_;
     std::deque<std::unique_ptr<Instance>> queued_;
     std::vector<std::unique_ptr<Instance>> active_;

@@ -163,6 +163,32 @@ class ResidentSet:
             raise CudaEnumerationError(1, err.value.decode(errors="replace"))
         return self
 
+    @classmethod
+    def from_tsp(cls, costs: Iterable, device: int = 0) -> "ResidentSet":
+        """TSP MDDs on the device (pmdd_resident_build_tsp) from cost matrices
+        (nobjs, n, n): the n-city structure is built once on the GPU and shared, each
+        instance uploads only its weight table."""
+        mats = [np.ascontiguousarray(c, dtype=np.int32) for c in costs]
+        n = len(mats)
+        specs = (_native.PmddTsp * max(n, 1))()
+        P32 = ctypes.POINTER(ctypes.c_int32)
+        for i, c in enumerate(mats):
+            if c.ndim != 3 or c.shape[1] != c.shape[2]:
+                raise ValueError(f"instance {i}: costs must be (nobjs, n, n)")
+            specs[i] = _native.PmddTsp(c.shape[1], c.shape[0], c.ctypes.data_as(P32))
+        lib = _native.gpu_lib()
+        err = ctypes.create_string_buffer(512)
+        self = cls.__new__(cls)
+        self.dds = []
+        self._lib = lib
+        self.device = device
+        self.count = n
+        self.problem_type = 3
+        self._h = lib.pmdd_resident_build_tsp(specs, n, device, err, len(err))
+        if not self._h:
+            raise CudaEnumerationError(1, err.value.decode(errors="replace"))
+        return self
+
     @property
     def device_bytes(self) -> int:
         return self._lib.pmdd_resident_bytes(self._h)

@@ -44,12 +44,21 @@ def setpacking_text(n: int, m: int, nobjs: int, seed: int) -> str:
     return "\n".join(lines) + "\n"
 
 
-def tsp_text(n: int, nobjs: int, seed: int) -> str:
+def tsp_arrays(n: int, nobjs: int, seed: int) -> np.ndarray:
+    """Cost matrices (nobjs, n, n) of the instance tsp_text writes."""
     rng = np.random.default_rng(seed)
-    lines = [f"{nobjs}", f"{n}"]
-    for _ in range(nobjs):
+    cost = np.empty((nobjs, n, n), dtype=np.int32)
+    for o in range(nobjs):
         mat = rng.integers(1, 1001, size=(n, n))
         np.fill_diagonal(mat, 0)
+        cost[o] = mat
+    return cost
+
+
+def tsp_text(n: int, nobjs: int, seed: int) -> str:
+    cost = tsp_arrays(n, nobjs, seed)
+    lines = [f"{nobjs}", f"{n}"]
+    for mat in cost:
         lines += [" ".join(str(int(x)) for x in row) for row in mat]
     return "\n".join(lines) + "\n"
 

@@ -49,6 +49,17 @@ class Server:
         view = dd.view
         return self._lib.pmdd_server_submit(self._h, ctypes.byref(view), ctypes.byref(o), ctypes.c_uint64(req_id))
 
+    def submit_tsp(self, cost, req_id: int, method: int = 3, max_cand: int = DEFAULT_MAX_CAND,
+                   max_prod: int = DEFAULT_MAX_PROD) -> int:
+        """A TSP request by its cost matrices (nobjs, n, n): the server's shared n-city
+        structure is used and only the weight table is uploaded."""
+        c = np.ascontiguousarray(cost, dtype=np.int32)
+        if c.ndim != 3 or c.shape[1] != c.shape[2]:
+            raise ValueError("costs must be (nobjs, n, n)")
+        spec = _native.PmddTsp(c.shape[1], c.shape[0], c.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)))
+        o = _options(method, 3, 0, True, max_cand, max_prod, 0)
+        return self._lib.pmdd_server_submit_tsp(self._h, ctypes.byref(spec), ctypes.byref(o), ctypes.c_uint64(req_id))
+
     def run(self, max_steps: int = 0) -> int:
         r = self._lib.pmdd_server_run(self._h, max_steps)
         if r < 0:
