@@ -225,7 +225,9 @@ def single_instances(P, instances, device, with_ref):
 # --------------------------------------------------------------- served loop
 def served_loop(rate, n_req, seed, P, instances):
     """Poisson arrivals at `rate` req/s; KP (n~U{20..60}) / SP (n~U{60..100}) method 1 and
-    TSP (n~U{9..13}, method 3); latency = finish - arrival on the host clock.  Every
+    TSP (n~U{9..13}, method 3); latency = finish - arrival on the host clock.  Knapsack
+    and set-packing DDs are built on the host before the loop; a TSP request goes in by
+    its cost matrices (the server's shared n-city MDD on the device).  Every
     result's frontier CSV.gz and stats record are handed to the asynchronous writer as it
     is polled (the reference's per-request output); the writer's tail after the last
     result is reported beside the latencies."""
@@ -241,8 +243,9 @@ def served_loop(rate, n_req, seed, P, instances):
         elif kind == 1:
             specs.append((2, instances.setpacking_text(int(rng.integers(60, 101)), 20, 3, s), 1))
         else:
-            specs.append((3, instances.tsp_text(int(rng.integers(9, 14)), 3, s), 3))
-    dds = build_dds([(p, t, "") for p, t, _ in specs])
+            specs.append((3, instances.tsp_arrays(int(rng.integers(9, 14)), 3, s), 3))
+    built = iter(build_dds([(p, t, "") for p, t, _ in specs if p != 3]))
+    dds = [t if p == 3 else next(built) for p, t, _ in specs]
     gaps = rng.exponential(1.0 / rate, size=n_req)
     arrivals = np.cumsum(gaps)
     srv = P.Server()
@@ -256,7 +259,10 @@ def served_loop(rate, n_req, seed, P, instances):
     while finished < n_req:
         now = time.perf_counter() - t0
         while nxt < n_req and arrivals[nxt] <= now:
-            srv.submit(dds[nxt], nxt, method=specs[nxt][2])
+            if specs[nxt][0] == 3:
+                srv.submit_tsp(dds[nxt], nxt, method=specs[nxt][2])
+            else:
+                srv.submit(dds[nxt], nxt, method=specs[nxt][2])
             nxt += 1
         if srv.pending() == 0:
             if nxt < n_req:

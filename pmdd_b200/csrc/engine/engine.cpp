@@ -1423,7 +1423,8 @@ int Engine::step() {
                 size_t j = i;
                 while (j + 1 < g.second.size() && g.second[j + 1] == g.second[j] + 1) ++j;
                 const int n = static_cast<int>(j - i + 1);
-                const int per = std::max(1, (sms_ * 2) / n);
+                // three 256-thread blocks per SM: the prune kernel's register limit
+                const int per = std::max(1, (sms_ * 3) / n);
                 if (!cuda_ok(dev::launch_couple_round(std::get<0>(g.first), std::get<1>(g.first), du + g.second[i], n,
                                                       per, std::get<2>(g.first), stream_),
                              "coupling round"))
