@@ -346,9 +346,10 @@ __global__ void __launch_bounds__(kWriteThreads) big_write_kernel(const ExpandJo
 template <int D, typename T>
 __global__ void __launch_bounds__(SfsSmallCfg<D, T>::kThreads) big_sfs_kernel(const ExpandJob *__restrict__ jobs,
                                                                          const BigWork *__restrict__ work,
+                                                                         const int32_t *__restrict__ order,
                                                                          int64_t pass) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const BigWork W = work[blockIdx.x];
+    const BigWork W = work[order ? order[blockIdx.x] : blockIdx.x];
     const ExpandJob &J = jobs[W.job];
     BigItem B;
     if (!big_item(J, W, pass, &B) || B.n >= J.big_mark_min) return;
@@ -360,6 +361,48 @@ __global__ void __launch_bounds__(SfsSmallCfg<D, T>::kThreads) big_sfs_kernel(co
     const int32_t kept = sfs_block<D, T, SfsSmallCfg<D, T>>(smem_raw, static_cast<const T *>(J.big_pts) + B.soff * D,
                                                             B.n, s, static_cast<T *>(J.out_pts) + B.c0 * D);
     if (threadIdx.x == 0) J.out_size[B.item] = kept;
+}
+
+// SFS blocks largest destination first: one block sorts the pass's work list by
+// candidate count, descending (ties in list order; destinations outside the pass or for
+// the mark path count as empty), so that the longest blocks start first and the tail of
+// the launch is short.  num_work <= kBigOrderMax.
+__global__ void __launch_bounds__(1024) big_order_kernel(const ExpandJob *__restrict__ jobs,
+                                                         const BigWork *__restrict__ work, int num_work, int64_t pass,
+                                                         int32_t *__restrict__ order) {
+    __shared__ unsigned long long key[kBigOrderMax];
+    int m = 1;
+    while (m < num_work) m <<= 1;
+    constexpr unsigned long long kMaxN = (1ULL << 40) - 1;
+    for (int i = threadIdx.x; i < m; i += blockDim.x) {
+        unsigned long long k = ~0ULL;
+        if (i < num_work) {
+            const BigWork W = work[i];
+            const ExpandJob &J = jobs[W.job];
+            BigItem B;
+            unsigned long long n = 0;
+            if (big_item(J, W, pass, &B) && B.n < J.big_mark_min)
+                n = B.n > static_cast<int64_t>(kMaxN) ? kMaxN : static_cast<unsigned long long>(B.n);
+            k = ((kMaxN - n) << 12) | static_cast<unsigned long long>(i);
+        }
+        key[i] = k;
+    }
+    __syncthreads();
+    for (int k = 2; k <= m; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = threadIdx.x; i < m; i += blockDim.x) {
+                const int p = i ^ j;
+                if (p > i) {
+                    const unsigned long long a = key[i], b = key[p];
+                    if (((i & k) == 0) == (a > b)) {
+                        key[i] = b;
+                        key[p] = a;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    for (int i = threadIdx.x; i < num_work; i += blockDim.x) order[i] = static_cast<int32_t>(key[i] & 4095ULL);
 }
 
 template <int D, typename T>
@@ -376,7 +419,14 @@ static cudaError_t launch_big_t(const BigLaunch &L, cudaStream_t stream) {
     const int64_t want = (L.total + kFlatThreads - 1) / kFlatThreads;
     const unsigned grid = static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>(want, int64_t(L.sms) * 32)));
     big_expand_kernel<D, T><<<grid, kFlatThreads, 0, stream>>>(L.jobs, L.job_bases, L.num_jobs, L.total, L.pass);
-    if (L.with_sfs) big_sfs_kernel<D, T><<<L.num_work, Cfg::kThreads, Cfg::kSmem, stream>>>(L.jobs, L.work, L.pass);
+    if (L.with_sfs) {
+        const int32_t *order = nullptr;
+        if (L.order && L.num_work <= kBigOrderMax) {
+            big_order_kernel<<<1, 1024, 0, stream>>>(L.jobs, L.work, L.num_work, L.pass, L.order);
+            order = L.order;
+        }
+        big_sfs_kernel<D, T><<<L.num_work, Cfg::kThreads, Cfg::kSmem, stream>>>(L.jobs, L.work, order, L.pass);
+    }
     if (L.mark_cap > 0) {
         MarkPlan *plan = static_cast<MarkPlan *>(L.plan);
         big_plan_kernel<<<1, kPlanThreads, 0, stream>>>(L.jobs, L.work, L.num_work, L.pass, plan, L.mark_cap);

@@ -1371,6 +1371,17 @@ int Engine::step() {
         L.with_sfs = true;
         L.mark_cap = static_cast<int>(std::min<int64_t>(gl.mark_cap, static_cast<int64_t>(gl.big_count)));
         L.plan = nullptr;
+        // more SFS blocks than fit the SMs at once: start the largest destinations first
+        L.order = nullptr;
+        const bool ordered = L.num_work > sms_ * 3 && L.num_work <= dev::kBigOrderMax;
+        if (ordered) {
+            L.order = static_cast<int32_t *>(scratch(sizeof(int32_t) * static_cast<size_t>(L.num_work)));
+            if (!L.order) {
+                error_ = "engine bookkeeping allocation failed";
+                ok_ = false;
+                return -1;
+            }
+        }
         if (L.mark_cap > 0) {
             L.plan = scratch(dev::big_plan_bytes(L.mark_cap));
             if (!L.plan) {
@@ -1382,7 +1393,7 @@ int Engine::step() {
         for (int64_t pass = 0; pass < gl.big_passes; ++pass) {
             L.pass = pass;
             if (!cuda_ok(dev::launch_big(gl.d, gl.wide, L, stream_), "oversized-destination kernels")) return -1;
-            launches_ += L.mark_cap > 0 ? 5 : 2;
+            launches_ += (L.mark_cap > 0 ? 5 : 2) + (ordered ? 1 : 0);
         }
     }
     if (!sdjobs.empty()) {

@@ -28,7 +28,10 @@ struct BigLaunch {
     bool with_sfs;               // launch the SFS blocks (destinations below big_mark_min)
     void *plan;                  // big_plan_bytes(mark_cap) of scratch for the mark path
     int mark_cap;                // upper bound on mark-path destinations in the pass; 0: none
+    int32_t *order;              // num_work ints: SFS blocks largest destination first; nullptr: list order
 };
+// Most oversized destinations whose SFS blocks are put in size order (one block sorts them).
+constexpr int kBigOrderMax = 4096;
 size_t big_plan_bytes(int cap);
 cudaError_t launch_big(int d, bool wide, const BigLaunch &L, cudaStream_t stream);
 
