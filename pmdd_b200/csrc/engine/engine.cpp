@@ -948,6 +948,12 @@ int Engine::step() {
     std::vector<GroupLaunch> glaunch;
     std::vector<int64_t> tile_bases(exps.size()), item_bases(exps.size());  // group-relative
     std::vector<int64_t> big_bases(exps.size());                           // group-relative
+    // a step with fewer oversized destinations than SMs would leave most SMs idle with one
+    // SFS block each: send them all down the GPU-wide mark path instead (unless the
+    // crossover is fixed by PMDD_BIG_MARK_MIN)
+    int64_t step_big = 0;
+    for (const ExpPlan &e : exps) step_big += e.num_big;
+    const bool sparse_big = big_mark_min_fixed_ <= 0 && step_big > 0 && step_big < sms_;
     {
         size_t pos = 0;
         std::vector<ExpPlan> ordered;
@@ -1004,7 +1010,8 @@ int Engine::step() {
                     J.big_surv_idx = reinterpret_cast<int32_t *>(m + 3 * pb + ib);
                     J.big_window = e.big_window;
                     J.big_rows = e.big_rows;
-                    const int64_t mm = mark_min_for(I.d, I.opts.problem_type);
+                    const int64_t mm = sparse_big ? static_cast<int64_t>(dev::kSmallMax) + 1
+                                                  : mark_min_for(I.d, I.opts.problem_type);
                     J.big_mark_min = mm;
                     if (s.res.max_item >= mm) gl.mark_cap += e.big_rows / mm + 1;
                     gl.big_passes = std::max<int64_t>(gl.big_passes, (e.big_total + e.big_window - 1) / e.big_window);
