@@ -204,10 +204,10 @@ def single_instances(P, instances, device, with_ref):
         with open(path, "w") as f:
             f.write(text)
         for method in (1, 3):
-            P.enumerate_dd(dd, method=method)
+            P.enumerate_dd(dd, method=method, device=device)
             st = {}
             t0 = time.perf_counter()
-            pts = P.enumerate_dd(dd, method=method, stats=st)
+            pts = P.enumerate_dd(dd, method=method, stats=st, device=device)
             wall = time.perf_counter() - t0
             rec = {"instance": name, "method": method, "solutions": int(len(pts)),
                    "gpu_device_s": st["device_elapsed_s"], "gpu_call_s": wall,
@@ -223,7 +223,7 @@ def single_instances(P, instances, device, with_ref):
 
 
 # --------------------------------------------------------------- served loop
-def served_loop(rate, n_req, seed, P, instances):
+def served_loop(rate, n_req, seed, P, instances, device=0):
     """Poisson arrivals at `rate` req/s; KP (n~U{20..60}) / SP (n~U{60..100}) method 1 and
     TSP (n~U{9..13}, method 3); latency = finish - arrival on the host clock.  Knapsack
     and set-packing DDs are built on the host before the loop; a TSP request goes in by
@@ -248,7 +248,7 @@ def served_loop(rate, n_req, seed, P, instances):
     dds = [t if p == 3 else next(built) for p, t, _ in specs]
     gaps = rng.exponential(1.0 / rate, size=n_req)
     arrivals = np.cumsum(gaps)
-    srv = P.Server()
+    srv = P.Server(device=device)
     outdir = tempfile.mkdtemp(prefix="pmdd_served_")
     writer = FrontierWriter()
     t0 = time.perf_counter()
@@ -447,7 +447,7 @@ def main():
         flush.zero_()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        outs = P.enumerate_batch(dds, method=1)
+        outs = P.enumerate_batch(dds, method=1, device=device)
         t1 = time.perf_counter()
         if s >= args.warmup:
             e2e_wall += t1 - t0
@@ -485,7 +485,7 @@ def main():
         sub = dds if not args.quick else dds[::8]
         t0 = time.perf_counter()
         for d in sub:
-            P.enumerate_dd(d, method=1)
+            P.enumerate_dd(d, method=1, device=device)
         oat = len(sub) / (time.perf_counter() - t0)
         line["one_at_a_time"] = {"value": oat, "unit": "solves/s", "instances": len(sub),
                                  "batched_e2e_over_one_at_a_time": e2e_value / world / oat}
@@ -493,7 +493,7 @@ def main():
         served = []
         for rate in (50, 200, 800):
             n_req = {50: 100, 200: 200, 800: 400}[rate] // (4 if args.quick else 1)
-            served.append(served_loop(rate, n_req, rate, P, instances))
+            served.append(served_loop(rate, n_req, rate, P, instances, device))
         line["served"] = served
         # config-1 filter roofline: 1024 x KP d=3 n=40
         n1 = 256 if args.quick else 1024
@@ -532,7 +532,7 @@ def main():
         t0 = time.perf_counter()
         kdds = build_dds([(1, t, "") for t in kp_texts])
         t_hb = time.perf_counter() - t0
-        outs_h = P.enumerate_batch(kdds, method=1)
+        outs_h = P.enumerate_batch(kdds, method=1, device=device)
         t_host = time.perf_counter() - t0
         del kdds
         line["knapsack_with_construction"] = {
