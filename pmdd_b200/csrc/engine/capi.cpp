@@ -67,7 +67,14 @@ int64_t default_arena_bytes(int device) {
 
 // Caller holds slot.mu.
 int ensure_engine(int device, DeviceSlot &slot, std::string *err) {
-    if (slot.engine && slot.engine->ok()) return PMDD_OK;
+    if (slot.engine && slot.engine->ok()) {
+        // the calling thread may have another device current
+        if (!slot.engine->make_current()) {
+            *err = slot.engine->error();
+            return PMDD_ERR_CUDA;
+        }
+        return PMDD_OK;
+    }
     slot.engine.reset(new pmdd::Engine(device, default_arena_bytes(device), 0));
     slot.generation++;
     if (!slot.engine->ok()) {
@@ -858,6 +865,10 @@ int pmdd_resident_dd_copy(pmdd_resident *R, int32_t i, int32_t *layer_offsets, i
         return PMDD_ERR_CUDA;
     }
     const pmdd::Instance &T = *R->tmpl[i];
+    if (!slot.engine->make_current()) {
+        write_err(err, errlen, slot.engine->error());
+        return PMDD_ERR_CUDA;
+    }
     cudaStream_t st = slot.engine->stream();
     auto get = [&](void *dst, const void *src, size_t bytes) {
         return bytes == 0 || cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st) == cudaSuccess;

@@ -387,6 +387,10 @@ void prepare_tsp_instance(const TspStructure &S, int nobjs, const int32_t *cost,
 const TspStructure *Engine::tsp_structure(int n, std::string *err) {
     auto it = tsp_cache_.find(n);
     if (it != tsp_cache_.end()) return it->second.get();
+    if (!make_current()) {
+        *err = error_;
+        return nullptr;
+    }
     if (n < dev::kTspMinCities || n > dev::kTspMaxCities) {
         *err = "TSP structure: n must be in 2..20";
         return nullptr;
@@ -615,6 +619,10 @@ std::map<std::pair<int, int>, int64_t> read_tuning(const std::string &path) {
 
 void Engine::load_tuning() { tuned_mark_min_ = read_tuning(default_tuning_path()); }
 
+bool Engine::mark_min_set(int d, int problem_type) const {
+    return big_mark_min_fixed_ > 0 || tuned_mark_min_.count({d, problem_type}) > 0;
+}
+
 int64_t Engine::mark_min_for(int d, int problem_type) const {
     if (big_mark_min_fixed_ > 0) return big_mark_min_fixed_;
     auto it = tuned_mark_min_.find({d, problem_type});
@@ -707,7 +715,14 @@ bool Engine::carve_couple(Instance &I, int64_t ucap) {
     return true;
 }
 
+bool Engine::make_current() {
+    int cur = -1;
+    if (cudaGetDevice(&cur) == cudaSuccess && cur == device_) return true;
+    return cuda_ok(cudaSetDevice(device_), "cudaSetDevice");
+}
+
 bool Engine::upload_dd(Instance &I) {
+    if (!make_current()) return false;
     I.dd = static_cast<unsigned char *>(arena_.alloc(I.dev_bytes));
     if (!I.dd) return false;
     if (!cuda_ok(cudaMemcpyAsync(I.dd, I.blob_src ? I.blob_src : I.blob.data(), I.blob_bytes, cudaMemcpyHostToDevice, stream_), "DD upload"))
@@ -834,7 +849,7 @@ struct CountPlan {
 std::atomic<int64_t> g_total_launches{0};
 
 int Engine::step() {
-    if (!ok_) return -1;
+    if (!ok_ || !make_current()) return -1;
     const double step_t0 = trace_ ? now_s() : 0.0;
     struct LaunchTally {
         const int64_t &n;
@@ -949,11 +964,11 @@ int Engine::step() {
     std::vector<int64_t> tile_bases(exps.size()), item_bases(exps.size());  // group-relative
     std::vector<int64_t> big_bases(exps.size());                           // group-relative
     // a step with fewer oversized destinations than SMs would leave most SMs idle with one
-    // SFS block each: send them all down the GPU-wide mark path instead (unless the
-    // crossover is fixed by PMDD_BIG_MARK_MIN)
+    // SFS block each: with the built-in crossover, send them all down the GPU-wide mark
+    // path instead (a crossover fixed by PMDD_BIG_MARK_MIN or tuned for the family stands)
     int64_t step_big = 0;
     for (const ExpPlan &e : exps) step_big += e.num_big;
-    const bool sparse_big = big_mark_min_fixed_ <= 0 && step_big > 0 && step_big < sms_;
+    const bool sparse_big = step_big > 0 && step_big < sms_;
     {
         size_t pos = 0;
         std::vector<ExpPlan> ordered;
@@ -1010,8 +1025,9 @@ int Engine::step() {
                     J.big_surv_idx = reinterpret_cast<int32_t *>(m + 3 * pb + ib);
                     J.big_window = e.big_window;
                     J.big_rows = e.big_rows;
-                    const int64_t mm = sparse_big ? static_cast<int64_t>(dev::kSmallMax) + 1
-                                                  : mark_min_for(I.d, I.opts.problem_type);
+                    const int64_t mm = sparse_big && !mark_min_set(I.d, I.opts.problem_type)
+                                           ? static_cast<int64_t>(dev::kSmallMax) + 1
+                                           : mark_min_for(I.d, I.opts.problem_type);
                     J.big_mark_min = mm;
                     if (s.res.max_item >= mm) gl.mark_cap += e.big_rows / mm + 1;
                     gl.big_passes = std::max<int64_t>(gl.big_passes, (e.big_total + e.big_window - 1) / e.big_window);

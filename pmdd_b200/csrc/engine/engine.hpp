@@ -213,6 +213,9 @@ class Engine {
     // Device copy of a prepared request's DD (with the bottom-up CSR) that stays in
     // the arena until release_dd(); requests then share it via external_dd.
     bool upload_dd(Instance &I);
+    // Makes this engine's device current on the calling thread (a thread may drive the
+    // engines of several devices); every entry below that launches work calls it.
+    bool make_current();
     // Device pointers of a DD whose arrays are in I.dd (uploaded or built on the device),
     // and its bottom-up CSR when the instance carries one.
     bool bind_dd(Instance &I);
@@ -271,8 +274,11 @@ class Engine {
     bool trace_ = false;  // PMDD_TRACE=1: one stderr line per step
     // Oversized destinations of at least mark_min_for(d, problem type) candidates are
     // filtered by the GPU-wide mark/write pass instead of one SFS block: PMDD_BIG_MARK_MIN
-    // if set, else the tuned value for (d, problem type) from the tuning file, else 65536.
+    // if set, else the tuned value for (d, problem type) from the tuning file, else 65536
+    // (and, for that built-in value only, every oversized destination of a step that has
+    // fewer of them than SMs).
     int64_t mark_min_for(int d, int problem_type) const;
+    bool mark_min_set(int d, int problem_type) const;  // fixed or tuned, not built in
     void load_tuning();
     int64_t big_mark_min_fixed_ = 0;
     std::map<std::pair<int, int>, int64_t> tuned_mark_min_;
