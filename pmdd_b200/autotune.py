@@ -6,11 +6,16 @@ pairwise mark pass (more work, every SM).  The size from which the mark pass pay
 on the instance family: a knapsack stream has many mid-sized destinations, a 5-objective
 15-city TSP a few huge ones.  For each requested (objectives, problem type) this tuner
 times a calibration instance of that family under a list of crossover sizes, each in a
-fresh process (the engine reads PMDD_BIG_MARK_MIN at start-up), keeps the fastest, and
-writes the choice to the tuning file the engine reads at start-up:
+fresh process (the engine reads PMDD_BIG_MARK_MIN at start-up), and under the engine's
+built-in behaviour (65536, except that a step with fewer oversized destinations than SMs
+sends them all to the mark pass), keeps the fastest, and writes the choice to the tuning
+file the engine reads at start-up:
 
     {"version": 1, "entries": {"d<objectives>_p<problem type>": {"big_mark_min": n,
                                 "seconds": {"<n>": device seconds, ...}, "instance": "..."}}}
+
+A family for which the built-in behaviour is as fast as the best size gets an entry
+without "big_mark_min" ({"builtin": true, ...}), which the engine reads as untuned.
 
     python -m pmdd_b200.autotune --nobjs 3 5 --ptype 1 3 [--out PATH]
 
@@ -66,13 +71,18 @@ print(json.dumps({{"seconds": best}}))
 """
 
 
-def time_in_child(path: str, nobjs: int, problem_type: int, method: int, mark_min: int, repeats: int = 3,
-                  timeout: float = 600.0) -> Optional[float]:
+def time_in_child(path: str, nobjs: int, problem_type: int, method: int, mark_min: Optional[int],
+                  repeats: int = 3, timeout: float = 600.0) -> Optional[float]:
     """Best device time of `repeats` enumerations in a fresh process with the given
-    crossover; None if the run fails or times out."""
+    crossover (None: the engine's built-in behaviour, no tuning file); None if the run
+    fails or times out."""
     root = os.path.abspath(os.path.join(os.path.dirname(__file__), ".."))
     code = _CHILD.format(root=root, path=path, ptype=problem_type, nobjs=nobjs, method=method, repeats=repeats)
-    env = dict(os.environ, PMDD_BIG_MARK_MIN=str(int(mark_min)))
+    env = dict(os.environ, PMDD_TUNING_FILE=path + ".no-tuning.json")
+    if mark_min is None:
+        env.pop("PMDD_BIG_MARK_MIN", None)
+    else:
+        env["PMDD_BIG_MARK_MIN"] = str(int(mark_min))
     try:
         p = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=timeout)
     except subprocess.TimeoutExpired:
@@ -85,15 +95,18 @@ def time_in_child(path: str, nobjs: int, problem_type: int, method: int, mark_mi
         return None
 
 
-def choose(times: Dict[int, Optional[float]]) -> int:
-    """Fastest crossover.  Sizes within 2 % of the fastest tie: the default wins a tie
+def choose(times: Dict[int, Optional[float]], builtin: Optional[float] = None) -> Optional[int]:
+    """Fastest crossover, or None when the built-in behaviour (timed as `builtin`) is
+    within 2 % of the fastest.  Sizes within 2 % of the fastest tie: the default wins a tie
     (a calibration run whose destinations never reach the crossover says nothing about
     it), otherwise the larger size (fewer GPU-wide passes); no usable timing -> the
     default."""
     ok = {k: v for k, v in times.items() if v is not None}
     if not ok:
-        return DEFAULT_MARK_MIN
+        return None if builtin is not None else DEFAULT_MARK_MIN
     best = min(ok.values())
+    if builtin is not None and builtin <= best * 1.02:
+        return None
     tied = [k for k, v in ok.items() if v <= best * 1.02]
     return DEFAULT_MARK_MIN if DEFAULT_MARK_MIN in tied else max(tied)
 
@@ -112,8 +125,13 @@ def tune(families: Iterable[tuple], sizes: Sequence[int] = CANDIDATE_SIZES, meth
         with open(path, "w") as f:
             f.write(text)
         times = {int(s): timer(path, nobjs, ptype, method, int(s)) for s in sizes}
-        out[f"d{nobjs}_p{ptype}"] = {"big_mark_min": choose(times),
-                                     "seconds": {str(k): v for k, v in times.items()}, "instance": desc}
+        builtin = timer(path, nobjs, ptype, method, None)
+        seconds = {str(k): v for k, v in times.items()}
+        seconds["builtin"] = builtin
+        pick = choose(times, builtin)
+        entry = {"builtin": True} if pick is None else {"big_mark_min": pick}
+        entry.update({"seconds": seconds, "instance": desc})
+        out[f"d{nobjs}_p{ptype}"] = entry
     return out
 
 
@@ -146,7 +164,7 @@ def main(argv=None):
     entries = tune([(d, p) for d in args.nobjs for p in args.ptype])
     path = write(entries, args.out)
     for k, v in entries.items():
-        print(k, v["big_mark_min"], v["seconds"])
+        print(k, v.get("big_mark_min", "built-in"), v["seconds"])
     print("written", path)
 
 

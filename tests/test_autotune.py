@@ -24,12 +24,26 @@ def test_tune_with_a_fake_timer(tmp_path):
     def timer(path, nobjs, ptype, method, mark_min):
         calls.append((nobjs, ptype, mark_min))
         assert os.path.exists(path)
+        if mark_min is None:  # the built-in behaviour: slower for d=3, fastest for d=5
+            return 2.0 if nobjs == 3 else 0.5
         return 1.0 + abs(mark_min - 16384) / 1e6
 
     entries = autotune.tune([(3, 1), (5, 3)], sizes=(4096, 16384, 65536), timer=timer, workdir=str(tmp_path))
     assert set(entries) == {"d3_p1", "d5_p3"}
-    assert all(e["big_mark_min"] == 16384 for e in entries.values())
-    assert len(calls) == 6
+    assert entries["d3_p1"]["big_mark_min"] == 16384
+    assert entries["d5_p3"]["builtin"] is True and "big_mark_min" not in entries["d5_p3"]
+    assert len(calls) == 8
+    # the engine reads a built-in entry as untuned, the other one as tuned
+    path = autotune.write(entries, str(tmp_path / "t.json"))
+    lib = _native.gpu_lib()
+    assert lib.pmdd_tuned_mark_min(path.encode(), 3, 1) == 16384
+    assert lib.pmdd_tuned_mark_min(path.encode(), 5, 3) == 0
+
+
+def test_builtin_wins_ties():
+    assert autotune.choose({4096: 1.0, 65536: 2.0}, builtin=1.01) is None
+    assert autotune.choose({4096: 1.0, 65536: 2.0}, builtin=1.5) == 4096
+    assert autotune.choose({4096: None}, builtin=1.0) is None
 
 
 def test_calibration_instances_build():
