@@ -348,39 +348,50 @@ FlatDD build_indepset_bdd(const SetPackingData &sp, int nobjs) {
     check_nobjs(nobjs, sp.n_objs);
     const int n = sp.n_vars;
     const int W = (n + 63) / 64;
-    typedef std::vector<uint64_t> Bits;
-    // complement of the closed neighbourhood of each vertex
-    std::vector<Bits> keep(n, Bits(W, 0));
+    // complement of the closed neighbourhood of each vertex, W words each
+    std::vector<uint64_t> keep(static_cast<size_t>(n) * W, 0);
     {
-        std::vector<std::vector<char>> adj(n, std::vector<char>(n, 0));
+        std::vector<char> adj(static_cast<size_t>(n) * n, 0);
         for (const auto &cons : sp.vars_cons)
             for (size_t i = 0; i < cons.size(); ++i)
                 for (size_t j = i + 1; j < cons.size(); ++j) {
-                    adj[cons[i]][cons[j]] = 1;
-                    adj[cons[j]][cons[i]] = 1;
+                    adj[static_cast<size_t>(cons[i]) * n + cons[j]] = 1;
+                    adj[static_cast<size_t>(cons[j]) * n + cons[i]] = 1;
                 }
         for (int v = 0; v < n; ++v)
             for (int w = 0; w < n; ++w)
-                if (w != v && !adj[v][w]) keep[v][w / 64] |= (1ULL << (w % 64));
+                if (w != v && !adj[static_cast<size_t>(v) * n + w])
+                    keep[static_cast<size_t>(v) * W + w / 64] |= (1ULL << (w % 64));
     }
     BLayers L(n + 1);
     L[0].resize(1);
-    Bits root(W, 0);
-    for (int v = 0; v < n; ++v) root[v / 64] |= (1ULL << (v % 64));
-    std::vector<Bits> states(1, root);
+    // the states of a layer, flat (W words each), in node order
+    std::vector<uint64_t> states(W, 0), next;
+    for (int v = 0; v < n; ++v) states[v / 64] |= (1ULL << (v % 64));
+    size_t count = 1;
     std::vector<int> active(n);
     for (int v = 0; v < n; ++v) active[v] = v;
     std::vector<int> counter(n, 0);
     std::vector<int> var_layer(n, -1);
     std::vector<uint64_t> node_state;  // the states of every layer, in node order
+    std::vector<int32_t> table;        // open addressing: index of a next-layer state, -1 empty
+    std::vector<uint64_t> s0(W), s1(W);
+    auto hash_words = [W](const uint64_t *k) {
+        uint64_t h = 0x9e3779b97f4a7c15ULL;
+        for (int w = 0; w < W; ++w) {
+            h ^= k[w] + 0x9e3779b97f4a7c15ULL + (h << 6) + (h >> 2);
+            h *= 0xff51afd7ed558ccdULL;
+        }
+        return h ^ (h >> 32);
+    };
     for (int l = 1; l <= n; ++l) {
-        for (const Bits &s : states) node_state.insert(node_state.end(), s.begin(), s.end());
+        node_state.insert(node_state.end(), states.begin(), states.end());
         // min-in-state: vertex appearing in the fewest current states; ties go to the
         // first such entry of the active list, which shrinks by swap-with-last.
         for (int v : active) counter[v] = 0;
-        for (const Bits &s : states)
+        for (size_t i = 0; i < count; ++i)
             for (int w = 0; w < W; ++w) {
-                uint64_t x = s[w];
+                uint64_t x = states[i * W + w];
                 while (x) {
                     counter[w * 64 + __builtin_ctzll(x)]++;
                     x &= x - 1;
@@ -394,36 +405,45 @@ FlatDD build_indepset_bdd(const SetPackingData &sp, int nobjs) {
         active.pop_back();
         var_layer[l - 1] = vertex;
 
-        std::unordered_map<Bits, int32_t, WordsHash> map;
-        map.reserve(states.size() * 2 + 1);
-        std::vector<Bits> next;
-        auto lookup = [&](const Bits &s) -> int32_t {
-            auto it = map.find(s);
-            if (it != map.end()) return it->second;
-            const int32_t id = static_cast<int32_t>(next.size());
-            map.emplace(s, id);
-            next.push_back(s);
-            return id;
+        size_t cap = 16;
+        while (cap < 4 * count + 4) cap <<= 1;
+        table.assign(cap, -1);
+        next.clear();
+        int32_t next_count = 0;
+        // first sighting numbering: state i's 0-child, then its 1-child
+        auto lookup = [&](const uint64_t *k) -> int32_t {
+            size_t h = static_cast<size_t>(hash_words(k)) & (cap - 1);
+            for (;;) {
+                const int32_t id = table[h];
+                if (id < 0) {
+                    table[h] = next_count;
+                    next.insert(next.end(), k, k + W);
+                    return next_count++;
+                }
+                if (std::memcmp(next.data() + static_cast<size_t>(id) * W, k, sizeof(uint64_t) * W) == 0) return id;
+                h = (h + 1) & (cap - 1);
+            }
         };
         const uint64_t vbit = 1ULL << (vertex % 64);
         const int vw = vertex / 64;
-        Bits s0(W), s1(W);
-        for (size_t i = 0; i < states.size(); ++i) {
-            const Bits &s = states[i];
+        const uint64_t *kv = keep.data() + static_cast<size_t>(vertex) * W;
+        for (size_t i = 0; i < count; ++i) {
+            const uint64_t *s = states.data() + i * W;
             const bool was_set = (s[vw] & vbit) != 0;
-            s0 = s;
+            std::memcpy(s0.data(), s, sizeof(uint64_t) * W);
             s0[vw] &= ~vbit;
-            L[l - 1][i].arc[0] = lookup(s0);
+            L[l - 1][i].arc[0] = lookup(s0.data());
             if (was_set) {
-                for (int w = 0; w < W; ++w) s1[w] = s0[w] & keep[vertex][w];
-                L[l - 1][i].arc[1] = lookup(s1);
+                for (int w = 0; w < W; ++w) s1[w] = s0[w] & kv[w];
+                L[l - 1][i].arc[1] = lookup(s1.data());
             }
         }
-        L[l].resize(next.size());
+        L[l].resize(next_count);
         states.swap(next);
+        count = static_cast<size_t>(next_count);
     }
     if (L[n].size() != 1) throw std::runtime_error("independent-set BDD did not close to a single terminal");
-    node_state.insert(node_state.end(), states[0].begin(), states[0].end());
+    node_state.insert(node_state.end(), states.begin(), states.begin() + W);
     std::vector<std::vector<int>> one_w(n, std::vector<int>(nobjs, 0));
     for (int l = 0; l < n; ++l)
         for (int o = 0; o < nobjs; ++o) one_w[l][o] = sp.objs[o][var_layer[l]];
