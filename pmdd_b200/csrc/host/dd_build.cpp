@@ -12,6 +12,9 @@
 #include <fstream>
 #include <sstream>
 #include <stdexcept>
+#include <map>
+#include <memory>
+#include <mutex>
 #include <unordered_map>
 
 namespace pmdd {
@@ -464,9 +467,9 @@ FlatDD build_indepset_bdd(const SetPackingData &sp, int nobjs) {
 // city over states (visited set, last city), then the terminal reached by returning to
 // city 0.  Arc weights are negated costs (src/pmdd/mdd/tsp_mdd.cpp:21-196).
 // Weight row 0 is zero; row 1 + i*n + j holds -cost[.][i][j].
-FlatDD build_tsp_mdd(const TSPData &t, int nobjs) {
-    check_nobjs(nobjs, t.n_objs);
-    const int n = t.n_cities;
+// The layers, nodes and arcs (with their weight-row indices) of the n-city MDD: they
+// depend on n alone, never on the costs.
+static FlatDD tsp_structure(int n, int nobjs) {
     const int nl = n + 2;
     struct St {
         uint64_t S;
@@ -536,16 +539,36 @@ FlatDD build_tsp_mdd(const TSPData &t, int nobjs) {
                 ++a;
             }
         }
-    const size_t nn = static_cast<size_t>(n) * n;
-    f.weights.assign((1 + nn) * nobjs, 0);
-    for (size_t ij = 0; ij < nn; ++ij)
-        for (int o = 0; o < nobjs; ++o) f.weights[(1 + ij) * nobjs + o] = -t.cost[o * nn + ij];
     f.info.original_width = f.info.reduced_width = -1;
     f.info.original_num_nodes = f.info.reduced_num_nodes = -1;
     f.info.max_num_in_arcs = max_in;
     f.info.total_num_in_arcs = total_in;
     f.info.num_layers = nl;
     f.info.problem_type = 3;
+    return f;
+}
+
+// Structures of up to 16 cities are kept for the life of the process (all threads share
+// them); larger ones are built per call.
+FlatDD build_tsp_mdd(const TSPData &t, int nobjs) {
+    check_nobjs(nobjs, t.n_objs);
+    const int n = t.n_cities;
+    FlatDD f;
+    if (n >= 1 && n <= 16) {
+        static std::mutex mu;
+        static std::map<int, std::unique_ptr<FlatDD>> cache;
+        std::lock_guard<std::mutex> lk(mu);
+        std::unique_ptr<FlatDD> &c = cache[n];
+        if (!c) c.reset(new FlatDD(tsp_structure(n, 1)));
+        f = *c;
+    } else {
+        f = tsp_structure(n, nobjs);
+    }
+    f.nobjs = nobjs;
+    const size_t nn = static_cast<size_t>(n) * n;
+    f.weights.assign((1 + nn) * nobjs, 0);
+    for (size_t ij = 0; ij < nn; ++ij)
+        for (int o = 0; o < nobjs; ++o) f.weights[(1 + ij) * nobjs + o] = -t.cost[o * nn + ij];
     return f;
 }
 
