@@ -8,6 +8,7 @@
 
 #include <algorithm>
 #include <cctype>
+#include <climits>
 #include <cstring>
 #include <fstream>
 #include <sstream>
@@ -253,62 +254,159 @@ void check_nobjs(int nobjs, int have) {
 // (src/pmdd/bdd/knapsack_bdd.cpp:10-118); then reduction and the min-weight pass
 // (src/pmdd/bdd/knapsack_bdd.cpp:123-150).  The reference's second reduce + weight
 // pass (src/pmdd/main.cpp:143-153) finds nothing left to merge after the first one.
+// One constraint, non-negative weights: the reduced layers straight from dense arrays over
+// the used capacity 0..cap (the construction kpbuild.cu runs on the device).  Top-down, a
+// state's id is the rank of its first sighting (parents in id order, 0-arc before 1-arc),
+// as the map-based loop below numbers them; bottom-up, the feasible completions shrink as
+// the used capacity grows, so states whose (0-child, 1-child) classes agree are runs of
+// consecutive reachable states, and a class takes the rank of its smallest old id, as
+// reduce_bdd numbers them.  Returns false (nothing written) when the instance is not of
+// that form or the dense arrays would exceed 2^26 entries.
+static bool knapsack_dense_layers(const KnapsackData &k, BLayers *Lout, int64_t *ow, int64_t *on) {
+    const int n = k.n_vars;
+    if (n < 1 || k.n_cons != 1 || k.rhs[0] < 0) return false;
+    for (int l = 0; l < n; ++l)
+        if (k.coeffs[0][l] < 0) return false;
+    const int64_t cap = k.rhs[0], S = cap + 1;
+    if (static_cast<int64_t>(n) * S > (static_cast<int64_t>(1) << 26)) return false;
+    std::vector<int32_t> idx(static_cast<size_t>(n * S), -1);  // layers 0..n-1
+    std::vector<int32_t> width(n + 1, 0);
+    idx[0] = 0;
+    width[0] = 1;
+    std::vector<int64_t> key(static_cast<size_t>(S));
+    std::vector<int32_t> rank;
+    const int64_t kNone = INT64_MAX;
+    for (int l = 0; l + 1 < n; ++l) {
+        const int32_t *cur = idx.data() + l * S;
+        int32_t *nxt = idx.data() + (l + 1) * S;
+        const int64_t w = k.coeffs[0][l];
+        rank.assign(2 * static_cast<size_t>(width[l]), 0);
+        for (int64_t st = 0; st < S; ++st) {
+            int64_t kk = kNone;
+            if (cur[st] >= 0) kk = 2 * static_cast<int64_t>(cur[st]);
+            if (st >= w && cur[st - w] >= 0) kk = std::min(kk, 2 * static_cast<int64_t>(cur[st - w]) + 1);
+            key[st] = kk;
+            if (kk != kNone) rank[kk] = 1;
+        }
+        int32_t run = 0;
+        for (int32_t &r : rank) {
+            const int32_t x = r;
+            r = run;
+            run += x;
+        }
+        for (int64_t st = 0; st < S; ++st) nxt[st] = key[st] == kNone ? -1 : rank[key[st]];
+        width[l + 1] = run;
+    }
+    width[n] = 1;
+    BLayers &L = *Lout;
+    L.assign(n + 1, std::vector<BNode>());
+    L[n].resize(1);
+    std::vector<int32_t> remap_next(1, 0), remap_cur, class_of, first_of;
+    struct Cls {
+        int32_t c0, c1, minold;
+    };
+    std::vector<Cls> cls;
+    for (int l = n - 1; l >= 0; --l) {
+        const int32_t *cur = idx.data() + l * S;
+        const int32_t *nxt = l + 1 < n ? idx.data() + (l + 1) * S : nullptr;
+        const int64_t w = k.coeffs[0][l];
+        cls.clear();
+        class_of.assign(width[l], -1);
+        for (int64_t st = 0; st < S; ++st) {
+            const int32_t old = cur[st];
+            if (old < 0) continue;
+            const int32_t c0 = remap_next[nxt ? nxt[st] : 0];
+            const int32_t c1 = st + w <= cap ? remap_next[nxt ? nxt[st + w] : 0] : -1;
+            if (cls.empty() || cls.back().c0 != c0 || cls.back().c1 != c1) cls.push_back({c0, c1, old});
+            else cls.back().minold = std::min(cls.back().minold, old);
+            class_of[old] = static_cast<int32_t>(cls.size()) - 1;
+        }
+        // number the classes by their smallest old id
+        first_of.assign(width[l], -1);
+        for (size_t c = 0; c < cls.size(); ++c) first_of[cls[c].minold] = static_cast<int32_t>(c);
+        std::vector<int32_t> newid(cls.size(), -1);
+        int32_t next_id = 0;
+        for (int32_t x = 0; x < width[l]; ++x)
+            if (first_of[x] >= 0) newid[first_of[x]] = next_id++;
+        L[l].resize(cls.size());
+        for (size_t c = 0; c < cls.size(); ++c) {
+            L[l][newid[c]].arc[0] = cls[c].c0;
+            L[l][newid[c]].arc[1] = cls[c].c1;
+        }
+        remap_cur.assign(width[l], -1);
+        for (int32_t x = 0; x < width[l]; ++x)
+            if (class_of[x] >= 0) remap_cur[x] = newid[class_of[x]];
+        remap_next.swap(remap_cur);
+    }
+    *ow = 0;
+    *on = 0;
+    for (int l = 0; l <= n; ++l) {
+        *ow = std::max<int64_t>(*ow, width[l]);
+        *on += width[l];
+    }
+    return true;
+}
+
 FlatDD build_knapsack_bdd(const KnapsackData &k, int nobjs) {
     check_nobjs(nobjs, k.num_objs);
     const int n = k.n_vars, m = k.n_cons;
-    BLayers L(n + 1);
-    L[0].resize(1);
-    L[n].resize(1);  // terminal
-    std::vector<std::vector<int>> states(1, std::vector<int>(m, 0));
-    const bool single = (m == 1) && k.rhs[0] >= 0 && k.rhs[0] <= (1 << 26);
-    for (int l = 0; l < n; ++l) {
-        std::vector<std::vector<int>> next_states;
-        auto feasible_add = [&](const std::vector<int> &s, std::vector<int> *out) {
-            out->resize(m);
-            for (int c = 0; c < m; ++c) {
-                (*out)[c] = s[c] + k.coeffs[c][l];
-                if ((*out)[c] > k.rhs[c]) return false;
-            }
-            return true;
-        };
-        if (l < n - 1) {
-            std::unordered_map<std::vector<int>, int32_t, VecHash> map;
-            std::vector<int32_t> dense;
-            if (single) dense.assign(static_cast<size_t>(k.rhs[0]) + 1, -1);
-            auto lookup = [&](const std::vector<int> &s) -> int32_t {
-                if (single && s[0] >= 0) {
-                    int32_t &slot = dense[s[0]];
-                    if (slot < 0) {
-                        slot = static_cast<int32_t>(next_states.size());
-                        next_states.push_back(s);
-                    }
-                    return slot;
+    BLayers L;
+    int64_t ow = 0, on = 0;
+    const bool dense = knapsack_dense_layers(k, &L, &ow, &on);
+    if (!dense) {
+        L.assign(n + 1, std::vector<BNode>());
+        L[0].resize(1);
+        L[n].resize(1);  // terminal
+        std::vector<std::vector<int>> states(1, std::vector<int>(m, 0));
+        const bool single = (m == 1) && k.rhs[0] >= 0 && k.rhs[0] <= (1 << 26);
+        for (int l = 0; l < n; ++l) {
+            std::vector<std::vector<int>> next_states;
+            auto feasible_add = [&](const std::vector<int> &s, std::vector<int> *out) {
+                out->resize(m);
+                for (int c = 0; c < m; ++c) {
+                    (*out)[c] = s[c] + k.coeffs[c][l];
+                    if ((*out)[c] > k.rhs[c]) return false;
                 }
-                auto it = map.find(s);
-                if (it != map.end()) return it->second;
-                const int32_t id = static_cast<int32_t>(next_states.size());
-                map.emplace(s, id);
-                next_states.push_back(s);
-                return id;
+                return true;
             };
-            std::vector<int> s1;
-            for (size_t i = 0; i < states.size(); ++i) {
-                L[l][i].arc[0] = lookup(states[i]);
-                if (feasible_add(states[i], &s1)) L[l][i].arc[1] = lookup(s1);
-            }
-            L[l + 1].resize(next_states.size());
-            states.swap(next_states);
-        } else {
-            std::vector<int> s1;
-            for (size_t i = 0; i < states.size(); ++i) {
-                L[l][i].arc[0] = 0;
-                if (feasible_add(states[i], &s1)) L[l][i].arc[1] = 0;
+            if (l < n - 1) {
+                std::unordered_map<std::vector<int>, int32_t, VecHash> map;
+                std::vector<int32_t> dense;
+                if (single) dense.assign(static_cast<size_t>(k.rhs[0]) + 1, -1);
+                auto lookup = [&](const std::vector<int> &s) -> int32_t {
+                    if (single && s[0] >= 0) {
+                        int32_t &slot = dense[s[0]];
+                        if (slot < 0) {
+                            slot = static_cast<int32_t>(next_states.size());
+                            next_states.push_back(s);
+                        }
+                        return slot;
+                    }
+                    auto it = map.find(s);
+                    if (it != map.end()) return it->second;
+                    const int32_t id = static_cast<int32_t>(next_states.size());
+                    map.emplace(s, id);
+                    next_states.push_back(s);
+                    return id;
+                };
+                std::vector<int> s1;
+                for (size_t i = 0; i < states.size(); ++i) {
+                    L[l][i].arc[0] = lookup(states[i]);
+                    if (feasible_add(states[i], &s1)) L[l][i].arc[1] = lookup(s1);
+                }
+                L[l + 1].resize(next_states.size());
+                states.swap(next_states);
+            } else {
+                std::vector<int> s1;
+                for (size_t i = 0; i < states.size(); ++i) {
+                    L[l][i].arc[0] = 0;
+                    if (feasible_add(states[i], &s1)) L[l][i].arc[1] = 0;
+                }
             }
         }
+        layer_shape(L, &ow, &on);
+        reduce_bdd(L);
     }
-    int64_t ow, on;
-    layer_shape(L, &ow, &on);
-    reduce_bdd(L);
     int64_t rw, rn;
     layer_shape(L, &rw, &rn);
 
