@@ -8,19 +8,20 @@
 //       each runs the sort-filter-skyline of sfs.cuh, which compares each point only
 //       with the maxima found so far; many such destinations keep the GPU busy side by
 //       side;
-//   big_plan_kernel, big_mark_kernel, big_write_kernel: destinations of big_mark_min
-//       candidates and more, whose single SFS block would outlast the rest of the step.
-//       The plan lists their 256-candidate chunks; one mark block per chunk streams the
-//       destination's candidates through shared memory and sweeps every other arc run
-//       with warp-uniform broadcast reads (shifts of one non-dominated, duplicate-free
-//       parent frontier never dominate each other; a point before the run dominates on
-//       >= alone, a point after it only when it also differs, so of equal points the
-//       first stays) and stops once its candidates are all dominated; one block per
-//       destination then compacts the survivors into the slot.
+//   big_plan_kernel .. big_write_kernel: destinations of big_mark_min candidates and
+//       more, whose single SFS block would outlast the rest of the step.  The plan lists
+//       their 256-candidate chunks.  big_pivot_kernel picks each destination's pivots (the
+//       candidates of largest objective sum, from a sorted sample of sums);
+//       big_prefilter_kernel drops every candidate a pivot dominates; big_compact_kernel
+//       packs the rest, in candidate order; big_rplan_kernel lists their chunks; one
+//       big_mark_kernel block per chunk streams the remaining rows through shared memory
+//       with warp-uniform broadcast reads and stops once its rows are all dominated (of
+//       equal points the first stays); one big_write_kernel block per destination
+//       compacts the survivors into the slot.  The pivots leave the pairwise sweep a
+//       fraction of the candidates, and it costs the square of what it is given.
 //
-// Measured on the 5-objective 15-city TSP, a 1.08 M-candidate destination takes 0.54 s
-// on the mark path against 34 s in one SFS block, while for steps of thousands of
-// mid-sized destinations the SFS blocks win (they do less work than the all-pairs sweep).
+// For steps of thousands of mid-sized destinations the SFS blocks win (they do less work
+// than the pairwise sweep); for a few huge ones the mark path does.
 #include "kernels.cuh"
 #include "sfs.cuh"
 
@@ -124,25 +125,59 @@ __device__ __forceinline__ int32_t run_of(const ExpandJob &J, const BigItem &B, 
     return lo;
 }
 
-// Chunks of the destinations that take the mark path in one pass: work item work_idx[h]
-// owns chunks [chunk_base[h], chunk_base[h + 1]).
+// The destinations that take the mark path in one pass.  Destination h is work item
+// work_idx[h]; its candidates form chunks [chunk_base[h], chunk_base[h + 1]) of 256, its
+// piv_count[h] pivots sit in big_surv / big_surv_idx, the r_count[h] candidates no pivot
+// dominates sit in big_pts2 and form chunks [rchunk_base[h], rchunk_base[h + 1]).
 struct MarkPlan {
     int32_t count;
     int32_t pad;
-    int64_t total;
-    // followed by int32 work_idx[cap] and int64 chunk_base[cap + 1] (see plan_arrays)
+    int64_t total;   // chunks over all candidates
+    int64_t rtotal;  // chunks over the candidates left by the pivots
 };
 
-__device__ __forceinline__ void plan_arrays(MarkPlan *plan, int cap, int32_t **work_idx, int64_t **chunk_base) {
-    char *p = reinterpret_cast<char *>(plan) + 256;
-    *work_idx = reinterpret_cast<int32_t *>(p);
-    *chunk_base = reinterpret_cast<int64_t *>(p + ((static_cast<size_t>(cap) * 4 + 255) & ~static_cast<size_t>(255)));
+struct PlanArrays {
+    int32_t *work_idx;     // [cap]
+    int64_t *chunk_base;   // [cap + 1]
+    int64_t *rchunk_base;  // [cap + 1]
+    int64_t *r_count;      // [cap]
+    int32_t *piv_count;    // [cap]
+};
+
+__host__ __device__ __forceinline__ size_t plan_round(size_t b) { return (b + 255) & ~static_cast<size_t>(255); }
+
+__device__ __forceinline__ PlanArrays plan_arrays(const MarkPlan *plan, int cap) {
+    char *p = reinterpret_cast<char *>(const_cast<MarkPlan *>(plan)) + 256;
+    const size_t c = static_cast<size_t>(cap);
+    PlanArrays A;
+    A.work_idx = reinterpret_cast<int32_t *>(p);
+    p += plan_round(c * 4);
+    A.chunk_base = reinterpret_cast<int64_t *>(p);
+    p += plan_round((c + 1) * 8);
+    A.rchunk_base = reinterpret_cast<int64_t *>(p);
+    p += plan_round((c + 1) * 8);
+    A.r_count = reinterpret_cast<int64_t *>(p);
+    p += plan_round(c * 8);
+    A.piv_count = reinterpret_cast<int32_t *>(p);
+    return A;
+}
+
+// The destination of mark-path chunk b (chunk bases `base` over plan->count destinations).
+__device__ __forceinline__ int chunk_owner(const int64_t *base, int count, int64_t b) {
+    int lo = 0, hi = count - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (base[mid] <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
 }
 
 }  // namespace
 
 size_t big_plan_bytes(int cap) {
-    return 256 + ((static_cast<size_t>(cap) * 4 + 255) & ~static_cast<size_t>(255)) + 8 * (static_cast<size_t>(cap) + 1);
+    const size_t c = static_cast<size_t>(cap);
+    return 256 + plan_round(c * 4) + 2 * plan_round((c + 1) * 8) + plan_round(c * 8) + plan_round(c * 4);
 }
 
 // Materialise the oversized candidates of one pass (AoS, D values each).
@@ -172,9 +207,9 @@ __global__ void __launch_bounds__(kPlanThreads) big_plan_kernel(const ExpandJob 
                                                                 int64_t pass, MarkPlan *plan, int cap) {
     __shared__ int64_t warp_buf[32];
     __shared__ int64_t s_total;
-    int32_t *work_idx;
-    int64_t *chunk_base;
-    plan_arrays(plan, cap, &work_idx, &chunk_base);
+    const PlanArrays A = plan_arrays(plan, cap);
+    int32_t *work_idx = A.work_idx;
+    int64_t *chunk_base = A.chunk_base;
     int64_t chunks = 0, count = 0;
     for (int b0 = 0; b0 < num_work; b0 += kPlanThreads) {
         const int w = b0 + threadIdx.x;
@@ -242,7 +277,202 @@ __device__ __forceinline__ bool sweep_after(const PackedPt<D, T> *ys, int a, int
     return dom;
 }
 
-// One block per planned chunk of 256 candidates (grid: an upper bound; extra blocks leave).
+// Pivots: the candidates of largest objective sum, about pivot_target(n) of a destination's
+// n.  A candidate that a pivot dominates is dropped at once.  Whatever dominates a remaining
+// candidate is itself remaining (a pivot dominating the dominator would dominate the
+// candidate as well, equal points included), so the exact pairwise sweep then runs over the
+// remaining candidates only: on 5-objective TSP destinations about a quarter of them.
+constexpr int kPivotThreads = 1024;
+constexpr int kPivotSample = 4096;
+constexpr int kPivotMax = 8192;
+constexpr int kCompactThreads = 1024;
+
+__device__ __forceinline__ int64_t pivot_target(int64_t n) {
+    const int64_t t = n / 64;
+    return t < 512 ? 512 : (t > 4096 ? 4096 : t);
+}
+
+// Objective sum as the pivot ranking key; it wraps for int64 objectives, which changes only
+// the choice of pivots, never the result.
+template <int D, typename T>
+__device__ __forceinline__ long long pivot_key(const T *p) {
+    unsigned long long s = 0;
+#pragma unroll
+    for (int o = 0; o < D; ++o) s += static_cast<unsigned long long>(static_cast<long long>(p[o]));
+    return static_cast<long long>(s);
+}
+
+// One block per mark-path destination: the sums of an even sample of up to 4096 candidates,
+// sorted, give the threshold of the pivot_target(n) largest; the candidates at or above it
+// (the first kPivotMax in candidate order) are copied with their positions to the
+// destination's big_surv / big_surv_idx rows.
+template <int D, typename T>
+__global__ void __launch_bounds__(kPivotThreads) big_pivot_kernel(const ExpandJob *__restrict__ jobs,
+                                                                  const BigWork *__restrict__ work, int64_t pass,
+                                                                  const MarkPlan *__restrict__ plan, int cap) {
+    __shared__ long long key[kPivotSample];
+    __shared__ int32_t warp_buf[32];
+    __shared__ int32_t s_total;
+    const int h = blockIdx.x;
+    if (h >= plan->count) return;
+    const PlanArrays A = plan_arrays(plan, cap);
+    const BigWork W = work[A.work_idx[h]];
+    const ExpandJob &J = jobs[W.job];
+    BigItem B;
+    big_item(J, W, pass, &B);
+    const int64_t n = B.n;
+    if (n >= 0x7fffffffLL) {  // positions are int32: no pivots, every candidate stays
+        if (threadIdx.x == 0) A.piv_count[h] = 0;
+        return;
+    }
+    const T *P = static_cast<const T *>(J.big_pts) + B.soff * D;
+    T *PV = static_cast<T *>(J.big_surv) + B.soff * D;
+    int32_t *PI = J.big_surv_idx + B.soff;
+    const int m = n < kPivotSample ? static_cast<int>(n) : kPivotSample;
+    int msz = 1;
+    while (msz < m) msz <<= 1;
+    constexpr long long kLowest = -0x7fffffffffffffffLL - 1;
+    for (int k = threadIdx.x; k < msz; k += kPivotThreads)
+        key[k] = k < m ? pivot_key<D, T>(P + (static_cast<int64_t>(k) * n / m) * D) : kLowest;
+    __syncthreads();
+    for (int k = 2; k <= msz; k <<= 1)  // bitonic sort, descending
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = threadIdx.x; i < msz; i += kPivotThreads) {
+                const int q = i ^ j;
+                if (q > i) {
+                    const long long a = key[i], b = key[q];
+                    if (((i & k) == 0) == (a < b)) {
+                        key[i] = b;
+                        key[q] = a;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    int64_t r = (static_cast<int64_t>(m) * pivot_target(n) + n - 1) / n - 1;
+    r = r < 0 ? 0 : (r >= m ? m - 1 : r);
+    const long long tau = key[r];
+    int32_t carry = 0;
+    for (int64_t b0 = 0; b0 < n && carry < kPivotMax; b0 += kPivotThreads) {
+        const int64_t i = b0 + threadIdx.x;
+        const int32_t sel = (i < n && pivot_key<D, T>(P + i * D) >= tau) ? 1 : 0;
+        const int32_t ex = block_exclusive_scan<int32_t, kPivotThreads>(sel, warp_buf, &s_total);
+        const int32_t pos = carry + ex;
+        if (sel && pos < kPivotMax) {
+#pragma unroll
+            for (int o = 0; o < D; ++o) PV[static_cast<int64_t>(pos) * D + o] = P[i * D + o];
+            PI[pos] = static_cast<int32_t>(i);
+        }
+        carry += s_total;
+    }
+    if (threadIdx.x == 0) A.piv_count[h] = carry < kPivotMax ? carry : kPivotMax;
+}
+
+// One block per 256-candidate chunk (grid: an upper bound; extra blocks leave): flags, in
+// the keep bytes, the candidates no pivot dominates (of equal points the earlier one
+// dominates).
+template <int D, typename T>
+__global__ void __launch_bounds__(kMarkThreads) big_prefilter_kernel(const ExpandJob *__restrict__ jobs,
+                                                                     const BigWork *__restrict__ work, int64_t pass,
+                                                                     const MarkPlan *__restrict__ plan, int cap) {
+    constexpr int TY = MarkCfg<D, T>::kTile;
+    __shared__ PackedPt<D, T> ys[TY];
+    __shared__ int32_t yi[TY];
+    const int64_t b = blockIdx.x;
+    if (b >= plan->total) return;
+    const PlanArrays A = plan_arrays(plan, cap);
+    const int h = chunk_owner(A.chunk_base, plan->count, b);
+    const BigWork W = work[A.work_idx[h]];
+    const ExpandJob &J = jobs[W.job];
+    BigItem B;
+    big_item(J, W, pass, &B);
+    const T *P = static_cast<const T *>(J.big_pts) + B.soff * D;
+    const T *PV = static_cast<const T *>(J.big_surv) + B.soff * D;
+    const int32_t *PI = J.big_surv_idx + B.soff;
+    uint8_t *flag = reinterpret_cast<uint8_t *>(J.big_idx) + B.soff;
+    const int npiv = A.piv_count[h];
+    const int64_t i = (b - A.chunk_base[h]) * kMarkThreads + threadIdx.x;
+    const bool valid = i < B.n;
+    T p[D];
+#pragma unroll
+    for (int o = 0; o < D; ++o) p[o] = valid ? P[i * D + o] : T(0);
+    bool dom = !valid;
+    for (int t0 = 0; t0 < npiv; t0 += TY) {
+        const int cnt = npiv - t0 < TY ? npiv - t0 : TY;
+        for (int k = threadIdx.x; k < cnt; k += kMarkThreads) {
+            ys[k] = load_global_pt<D, T>(PV, t0 + k);
+            yi[k] = PI[t0 + k];
+        }
+        __syncthreads();
+        if (!__all_sync(kFull, dom)) {
+            for (int j = 0; j < cnt; ++j) {
+                const PackedPt<D, T> c = ys[j];
+                dom |= ge_all<D, T>(c, p) && (yi[j] < i || !eq_all<D, T>(c, p));
+                if ((j & 31) == 31 && __all_sync(kFull, dom)) break;
+            }
+        }
+        if (__syncthreads_and(dom)) break;  // also: the tile may be overwritten now
+    }
+    if (valid) flag[i] = dom ? 0 : 1;
+}
+
+// One block per mark-path destination: the flagged candidates, in candidate order, into
+// the destination's big_pts2 rows.
+template <int D, typename T>
+__global__ void __launch_bounds__(kCompactThreads) big_compact_kernel(const ExpandJob *__restrict__ jobs,
+                                                                      const BigWork *__restrict__ work, int64_t pass,
+                                                                      const MarkPlan *__restrict__ plan, int cap) {
+    __shared__ int32_t warp_buf[32];
+    __shared__ int32_t s_total;
+    const int h = blockIdx.x;
+    if (h >= plan->count) return;
+    const PlanArrays A = plan_arrays(plan, cap);
+    const BigWork W = work[A.work_idx[h]];
+    const ExpandJob &J = jobs[W.job];
+    BigItem B;
+    big_item(J, W, pass, &B);
+    const T *P = static_cast<const T *>(J.big_pts) + B.soff * D;
+    T *R = static_cast<T *>(J.big_pts2) + B.soff * D;
+    const uint8_t *flag = reinterpret_cast<const uint8_t *>(J.big_idx) + B.soff;
+    int64_t carry = 0;
+    for (int64_t b0 = 0; b0 < B.n; b0 += kCompactThreads) {
+        const int64_t i = b0 + threadIdx.x;
+        const int32_t k = i < B.n ? flag[i] : 0;
+        const int32_t ex = block_exclusive_scan<int32_t, kCompactThreads>(k, warp_buf, &s_total);
+        if (k) {
+#pragma unroll
+            for (int o = 0; o < D; ++o) R[(carry + ex) * D + o] = P[i * D + o];
+        }
+        carry += s_total;
+    }
+    if (threadIdx.x == 0) A.r_count[h] = carry;
+}
+
+// One block: the 256-row chunks of the pivot-filtered rows.
+__global__ void __launch_bounds__(kPlanThreads) big_rplan_kernel(MarkPlan *plan, int cap) {
+    __shared__ int64_t warp_buf[32];
+    __shared__ int64_t s_total;
+    const PlanArrays A = plan_arrays(plan, cap);
+    const int count = plan->count;
+    int64_t chunks = 0;
+    for (int b0 = 0; b0 < count; b0 += kPlanThreads) {
+        const int h = b0 + threadIdx.x;
+        const int64_t nch = h < count ? (A.r_count[h] + kMarkThreads - 1) / kMarkThreads : 0;
+        const int64_t cb = chunks + block_exclusive_scan<int64_t, kPlanThreads>(nch, warp_buf, &s_total);
+        if (h < count) A.rchunk_base[h] = cb;
+        chunks += s_total;
+    }
+    if (threadIdx.x == 0) {
+        A.rchunk_base[count] = chunks;
+        plan->rtotal = chunks;
+    }
+}
+
+// One block per 256 pivot-filtered rows (grid: an upper bound; extra blocks leave): each
+// row streams all rows of its destination through shared memory with warp-uniform broadcast
+// reads and stops once its block's rows are all dominated.  Rows keep candidate order, so a
+// row before the warp's 32 dominates on >= alone, one after them only when it also differs
+// (of equal points the first stays).
 template <int D, typename T>
 __global__ void __launch_bounds__(kMarkThreads) big_mark_kernel(const ExpandJob *__restrict__ jobs,
                                                                 const BigWork *__restrict__ work, int64_t pass,
@@ -250,59 +480,39 @@ __global__ void __launch_bounds__(kMarkThreads) big_mark_kernel(const ExpandJob 
     constexpr int TY = MarkCfg<D, T>::kTile;
     __shared__ PackedPt<D, T> ys[TY];
     const int64_t b = blockIdx.x;
-    if (b >= plan->total) return;
-    int32_t *work_idx;
-    int64_t *chunk_base;
-    plan_arrays(const_cast<MarkPlan *>(plan), cap, &work_idx, &chunk_base);
-    int lo = 0, hi = plan->count - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (chunk_base[mid] <= b) lo = mid;
-        else hi = mid - 1;
-    }
-    const BigWork W = work[work_idx[lo]];
+    if (b >= plan->rtotal) return;
+    const PlanArrays A = plan_arrays(plan, cap);
+    const int h = chunk_owner(A.rchunk_base, plan->count, b);
+    const BigWork W = work[A.work_idx[h]];
     const ExpandJob &J = jobs[W.job];
     BigItem B;
     big_item(J, W, pass, &B);  // the plan only lists destinations of this pass
-    const int64_t base = (b - chunk_base[lo]) * kMarkThreads;
-    const T *P = static_cast<const T *>(J.big_pts) + B.soff * D;
+    const int64_t n = A.r_count[h];
+    const T *R = static_cast<const T *>(J.big_pts2) + B.soff * D;
     uint8_t *keep = reinterpret_cast<uint8_t *>(J.big_idx) + B.soff;
-    const int tid = threadIdx.x;
-    const int64_t i = base + tid;
-    const bool valid = i < B.n;
-    int64_t rs = 0, re = 0;
+    const int64_t base = (b - A.rchunk_base[h]) * kMarkThreads;
+    const int64_t i = base + threadIdx.x;
+    const int64_t w0 = base + (threadIdx.x & ~31);
+    const bool valid = i < n;
     T p[D];
-    if (valid) {
-        run_of(J, B, i, &rs, &re);
 #pragma unroll
-        for (int o = 0; o < D; ++o) p[o] = P[i * D + o];
-    } else {
-#pragma unroll
-        for (int o = 0; o < D; ++o) p[o] = T(0);
-    }
-    const int64_t rs0 = __shfl_sync(kFull, rs, 0), re0 = __shfl_sync(kFull, re, 0);
-    const bool uni = __all_sync(kFull, valid && rs == rs0 && re == re0);
+    for (int o = 0; o < D; ++o) p[o] = valid ? R[i * D + o] : T(0);
     bool dom = !valid;
-    for (int64_t t0 = 0; t0 < B.n; t0 += TY) {
-        const int cnt = static_cast<int>(B.n - t0 < TY ? B.n - t0 : TY);
-        for (int k = tid; k < cnt; k += kMarkThreads) ys[k] = load_global_pt<D, T>(P, t0 + k);
+    for (int64_t t0 = 0; t0 < n; t0 += TY) {
+        const int cnt = static_cast<int>(n - t0 < TY ? n - t0 : TY);
+        for (int k = threadIdx.x; k < cnt; k += kMarkThreads) ys[k] = load_global_pt<D, T>(R, t0 + k);
         __syncthreads();
         if (!__all_sync(kFull, dom)) {
-            if (uni) {
-                // tile positions before the run, then after it
-                const int64_t bb = rs0 - t0, aa = re0 - t0;
-                const int b_end = static_cast<int>(bb < 0 ? 0 : (bb > cnt ? cnt : bb));
-                const int a_beg = static_cast<int>(aa < 0 ? 0 : (aa > cnt ? cnt : aa));
-                dom = sweep_before<D, T>(ys, 0, b_end, p, dom);
-                if (!__all_sync(kFull, dom)) dom = sweep_after<D, T>(ys, a_beg, cnt, p, dom);
-            } else {
-                for (int j = 0; j < cnt; ++j) {
-                    const int64_t jg = t0 + j;
+            const int64_t bb = w0 - t0, aa = w0 + 32 - t0;
+            const int b_end = static_cast<int>(bb < 0 ? 0 : (bb > cnt ? cnt : bb));
+            const int a_beg = static_cast<int>(aa < 0 ? 0 : (aa > cnt ? cnt : aa));
+            dom = sweep_before<D, T>(ys, 0, b_end, p, dom);
+            if (!__all_sync(kFull, dom)) {
+                for (int j = b_end; j < a_beg; ++j) {  // the warp's own rows
                     const PackedPt<D, T> c = ys[j];
-                    if (!dom && (jg < rs || jg >= re) && ge_all<D, T>(c, p) && (jg < i || !eq_all<D, T>(c, p)))
-                        dom = true;
-                    if ((j & 31) == 31 && __all_sync(kFull, dom)) break;
+                    dom |= ge_all<D, T>(c, p) && (t0 + j < i || !eq_all<D, T>(c, p));
                 }
+                dom = sweep_after<D, T>(ys, a_beg, cnt, p, dom);
             }
         }
         if (__syncthreads_and(dom)) break;  // also: the tile may be overwritten now
@@ -310,7 +520,8 @@ __global__ void __launch_bounds__(kMarkThreads) big_mark_kernel(const ExpandJob 
     if (valid) keep[i] = dom ? 0 : 1;
 }
 
-// One block per planned destination (grid: `cap`; extra blocks leave).
+// One block per planned destination (grid: `cap`; extra blocks leave): the kept rows, in
+// candidate order, into the destination's slot.
 template <int D, typename T>
 __global__ void __launch_bounds__(kWriteThreads) big_write_kernel(const ExpandJob *__restrict__ jobs,
                                                                   const BigWork *__restrict__ work, int64_t pass,
@@ -318,24 +529,23 @@ __global__ void __launch_bounds__(kWriteThreads) big_write_kernel(const ExpandJo
     __shared__ int32_t warp_buf[32];
     __shared__ int32_t s_total;
     if (static_cast<int>(blockIdx.x) >= plan->count) return;
-    int32_t *work_idx;
-    int64_t *chunk_base;
-    plan_arrays(const_cast<MarkPlan *>(plan), cap, &work_idx, &chunk_base);
-    const BigWork W = work[work_idx[blockIdx.x]];
+    const PlanArrays A = plan_arrays(plan, cap);
+    const BigWork W = work[A.work_idx[blockIdx.x]];
     const ExpandJob &J = jobs[W.job];
     BigItem B;
     big_item(J, W, pass, &B);
-    const T *P = static_cast<const T *>(J.big_pts) + B.soff * D;
+    const int64_t n = A.r_count[blockIdx.x];
+    const T *R = static_cast<const T *>(J.big_pts2) + B.soff * D;
     const uint8_t *keep = reinterpret_cast<const uint8_t *>(J.big_idx) + B.soff;
     T *out = static_cast<T *>(J.out_pts) + B.c0 * D;
     int64_t carry = 0;
-    for (int64_t b0 = 0; b0 < B.n; b0 += kWriteThreads) {
+    for (int64_t b0 = 0; b0 < n; b0 += kWriteThreads) {
         const int64_t i = b0 + threadIdx.x;
-        const int32_t k = i < B.n ? keep[i] : 0;
+        const int32_t k = i < n ? keep[i] : 0;
         const int32_t ex = block_exclusive_scan<int32_t, kWriteThreads>(k, warp_buf, &s_total);
         if (k) {
 #pragma unroll
-            for (int o = 0; o < D; ++o) out[(carry + ex) * D + o] = P[i * D + o];
+            for (int o = 0; o < D; ++o) out[(carry + ex) * D + o] = R[i * D + o];
         }
         carry += s_total;
     }
@@ -431,9 +641,12 @@ static cudaError_t launch_big_t(const BigLaunch &L, cudaStream_t stream) {
         MarkPlan *plan = static_cast<MarkPlan *>(L.plan);
         big_plan_kernel<<<1, kPlanThreads, 0, stream>>>(L.jobs, L.work, L.num_work, L.pass, plan, L.mark_cap);
         // chunks: at most one per 256 candidates of the pass plus one per listed destination
-        const int64_t chunks = (L.total + kMarkThreads - 1) / kMarkThreads + L.mark_cap;
-        big_mark_kernel<D, T><<<static_cast<unsigned>(chunks), kMarkThreads, 0, stream>>>(L.jobs, L.work, L.pass, plan,
-                                                                                         L.mark_cap);
+        const unsigned chunks = static_cast<unsigned>((L.total + kMarkThreads - 1) / kMarkThreads + L.mark_cap);
+        big_pivot_kernel<D, T><<<L.mark_cap, kPivotThreads, 0, stream>>>(L.jobs, L.work, L.pass, plan, L.mark_cap);
+        big_prefilter_kernel<D, T><<<chunks, kMarkThreads, 0, stream>>>(L.jobs, L.work, L.pass, plan, L.mark_cap);
+        big_compact_kernel<D, T><<<L.mark_cap, kCompactThreads, 0, stream>>>(L.jobs, L.work, L.pass, plan, L.mark_cap);
+        big_rplan_kernel<<<1, kPlanThreads, 0, stream>>>(plan, L.mark_cap);
+        big_mark_kernel<D, T><<<chunks, kMarkThreads, 0, stream>>>(L.jobs, L.work, L.pass, plan, L.mark_cap);
         big_write_kernel<D, T><<<L.mark_cap, kWriteThreads, 0, stream>>>(L.jobs, L.work, L.pass, plan, L.mark_cap);
     }
     return cudaGetLastError();

@@ -1416,7 +1416,7 @@ int Engine::step() {
         for (int64_t pass = 0; pass < gl.big_passes; ++pass) {
             L.pass = pass;
             if (!cuda_ok(dev::launch_big(gl.d, gl.wide, L, stream_), "oversized-destination kernels")) return -1;
-            launches_ += (L.mark_cap > 0 ? 5 : 2) + (ordered ? 1 : 0);
+            launches_ += (L.mark_cap > 0 ? 9 : 2) + (ordered ? 1 : 0);
         }
     }
     if (!sdjobs.empty()) {

@@ -152,8 +152,14 @@ import numpy as np
 import oracle
 import pmdd_b200 as P
 from pmdd_b200 import instances
+rng = np.random.default_rng(1)
+ties = ["5", "10"]  # 5-objective 10-city TSP with costs 0..2: equal candidates from different arcs
+for _ in range(5):
+    m = rng.integers(0, 3, size=(10, 10))
+    np.fill_diagonal(m, 0)
+    ties += [" ".join(str(int(x)) for x in row) for row in m]
 cases = [(3, 5, instances.tsp_text(10, 5, 77)), (1, 3, instances.knapsack_text(48, 3, 4)),
-         (1, 3, instances.knapsack_text(30, 3, 9))]
+         (1, 3, instances.knapsack_text(30, 3, 9)), (3, 5, "\n".join(ties) + "\n"), (3, 7, instances.tsp_text(9, 7, 3))]
 for ptype, d, text in cases:
     dd = P.DecisionDiagram.from_text(text, ptype, d)
     for method in (1, 3):
