@@ -1,15 +1,14 @@
 """Autotuner for the oversized-destination crossover, cached per (objectives, problem type).
 
 Destinations too large for a shared-memory tile are filtered one of two ways: one
-sort-filter-skyline block each (little work, one SM per destination) or the GPU-wide
-pairwise mark pass (more work, every SM).  The size from which the mark pass pays depends
-on the instance family: a knapsack stream has many mid-sized destinations, a 5-objective
-15-city TSP a few huge ones.  For each requested (objectives, problem type) this tuner
-times a calibration instance of that family under a list of crossover sizes, each in a
-fresh process (the engine reads PMDD_BIG_MARK_MIN at start-up), and under the engine's
-built-in behaviour (65536, except that a step with fewer oversized destinations than SMs
-sends them all to the mark pass), keeps the fastest, and writes the choice to the tuning
-file the engine reads at start-up:
+sort-filter-skyline block each (one SM per destination) or the GPU-wide pass that drops
+what the largest-sum pivots dominate and sweeps the rest pairwise (every SM).  The size
+from which the GPU-wide pass pays depends on the instance family.  For each requested
+(objectives, problem type) this tuner times a calibration instance of that family under a
+list of crossover sizes, each in a fresh process (the engine reads PMDD_BIG_MARK_MIN at
+start-up), and under the engine's built-in behaviour (1025: every destination with more
+candidates than a tile holds takes the GPU-wide pass), keeps the fastest, and writes the
+choice to the tuning file the engine reads at start-up:
 
     {"version": 1, "entries": {"d<objectives>_p<problem type>": {"big_mark_min": n,
                                 "seconds": {"<n>": device seconds, ...}, "instance": "..."}}}
@@ -20,7 +19,7 @@ without "big_mark_min" ({"builtin": true, ...}), which the engine reads as untun
     python -m pmdd_b200.autotune --nobjs 3 5 --ptype 1 3 [--out PATH]
 
 The file is PMDD_TUNING_FILE if set, else $XDG_CACHE_HOME/pmdd_b200/tuning.json or
-~/.cache/pmdd_b200/tuning.json.  Without a file the engine uses 65536 for every family.
+~/.cache/pmdd_b200/tuning.json.  Without a file the engine uses 1025 for every family.
 """
 from __future__ import annotations
 
@@ -33,8 +32,8 @@ from typing import Callable, Dict, Iterable, Optional, Sequence
 
 from . import instances
 
-CANDIDATE_SIZES = (4096, 16384, 65536, 262144, 1 << 40)
-DEFAULT_MARK_MIN = 65536
+CANDIDATE_SIZES = (1025, 4096, 16384, 65536, 1 << 40)
+DEFAULT_MARK_MIN = 1025
 
 
 def tuning_path() -> str:

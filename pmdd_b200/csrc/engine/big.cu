@@ -20,8 +20,10 @@
 //       compacts the survivors into the slot.  The pivots leave the pairwise sweep a
 //       fraction of the candidates, and it costs the square of what it is given.
 //
-// For steps of thousands of mid-sized destinations the SFS blocks win (they do less work
-// than the pairwise sweep); for a few huge ones the mark path does.
+// With the pivots the GPU-wide pass wins from the smallest oversized destinations up (on
+// the batched knapsack / set-packing stream as on single 5-objective TSPs), so by default
+// it takes every destination above kSmallMax candidates; SFS blocks keep those that leave
+// the tiles for their arc count, and whatever a fixed or tuned crossover assigns them.
 #include "kernels.cuh"
 #include "sfs.cuh"
 

@@ -619,14 +619,10 @@ std::map<std::pair<int, int>, int64_t> read_tuning(const std::string &path) {
 
 void Engine::load_tuning() { tuned_mark_min_ = read_tuning(default_tuning_path()); }
 
-bool Engine::mark_min_set(int d, int problem_type) const {
-    return big_mark_min_fixed_ > 0 || tuned_mark_min_.count({d, problem_type}) > 0;
-}
-
 int64_t Engine::mark_min_for(int d, int problem_type) const {
     if (big_mark_min_fixed_ > 0) return big_mark_min_fixed_;
     auto it = tuned_mark_min_.find({d, problem_type});
-    return it != tuned_mark_min_.end() ? it->second : 65536;
+    return it != tuned_mark_min_.end() ? it->second : static_cast<int64_t>(dev::kSmallMax) + 1;
 }
 
 void *Engine::scratch(size_t bytes) {
@@ -963,12 +959,6 @@ int Engine::step() {
     std::vector<GroupLaunch> glaunch;
     std::vector<int64_t> tile_bases(exps.size()), item_bases(exps.size());  // group-relative
     std::vector<int64_t> big_bases(exps.size());                           // group-relative
-    // a step with fewer oversized destinations than SMs would leave most SMs idle with one
-    // SFS block each: with the built-in crossover, send them all down the GPU-wide mark
-    // path instead (a crossover fixed by PMDD_BIG_MARK_MIN or tuned for the family stands)
-    int64_t step_big = 0;
-    for (const ExpPlan &e : exps) step_big += e.num_big;
-    const bool sparse_big = step_big > 0 && step_big < sms_;
     {
         size_t pos = 0;
         std::vector<ExpPlan> ordered;
@@ -1025,9 +1015,7 @@ int Engine::step() {
                     J.big_surv_idx = reinterpret_cast<int32_t *>(m + 3 * pb + ib);
                     J.big_window = e.big_window;
                     J.big_rows = e.big_rows;
-                    const int64_t mm = sparse_big && !mark_min_set(I.d, I.opts.problem_type)
-                                           ? static_cast<int64_t>(dev::kSmallMax) + 1
-                                           : mark_min_for(I.d, I.opts.problem_type);
+                    const int64_t mm = mark_min_for(I.d, I.opts.problem_type);
                     J.big_mark_min = mm;
                     if (s.res.max_item >= mm) gl.mark_cap += e.big_rows / mm + 1;
                     gl.big_passes = std::max<int64_t>(gl.big_passes, (e.big_total + e.big_window - 1) / e.big_window);

@@ -273,12 +273,11 @@ class Engine {
     KernelTimes ktimes_;
     bool trace_ = false;  // PMDD_TRACE=1: one stderr line per step
     // Oversized destinations of at least mark_min_for(d, problem type) candidates are
-    // filtered by the GPU-wide mark/write pass instead of one SFS block: PMDD_BIG_MARK_MIN
-    // if set, else the tuned value for (d, problem type) from the tuning file, else 65536
-    // (and, for that built-in value only, every oversized destination of a step that has
-    // fewer of them than SMs).
+    // filtered by the GPU-wide pivot/mark pass instead of one SFS block: PMDD_BIG_MARK_MIN
+    // if set, else the tuned value for (d, problem type) from the tuning file, else
+    // kSmallMax + 1 (every destination too large for a tile; SFS blocks then take only
+    // destinations that leave the tiles for their arc count).
     int64_t mark_min_for(int d, int problem_type) const;
-    bool mark_min_set(int d, int problem_type) const;  // fixed or tuned, not built in
     void load_tuning();
     int64_t big_mark_min_fixed_ = 0;
     std::map<std::pair<int, int>, int64_t> tuned_mark_min_;

@@ -13,7 +13,7 @@ def test_choose_picks_fastest_and_breaks_ties_upward():
     assert autotune.choose({4096: 1.00, 65536: 1.01, 262144: 3.0}) == 65536  # within 2 %: larger size
     assert autotune.choose({4096: None, 65536: None}) == autotune.DEFAULT_MARK_MIN
     assert autotune.choose({4096: None, 16384: 0.5}) == 16384
-    flat = {4096: 0.0077, 16384: 0.0077, 65536: 0.0077, 1 << 40: 0.0077}  # crossover never reached
+    flat = {1025: 0.0077, 4096: 0.0077, 16384: 0.0077, 1 << 40: 0.0077}  # crossover never reached
     assert autotune.choose(flat) == autotune.DEFAULT_MARK_MIN
     assert autotune.choose({16384: 1.0, 262144: 1.01, 1 << 40: 1.005}) == 1 << 40
 
