@@ -40,6 +40,13 @@ def test_tune_with_a_fake_timer(tmp_path):
     assert lib.pmdd_tuned_mark_min(path.encode(), 5, 3) == 0
 
 
+def test_default_is_among_the_timed_sizes():
+    """A tie can only go to the default if the tuner times it; it is the engine's built-in
+    crossover, one above the largest tile destination (kSmallMax + 1)."""
+    assert autotune.DEFAULT_MARK_MIN in autotune.CANDIDATE_SIZES
+    assert autotune.DEFAULT_MARK_MIN == 1025
+
+
 def test_builtin_wins_ties():
     assert autotune.choose({4096: 1.0, 65536: 2.0}, builtin=1.01) is None
     assert autotune.choose({4096: 1.0, 65536: 2.0}, builtin=1.5) == 4096
