@@ -275,7 +275,8 @@ const char *pmdd_version(void);
 int64_t pmdd_launch_count(void);
 /* The oversized-destination crossover (candidates from which a destination is filtered
  * by the GPU-wide pass rather than one sort-filter-skyline block) that the tuning file
- * at `path` holds for (nobjs, problem_type), or 0 if it holds none.  path NULL: the file
+ * at `path` holds for (nobjs, problem_type), or 0 if it holds none (engines then use their
+ * built-in crossover, 1025: every destination too large for a tile).  path NULL: the file
  * engines read at start-up (PMDD_TUNING_FILE, else the per-user cache written by
  * pmdd_b200.autotune).  No counterpart in the reference, which has one filter path. */
 int64_t pmdd_tuned_mark_min(const char *path, int32_t nobjs, int32_t problem_type);
