@@ -9,8 +9,9 @@
 //       with the maxima found so far; many such destinations keep the GPU busy side by
 //       side;
 //   big_plan_kernel .. big_write_kernel: destinations of big_mark_min candidates and
-//       more, each spread over every SM.  The plan lists their 256-candidate chunks.  big_pivot_kernel picks each destination's pivots (the
-//       candidates of largest objective sum, from a sorted sample of sums);
+//       more, each spread over every SM.  The plan lists their 256-candidate chunks.
+//       big_pivot_kernel picks each destination's pivots (the candidates of largest
+//       objective sum, from a sorted sample of sums);
 //       big_prefilter_kernel drops every candidate a pivot dominates; big_compact_kernel
 //       packs the rest, in candidate order; big_rplan_kernel lists their chunks; one
 //       big_mark_kernel block per chunk streams the remaining rows through shared memory
