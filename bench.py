@@ -295,6 +295,59 @@ def served_loop(rate, n_req, seed, P, instances, device=0):
             "outputs_written": written, "writer_tail_ms": tail_ms}
 
 
+def config1_filter(P, dds, device, peak, flush=None):
+    """One resident enumeration of a set of config-1 DDs (after the caller's warm-up):
+    the tile kernel's and the whole filter's algorithmic bytes over their kernel time."""
+    import torch
+
+    r1 = P.ResidentSet(dds, device=device)
+    try:
+        r1.enumerate(method=1, keep=False)
+        st1 = {}
+        if flush is not None:
+            flush.zero_()
+        torch.cuda.synchronize()
+        r1.enumerate(method=1, stats=st1, keep=False)
+    finally:
+        r1.close()
+    b1 = (st1["work_tile_candidates_total"] + st1["work_tile_survivors_total"]) * 3 * 4
+    a1 = b1 / st1["kernel_expand_td_s"] / 1e9
+    bf = (st1["work_candidates_total"] + st1["work_frontier_survivors_total"]) * 3 * 4
+    tf = st1["kernel_expand_td_s"] + st1["kernel_dominance_s"]
+    af = bf / tf / 1e9
+    return {"instances": len(dds), "solves_per_s": len(dds) / st1["device_elapsed_s"],
+            "achieved_gbs": a1, "frac_of_peak": a1 / peak,
+            "kernel_s": st1["kernel_expand_td_s"], "algorithmic_bytes": int(b1),
+            "tile_launches": int(st1["tile_launches"]),
+            "filter_achieved_gbs": af, "filter_frac_of_peak": af / peak,
+            "filter_kernel_s": tf, "filter_algorithmic_bytes": int(bf),
+            "device_s": st1["device_elapsed_s"]}
+
+
+def config1_only(args):
+    """`--config1 N`: the config-1 filter leg alone (N x KP d=3 n=40, seeds 0..N-1,
+    method 1), `--warmup` untimed resident enumerations then `--steps` timed ones; one
+    JSON line.  This is the command the committed tile-kernel profiles run under ncu."""
+    import torch
+
+    import pmdd_b200 as P
+    from pmdd_b200 import instances
+
+    torch.cuda.set_device(0)
+    peak, peak_kind = read_peaks()
+    dds = build_dds([(1, instances.knapsack_text(40, 3, s), "") for s in range(args.config1)])
+    res = P.ResidentSet(dds, device=0)
+    for _ in range(args.warmup):
+        res.enumerate(method=1, keep=False)
+    res.close()
+    runs = [config1_filter(P, dds, 0, peak) for _ in range(max(1, args.steps))]
+    best = max(runs, key=lambda r: r["achieved_gbs"])
+    best["peak_gbs"] = peak
+    best["peak_kind"] = peak_kind
+    best["runs"] = len(runs)
+    print(json.dumps({"config1_filter": best}))
+
+
 # ------------------------------------------------------------------- main
 def main():
     ap = argparse.ArgumentParser()
@@ -306,7 +359,13 @@ def main():
     ap.add_argument("--no-extras", action="store_true", help="skip one-at-a-time, served, config-1 and CPU legs")
     ap.add_argument("--subset", type=int, default=0,
                     help="profile a subset: every k-th instance of the stream (k = value); not a bench line")
+    ap.add_argument("--config1", type=int, default=0,
+                    help="only the config-1 filter leg on this many KP d=3 n=40 instances (profiling aid; "
+                         "prints its own JSON line, not a bench line)")
     args = ap.parse_args()
+    if args.config1 > 0:
+        config1_only(args)
+        return
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -496,26 +555,11 @@ def main():
             served.append(served_loop(rate, n_req, rate, P, instances, device))
         line["served"] = served
         # config-1 filter roofline: 1024 x KP d=3 n=40
+        # (tile kernel alone, and the whole filter: tiles + oversized-destination path)
         n1 = 256 if args.quick else 1024
         dd1 = build_dds([(1, instances.knapsack_text(40, 3, s), "") for s in range(n1)])
-        r1 = P.ResidentSet(dd1, device=device)
-        r1.enumerate(method=1, keep=False)
-        st1 = {}
-        flush.zero_()
-        torch.cuda.synchronize()
-        r1.enumerate(method=1, stats=st1, keep=False)
-        # tile kernel alone, and the whole filter (tiles + oversized-destination path)
-        b1 = (st1["work_tile_candidates_total"] + st1["work_tile_survivors_total"]) * 3 * 4
-        a1 = b1 / st1["kernel_expand_td_s"] / 1e9
-        bf = (st1["work_candidates_total"] + st1["work_frontier_survivors_total"]) * 3 * 4
-        tf = st1["kernel_expand_td_s"] + st1["kernel_dominance_s"]
-        af = bf / tf / 1e9
-        line["config1_filter"] = {"instances": n1, "solves_per_s": n1 / st1["device_elapsed_s"],
-                                  "achieved_gbs": a1, "frac_of_peak": a1 / peak,
-                                  "kernel_s": st1["kernel_expand_td_s"], "algorithmic_bytes": int(b1),
-                                  "filter_achieved_gbs": af, "filter_frac_of_peak": af / peak,
-                                  "filter_kernel_s": tf, "filter_algorithmic_bytes": int(bf)}
-        r1.close()
+        line["config1_filter"] = config1_filter(P, dd1, device, peak, flush)
+        del dd1
         # the knapsack half of the stream with DD construction inside the timed region:
         # built on the device from the instance arrays and enumerated from there, against
         # the host constructors (16 threads) + upload + enumeration

@@ -41,7 +41,8 @@ enum pmdd_status {
     PMDD_ERR_INTERNAL = 6,       /* device-side consistency check failed */
     PMDD_ERR_CANCELLED = 7,      /* request cancelled before completion */
     PMDD_ERR_NO_DEVICE = 8,      /* no CUDA device / extension not usable */
-    PMDD_ERR_RANGE = 9,          /* objective sums exceed the supported integer range */
+    PMDD_ERR_RANGE = 9,          /* objective sums exceed the supported integer range, or a
+                                    size exceeds a fixed limit (pmdd_pareto_filter_noalloc) */
     PMDD_ERR_IO = 10             /* an output file could not be written (pmdd_host.h writers) */
 };
 
@@ -163,16 +164,18 @@ int pmdd_pareto_filter(const int32_t *points, int64_t num_points, int32_t nobjs,
                        int32_t device, char *err, size_t errlen);
 
 /* Allocation-free variant of pmdd_pareto_filter, for callers that cannot allocate
- * device memory (inside stream capture, under an allocator that owns the device, or
- * in services that forbid allocation after start-up).  No counterpart in the
- * reference.  Device buffers: d_points (num_points*nobjs) in, d_out (same capacity)
- * out; *out_points (host) receives the count; `stream` is a cudaStream_t (NULL: the
+ * device memory: libraries running beside a framework allocator that has reserved the
+ * device's memory, and services that forbid cudaMalloc / cudaFree after start-up
+ * because those calls can synchronise the device.  No counterpart in the reference.
+ * Device buffers: d_points (num_points*nobjs) in, d_out (same capacity) out;
+ * *out_points (host) receives the count; `stream` is a cudaStream_t (NULL: the
  * default stream).  Scratch comes from a fixed device array of about 9.4 MB that every
  * device loading this library holds until exit: at most 131072 points of at most 8
  * objectives per call (larger sets return PMDD_ERR_RANGE).  Calls share that array, so
  * calls that overlap on the GPU race; serialise them.  The first call on a device
  * looks up the array's address and should happen before any stream capture.
- * Allocates nothing; synchronises `stream` before returning. */
+ * Allocates nothing; copies the count to the host and synchronises `stream` before
+ * returning. */
 int pmdd_pareto_filter_noalloc(const int32_t *d_points, int64_t num_points, int32_t nobjs, int32_t *d_out,
                                int64_t *out_points, void *stream, char *err, size_t errlen);
 

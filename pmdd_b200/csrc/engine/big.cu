@@ -621,12 +621,9 @@ template <int D, typename T>
 static cudaError_t launch_big_t(const BigLaunch &L, cudaStream_t stream) {
     if (L.num_work <= 0 || L.total <= 0) return cudaSuccess;
     using Cfg = SfsSmallCfg<D, T>;
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(big_sfs_kernel<D, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             static_cast<int>(Cfg::kSmem));
+    {
+        const cudaError_t e = ensure_smem_limit(reinterpret_cast<const void *>(big_sfs_kernel<D, T>), Cfg::kSmem);
         if (e != cudaSuccess) return e;
-        attr_set = true;
     }
     const int64_t want = (L.total + kFlatThreads - 1) / kFlatThreads;
     const unsigned grid = static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>(want, int64_t(L.sms) * 32)));

@@ -4,8 +4,29 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include <mutex>
+#include <set>
+#include <utility>
+
 namespace pmdd {
 namespace dev {
+
+// Raises a kernel's dynamic shared-memory limit on the current device, once per
+// (kernel, device).  The attribute belongs to the device's context, so a process that
+// drives several GPUs, or calls in with another device current, sets it on each; the
+// registry is shared by every host thread.
+inline cudaError_t ensure_smem_limit(const void *func, size_t bytes) {
+    static std::mutex mu;
+    static std::set<std::pair<const void *, int>> done;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(mu);
+    if (done.count({func, dev})) return cudaSuccess;
+    e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
+    if (e == cudaSuccess) done.insert({func, dev});
+    return e;
+}
 
 // Fused expand+filter tiles: a tile owns every destination whose candidate range
 // starts inside its window of at most kTileWindow candidates; destinations of at most

@@ -620,15 +620,11 @@ static cudaError_t launch_couple_round_t(const CoupleJob *jobs, int num_jobs, in
                                         cudaStream_t stream) {
     const size_t smem = static_cast<size_t>(kCoupleFS) * sizeof(PackedPt<D, T>);
     const size_t mark_smem = static_cast<size_t>(kMarkStage) * (sizeof(PackedPt<D, T>) + sizeof(int32_t));
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(couple_prune_kernel<D, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             static_cast<int>(smem));
+    {
+        cudaError_t e = ensure_smem_limit(reinterpret_cast<const void *>(couple_prune_kernel<D, T>), smem);
         if (e != cudaSuccess) return e;
-        e = cudaFuncSetAttribute(couple_mark_kernel<D, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(mark_smem));
+        e = ensure_smem_limit(reinterpret_cast<const void *>(couple_mark_kernel<D, T>), mark_smem);
         if (e != cudaSuccess) return e;
-        attr_set = true;
     }
     if (seed) couple_seed_kernel<D, T><<<dim3(blocks_per_job, num_jobs), kCoupleThreads, 0, stream>>>(jobs);
     else couple_prune_kernel<D, T><<<dim3(blocks_per_job, num_jobs), kCoupleThreads, smem, stream>>>(jobs);

@@ -1,12 +1,13 @@
 // Allocation-free variant of the standalone Pareto filter (pmdd_pareto_filter).
 //
-// Some callers cannot allocate device memory at all: code running inside a CUDA graph
-// capture or a stream-ordered pipeline that must not synchronise on cudaMalloc, host
-// libraries embedded in frameworks whose allocator owns the whole device, and
-// real-time services that forbid allocation after start-up.  They own their input and
-// output buffers already; what they cannot do is obtain the filter's scratch space.
-// This entry point takes that scratch from a fixed, file-scope device array instead of
-// the engine's arena, and allocates nothing -- no cudaMalloc, no cudaFree, no engine.
+// Some callers cannot allocate device memory at all: host libraries embedded in a
+// framework whose caching allocator has already reserved the device's memory (a
+// cudaMalloc beside it fails or fragments that pool), and latency-bound services that
+// forbid allocation after start-up, because cudaMalloc and cudaFree can synchronise
+// the device and stall every stream on it.  They own their input and output buffers
+// already; what they cannot do is obtain the filter's scratch space.  This entry
+// point takes that scratch from a fixed, file-scope device array instead of the
+// engine's arena, and allocates nothing -- no cudaMalloc, no cudaFree, no engine.
 //
 // Limits and sharing:
 //  * at most kNoAllocMaxPoints points of at most 8 objectives per call (larger inputs
@@ -20,7 +21,9 @@
 //    other's results -- serialise them;
 //  * the first call on each device looks up the array's device address
 //    (cudaGetSymbolAddress) with that device current; make that first call before any
-//    stream capture begins.
+//    stream capture begins;
+//  * the call copies the result count to the host and synchronises `stream` before it
+//    returns.
 #include <mutex>
 
 #include "pareto.cuh"

@@ -38,12 +38,9 @@ template <int D>
 static cudaError_t launch_pareto_t(const int32_t *in, int64_t n, void *scratch, int32_t *out, int64_t *out_n,
                                    cudaStream_t stream) {
     using Cfg = SfsCfg<D, int32_t>;
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(pareto_filter_kernel<D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             static_cast<int>(Cfg::kSmem));
+    {
+        const cudaError_t e = ensure_smem_limit(reinterpret_cast<const void *>(pareto_filter_kernel<D>), Cfg::kSmem);
         if (e != cudaSuccess) return e;
-        attr_set = true;
     }
     pareto_filter_kernel<D><<<1, Cfg::kThreads, Cfg::kSmem, stream>>>(in, n, pareto_scratch_layout(scratch, D, n),
                                                                        out, out_n);

@@ -370,12 +370,9 @@ template <int D, typename T>
 static cudaError_t launch_expand_tiles_t(const ExpandJob *jobs, const int64_t *tile_bases, int num_jobs,
                                          int64_t total_tiles, int grid, cudaStream_t stream) {
     const size_t smem = sizeof(TileSmem<D, T>);
-    static bool attr_set = false;  // per instantiation; setting it twice is harmless
-    if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(expand_tile_kernel<D, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             static_cast<int>(smem));
+    {
+        const cudaError_t e = ensure_smem_limit(reinterpret_cast<const void *>(expand_tile_kernel<D, T>), smem);
         if (e != cudaSuccess) return e;
-        attr_set = true;
     }
     if (total_tiles <= 0) return cudaSuccess;
     const int64_t g = std::min<int64_t>(total_tiles, grid);

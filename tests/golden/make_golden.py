@@ -132,7 +132,7 @@ def record(name, path, problem_type, nobjs, methods):
 
 
 def main():
-    ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref_root = sys.argv[1] if len(sys.argv) > 1 else os.environ["PMDD_REFERENCE_DIR"]
     for name, pt, d, text, methods in SYNTHETIC:
         path = os.path.join(HERE, f"{name}.dat")
         with open(path, "w") as f:
