@@ -233,19 +233,11 @@ def served_loop(rate, n_req, seed, P, instances, device=0):
     result is reported beside the latencies."""
     from pmdd_b200.writer import FrontierWriter
 
-    rng = np.random.default_rng(seed)
-    specs = []
-    for i in range(n_req):
-        kind = rng.integers(0, 3)
-        s = 50_000 + seed * 10_000 + i
-        if kind == 0:
-            specs.append((1, instances.knapsack_text(int(rng.integers(20, 61)), 3, s), 1))
-        elif kind == 1:
-            specs.append((2, instances.setpacking_text(int(rng.integers(60, 101)), 20, 3, s), 1))
-        else:
-            specs.append((3, instances.tsp_arrays(int(rng.integers(9, 14)), 3, s), 3))
+    mix = instances.served_mix(n_req, seed)
+    specs = [(p, instances.tsp_arrays_from_tag(tag) if p == 3 else text, m) for p, text, m, tag in mix]
     built = iter(build_dds([(p, t, "") for p, t, _ in specs if p != 3]))
     dds = [t if p == 3 else next(built) for p, t, _ in specs]
+    rng = np.random.default_rng(seed + 1)
     gaps = rng.exponential(1.0 / rate, size=n_req)
     arrivals = np.cumsum(gaps)
     srv = P.Server(device=device)

@@ -76,3 +76,32 @@ def stream_mix(num_knapsack: int = 512, num_setpacking: int = 256, nobjs: int = 
         s = seed0 + num_knapsack + j
         out.append((2, setpacking_text(n, 20, nobjs, s), f"sp{nobjs}_n{n}_s{s}"))
     return out
+
+
+def served_mix(n_req: int, seed: int):
+    """The served-loop request list: each request is knapsack (d=3, n ~ U{20..60},
+    method 1), set packing (d=3, n ~ U{60..100}, m = 20, method 1) or TSP (d=3,
+    n ~ U{9..13} cities, method 3) with equal odds, instance seeds 50000 + 10000*seed + i.
+    Returns (problem_type, text, method, tag) tuples; a TSP request's cost matrices are
+    tsp_arrays(n, 3, instance seed), the same instance its text describes."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n_req):
+        kind = rng.integers(0, 3)
+        s = 50_000 + seed * 10_000 + i
+        if kind == 0:
+            n = int(rng.integers(20, 61))
+            out.append((1, knapsack_text(n, 3, s), 1, f"kp3_n{n}_s{s}"))
+        elif kind == 1:
+            n = int(rng.integers(60, 101))
+            out.append((2, setpacking_text(n, 20, 3, s), 1, f"sp3_n{n}_s{s}"))
+        else:
+            n = int(rng.integers(9, 14))
+            out.append((3, tsp_text(n, 3, s), 3, f"tsp3_n{n}_s{s}"))
+    return out
+
+
+def tsp_arrays_from_tag(tag: str) -> np.ndarray:
+    """Cost matrices of a served-mix TSP request from its tag (tsp3_n<n>_s<seed>)."""
+    _, n, s = tag.split("_")
+    return tsp_arrays(int(n[1:]), 3, int(s[1:]))

@@ -41,3 +41,29 @@ def golden_frontier(rec, method):
 @pytest.fixture(scope="session")
 def golden():
     return golden_cases()
+
+
+HEADLINE = os.path.join(GOLDEN, "headline")
+
+
+def frontier_text(points) -> str:
+    """A frontier in the reference's --frontier-out text: rows in ascending
+    lexicographic order, objectives as %d joined by commas, one row per line
+    (src/pmdd/util/output_utils.cpp:87-152, enum/pareto_frontier.hpp:418-433)."""
+    import numpy as np
+
+    pts = np.asarray(points, dtype=np.int64)
+    if pts.shape[0] > 1:
+        pts = pts[np.lexsort(pts.T[::-1])]
+    return "".join(",".join(str(int(x)) for x in row) + "\n" for row in pts)
+
+
+def frontier_digest(points) -> str:
+    import hashlib
+
+    return hashlib.sha256(frontier_text(points).encode()).hexdigest()
+
+
+def headline(name):
+    with open(os.path.join(HEADLINE, name)) as f:
+        return json.load(f)
