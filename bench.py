@@ -275,6 +275,7 @@ def served_loop(rate, n_req, seed, P, instances, device=0):
             writer.submit(r.frontier, os.path.join(outdir, f"r{r.req_id}.frontier.csv.gz"),
                           os.path.join(outdir, "stats.jsonl"), rec)
     wall = time.perf_counter() - t0
+    info = srv.info()
     srv.close()
     tw = time.perf_counter()
     written = writer.flush()
@@ -284,7 +285,9 @@ def served_loop(rate, n_req, seed, P, instances, device=0):
     lat = np.array(lat)
     return {"rate_rps": rate, "requests": n_req, "p50_ms": float(np.percentile(lat, 50)),
             "p99_ms": float(np.percentile(lat, 99)), "solves_per_s": n_req / wall,
-            "outputs_written": written, "writer_tail_ms": tail_ms}
+            "outputs_written": written, "writer_tail_ms": tail_ms,
+            "admission": {k: int(info[k]) for k in ("admitted", "completed", "rejected", "failed", "queued_peak",
+                                                     "running_peak", "budget_bytes", "peak_used_bytes")}}
 
 
 def config1_filter(P, dds, device, peak, flush=None):

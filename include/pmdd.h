@@ -240,7 +240,21 @@ int pmdd_resident_dd_copy(pmdd_resident *res, int32_t i, int32_t *layer_offsets,
 /* ---------------------------------------------------------------- serving
  * A device-resident request loop with continuous batching: submitted requests are
  * admitted as slots and HBM budget free up; every admitted request advances one
- * layer per engine step, sharing each launch with the others. */
+ * layer per engine step, sharing each launch with the others.  No counterpart in the
+ * reference, which enumerates one instance per process (src/pmdd/main.cpp:67-467).
+ *
+ * Admission: a request is admitted when its predicted peak device footprint fits
+ * beside what the running requests hold and are predicted to grow by.  The prediction
+ * is the DD's device bytes plus two layers of frontier slots at the predicted largest
+ * layer (the larger of the layers the request has shown, its next layer once counted --
+ * exact -- and a per-(problem type, objectives, method) ratio of largest layer to DD
+ * arcs learned from finished requests), per-layer bookkeeping, and for method 3 the
+ * other side's frontier and the coupling block.  A request that does not fit waits;
+ * smaller ones behind it may pass until it has been passed over 32 times.  A request
+ * whose DD alone exceeds the budget finishes at once with PMDD_ERR_OOM; one that runs
+ * out of memory while running finishes with PMDD_ERR_OOM while the others continue
+ * (the reference's GPU path returns NULL with a reason and the CLI exits,
+ * src/pmdd/main.cpp:338-345, or lets a Thrust allocation exception escape). */
 typedef struct pmdd_server pmdd_server;
 
 typedef struct pmdd_result {
@@ -270,6 +284,27 @@ int pmdd_server_poll(pmdd_server *srv, pmdd_result *out);
 int pmdd_server_cancel(pmdd_server *srv, uint64_t req_id);
 /* Requests submitted but not yet finished (queued + running). */
 int pmdd_server_pending(const pmdd_server *srv);
+
+/* Serving counters and memory figures since the server was created.  `rejected`:
+ * finished with an error before admission (DD above the budget, invalid request);
+ * `failed`: finished with an error after admission (cancellations apart). */
+typedef struct pmdd_server_info {
+    int64_t submitted, admitted, completed, failed, rejected, cancelled;
+    int32_t queued, running;            /* now */
+    int32_t queued_peak, running_peak;  /* largest seen at an admission pass */
+    int64_t budget_bytes;               /* the engine arena's budget */
+    int64_t used_bytes;                 /* arena bytes in use now */
+    int64_t peak_used_bytes;            /* arena high-water mark */
+    int64_t reserved_growth_bytes;      /* predicted growth of the running requests */
+    int64_t injected_alloc_failures;    /* allocations failed by the test hook below */
+} pmdd_server_info;
+int pmdd_server_get_info(const pmdd_server *srv, pmdd_server_info *out);
+
+/* Test hook for the failure paths: after `after` more device-memory allocations of
+ * this server's engine, the next `count` fail as if the device were out of memory.
+ * Running requests that cannot get memory finish with PMDD_ERR_OOM; the server keeps
+ * serving the others.  No counterpart in the reference. */
+int pmdd_server_inject_alloc_failures(pmdd_server *srv, int64_t after, int64_t count);
 void pmdd_server_destroy(pmdd_server *srv);
 
 /* --------------------------------------------------------------- utilities */

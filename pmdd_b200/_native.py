@@ -110,6 +110,14 @@ class PmddStats(ctypes.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class PmddServerInfo(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int64) for n in ("submitted", "admitted", "completed", "failed", "rejected",
+                                              "cancelled")] + \
+               [(n, ctypes.c_int32) for n in ("queued", "running", "queued_peak", "running_peak")] + \
+               [(n, ctypes.c_int64) for n in ("budget_bytes", "used_bytes", "peak_used_bytes",
+                                              "reserved_growth_bytes", "injected_alloc_failures")]
+
+
 class PmddResult(ctypes.Structure):
     _fields_ = [
         ("req_id", ctypes.c_uint64),
@@ -214,6 +222,8 @@ GPU_SYMBOLS = {
     "pmdd_server_cancel": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64]),
     "pmdd_server_pending": (ctypes.c_int, [ctypes.c_void_p]),
     "pmdd_server_destroy": (None, [ctypes.c_void_p]),
+    "pmdd_server_get_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(PmddServerInfo)]),
+    "pmdd_server_inject_alloc_failures": (ctypes.c_int, [ctypes.c_void_p, c_i64, c_i64]),
     "pmdd_version": (ctypes.c_char_p, []),
     "pmdd_launch_count": (c_i64, []),
     "pmdd_tuned_mark_min": (c_i64, [ctypes.c_char_p, c_i32, c_i32]),

@@ -565,7 +565,9 @@ int pmdd_resident_enumerate(pmdd_resident *R, const pmdd_options *opts, pmdd_fro
         I->external_dd = true;
         I->tsp = T.tsp;
         I->with_out_csr = T.with_out_csr;
-        I->est_bytes = std::max<int64_t>(0, T.est_bytes - static_cast<int64_t>(T.dev_bytes));
+        I->min_bytes = 0;  // the DD is resident already
+        I->max_layer_arcs = T.max_layer_arcs;
+        I->max_layer_nodes = T.max_layer_nodes;
         I->submit_s = pmdd::now_s();
         reqs.push_back(std::move(I));
     }
@@ -913,11 +915,10 @@ int pmdd_server_submit(pmdd_server *srv, const pmdd_dd *dd, const pmdd_options *
     std::string msg;
     const int rc = pmdd::prepare_instance(*dd, o, req_id, I.get(), &msg);
     if (rc != PMDD_OK) {
+        I->id = req_id;
         I->status = rc;
         I->error = msg;
-        I->phase = pmdd::Instance::DONE;
-        I->finish_s = pmdd::now_s();
-        srv->engine->finished().push_back(std::move(I));
+        srv->engine->finish_rejected(std::move(I));
         return rc;
     }
     srv->engine->submit(std::move(I));
@@ -941,9 +942,7 @@ int pmdd_server_submit_tsp(pmdd_server *srv, const pmdd_tsp *t, const pmdd_optio
         I->id = req_id;
         I->status = PMDD_ERR_OOM;
         I->error = msg;
-        I->phase = pmdd::Instance::DONE;
-        I->finish_s = pmdd::now_s();
-        srv->engine->finished().push_back(std::move(I));
+        srv->engine->finish_rejected(std::move(I));
         return PMDD_ERR_OOM;
     }
     pmdd::prepare_tsp_instance(*S, t->nobjs, t->cost, o, req_id, I.get());
@@ -984,6 +983,35 @@ int pmdd_server_cancel(pmdd_server *srv, uint64_t req_id) {
 int pmdd_server_pending(const pmdd_server *srv) {
     if (!srv) return 0;
     return static_cast<int>(srv->engine->queued() + srv->engine->running());
+}
+
+int pmdd_server_get_info(const pmdd_server *srv, pmdd_server_info *out) {
+    if (!srv || !out) return PMDD_ERR_INVALID;
+    const pmdd::Engine &E = *srv->engine;
+    const pmdd::Engine::Counters &c = E.counters();
+    std::memset(out, 0, sizeof(*out));
+    out->submitted = static_cast<int64_t>(srv->submitted);
+    out->admitted = c.admitted;
+    out->completed = c.completed;
+    out->failed = c.failed;
+    out->rejected = c.rejected;
+    out->cancelled = c.cancelled;
+    out->queued = static_cast<int32_t>(E.queued());
+    out->running = static_cast<int32_t>(E.running());
+    out->queued_peak = static_cast<int32_t>(c.queued_peak);
+    out->running_peak = static_cast<int32_t>(c.running_peak);
+    out->budget_bytes = static_cast<int64_t>(E.arena().capacity());
+    out->used_bytes = static_cast<int64_t>(E.arena().used());
+    out->peak_used_bytes = static_cast<int64_t>(E.arena().peak());
+    out->reserved_growth_bytes = E.reserved_growth();
+    out->injected_alloc_failures = E.arena().injected_failures();
+    return PMDD_OK;
+}
+
+int pmdd_server_inject_alloc_failures(pmdd_server *srv, int64_t after, int64_t count) {
+    if (!srv || after < 0 || count < 0) return PMDD_ERR_INVALID;
+    srv->engine->inject_alloc_failures(after, count);
+    return PMDD_OK;
 }
 
 void pmdd_server_destroy(pmdd_server *srv) { delete srv; }

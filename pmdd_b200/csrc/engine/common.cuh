@@ -96,6 +96,15 @@ struct ExpandJob {
     int64_t big_rows;              // scratch rows (candidates) one pass can use
     uint32_t *err;
     unsigned long long *tile_surv; // survivors written by the tile kernel (added to)
+    // Lexicographic order (three objectives): a node whose flag is 1 holds its frontier in
+    // descending lexicographic order.  prev_sorted is indexed like prev_size; the tile
+    // kernels write out_sorted for every destination they stage (1 only when they wrote
+    // it in that order); nullptr when the job keeps no flags.
+    const uint8_t *prev_sorted;
+    uint8_t *out_sorted;
+    int32_t pair_max;              // lexicographic tiles: destinations of at most this many
+                                   // candidates are checked pairwise, larger ones by a staircase warp
+    int32_t pad1;
 };
 
 // Bytes of oversized-destination scratch per candidate point.

@@ -66,6 +66,15 @@ bool Arena::grow(size_t at_least) {
 }
 
 void *Arena::alloc(size_t bytes) {
+    if (inj_count_ > 0) {
+        if (inj_after_ > 0) {
+            --inj_after_;
+        } else {
+            --inj_count_;
+            ++injected_;
+            return nullptr;
+        }
+    }
     bytes = align256(bytes == 0 ? 1 : bytes);
     for (int attempt = 0; attempt < 2; ++attempt) {
         for (auto it = free_.begin(); it != free_.end(); ++it) {
@@ -211,6 +220,16 @@ static void setpacking_sd_layout(const pmdd_dd &dd, Instance *I) {
     }
 }
 
+// The DD shape the footprint prediction reads: widest layer in arcs and in nodes.
+static void set_shape(Instance *I, const std::vector<int32_t> &arc_at) {
+    I->max_layer_arcs = 0;
+    I->max_layer_nodes = 0;
+    for (int l = 0; l < I->L; ++l) {
+        I->max_layer_arcs = std::max<int64_t>(I->max_layer_arcs, arc_at[l + 1] - arc_at[l]);
+        I->max_layer_nodes = std::max<int64_t>(I->max_layer_nodes, I->layer_off[l + 1] - I->layer_off[l]);
+    }
+}
+
 int prepare_instance(const pmdd_dd &dd, const pmdd_options &o, uint64_t id, Instance *I, std::string *err,
                      bool with_out_csr, bool pack) {
     auto bad = [&](const std::string &m) {
@@ -330,10 +349,8 @@ int prepare_instance(const pmdd_dd &dd, const pmdd_options &o, uint64_t id, Inst
         dev = align256(dev + sizeof(int32_t) * static_cast<size_t>(N));       // cursor
     }
     I->dev_bytes = dev;
-    // admission estimate: the DD, plus a few layers' worth of frontier slots
-    int64_t widest_arcs = 0;
-    for (int l = 0; l < L; ++l) widest_arcs = std::max<int64_t>(widest_arcs, I->arc_at_layer[l + 1] - I->arc_at_layer[l]);
-    I->est_bytes = static_cast<int64_t>(dev) + 8 * widest_arcs * static_cast<int64_t>(d * I->elem() + 16);
+    set_shape(I, I->arc_at_layer);
+    I->min_bytes = static_cast<int64_t>(dev);
     I->submit_s = now_s();
     return PMDD_OK;
 }
@@ -378,9 +395,8 @@ void prepare_tsp_instance(const TspStructure &S, int nobjs, const int32_t *cost,
     I->with_out_csr = true;
     I->sd_kind = 0;
     I->has_sd_order = false;
-    int64_t widest_arcs = 0;
-    for (int l = 0; l < L; ++l) widest_arcs = std::max<int64_t>(widest_arcs, S.arc_at[l + 1] - S.arc_at[l]);
-    I->est_bytes = static_cast<int64_t>(I->dev_bytes) + 8 * widest_arcs * static_cast<int64_t>(d * I->elem() + 16);
+    set_shape(I, S.arc_at);
+    I->min_bytes = static_cast<int64_t>(I->dev_bytes);
     I->submit_s = now_s();
 }
 
@@ -491,9 +507,8 @@ void layout_built_knapsack(Instance *I, int d, bool wide, const std::vector<int3
     dev = align256(dev + sizeof(int32_t) * static_cast<size_t>(A));
     dev = align256(dev + sizeof(int32_t) * static_cast<size_t>(N));
     I->dev_bytes = dev;
-    int64_t widest_arcs = 0;
-    for (int l = 0; l < L; ++l) widest_arcs = std::max<int64_t>(widest_arcs, arc_at_layer[l + 1] - arc_at_layer[l]);
-    I->est_bytes = static_cast<int64_t>(dev) + 8 * widest_arcs * static_cast<int64_t>(d * I->elem() + 16);
+    set_shape(I, arc_at_layer);
+    I->min_bytes = static_cast<int64_t>(dev);
     I->submit_s = now_s();
 }
 
@@ -557,7 +572,12 @@ Engine::Engine(int device, int64_t budget_bytes, int max_slots) : device_(device
         return;
     }
     std::memset(h_init_.p, 0, 256);
-    *reinterpret_cast<int32_t *>(static_cast<char *>(h_init_.p) + 128) = 1;
+    *reinterpret_cast<int32_t *>(static_cast<char *>(h_init_.p) + 128) = 1;  // size of the root frontier
+    *(static_cast<unsigned char *>(h_init_.p) + 132) = 1;                   // one point is sorted
+    const char *lx = std::getenv("PMDD_LEX_TILES");
+    if (lx && lx[0] == '0') lex_tiles_ = false;
+    const char *pm = std::getenv("PMDD_LEX_PAIR_MAX");
+    if (pm && *pm && std::atoi(pm) >= 0) lex_pair_max_ = std::atoi(pm);
     ok_ = true;
 }
 
@@ -633,6 +653,60 @@ void *Engine::scratch(size_t bytes) {
 
 void Engine::submit(std::unique_ptr<Instance> inst) { queued_.push_back(std::move(inst)); }
 
+int64_t Engine::predicted_bytes(const Instance &I) const {
+    const auto key = std::make_tuple(I.opts.problem_type, I.d, I.opts.method);
+    auto it = cand_per_arc_.find(key);
+    const double ratio = it != cand_per_arc_.end() ? it->second : 1.0;
+    // the largest layer of candidates: what the request has shown so far, its next
+    // expansion once counted (exact), and the class's learned ratio to the DD's arcs
+    int64_t c = std::max<int64_t>(I.peak_cand, static_cast<int64_t>(ratio * static_cast<double>(I.A)));
+    for (const Side *s : {&I.td, &I.bu})
+        if (s->counted) c = std::max<int64_t>(c, s->res.total);
+    const int64_t pb = static_cast<int64_t>(I.d) * static_cast<int64_t>(I.elem());
+    int64_t b = I.external_dd ? 0 : static_cast<int64_t>(I.dev_bytes);
+    b += 2 * c * pb + 8 * I.max_layer_arcs + 28 * I.max_layer_nodes;
+    if (I.opts.method == 3) {
+        const int64_t ucap = std::max<int64_t>(1 << 17, I.max_layer_nodes * (I.d + 1) + 4096);
+        b += c * pb + static_cast<int64_t>(dev::couple_bytes(ucap, I.d, I.elem()));
+    }
+    return b;
+}
+
+int64_t Engine::current_bytes(const Instance &I) const {
+    const int64_t pb = static_cast<int64_t>(I.d) * static_cast<int64_t>(I.elem());
+    int64_t b = I.external_dd ? 0 : static_cast<int64_t>(I.dev_bytes);
+    for (const Side *s : {&I.td, &I.bu})
+        if (s->pts) b += s->slot_points * pb;
+    return b;
+}
+
+int64_t Engine::reserved_growth() const {
+    int64_t r = 0;
+    for (const auto &p : active_)
+        if (p->phase != Instance::DONE) r += std::max<int64_t>(0, predicted_bytes(*p) - current_bytes(*p));
+    return r;
+}
+
+void Engine::learn_footprint(const Instance &I) {
+    if (I.A <= 0 || I.peak_cand <= 0) return;
+    const double seen = static_cast<double>(I.peak_cand) / static_cast<double>(I.A);
+    double &r = cand_per_arc_.emplace(std::make_tuple(I.opts.problem_type, I.d, I.opts.method), seen).first->second;
+    r = std::max(0.95 * r, seen);
+}
+
+void Engine::record_finish(const Instance &I) {
+    if (I.status == PMDD_OK) {
+        counters_.completed++;
+        learn_footprint(I);
+    } else if (I.status == PMDD_ERR_CANCELLED) {
+        counters_.cancelled++;
+    } else if (I.admit_s > 0) {
+        counters_.failed++;
+    } else {
+        counters_.rejected++;
+    }
+}
+
 void Engine::release_side(Side &s) {
     arena_.release(s.pts);
     arena_.release(s.off);
@@ -642,6 +716,7 @@ void Engine::release_side(Side &s) {
     s.pts = nullptr;
     s.off = nullptr;
     s.size = nullptr;
+    s.sorted = nullptr;
     s.arc_off = nullptr;
     s.big_list = nullptr;
     s.counted = false;
@@ -674,6 +749,7 @@ bool Engine::cancel(uint64_t id) {
         if ((*it)->id == id) {
             fail(**it, PMDD_ERR_CANCELLED, "request cancelled");
             (*it)->finish_s = now_s();
+            record_finish(**it);
             finished_.push_back(std::move(*it));
             queued_.erase(it);
             return true;
@@ -784,14 +860,16 @@ bool Engine::admit(Instance &I) {
     }
     auto seed = [&](Side &s, int layer) -> bool {
         s.layer = layer;
+        s.slot_points = 1;
         s.pts = arena_.alloc(8 * 8);
         s.off = static_cast<int64_t *>(arena_.alloc(sizeof(int64_t)));
-        s.size = static_cast<int32_t *>(arena_.alloc(sizeof(int32_t)));
+        s.size = static_cast<int32_t *>(arena_.alloc(2 * sizeof(int32_t)));  // size | sorted flag
         if (!s.pts || !s.off || !s.size) return false;
+        s.sorted = reinterpret_cast<uint8_t *>(s.size + 1);
         const char *h = static_cast<const char *>(h_init_.p);
         cudaMemcpyAsync(s.pts, h, 64, cudaMemcpyHostToDevice, stream_);
         cudaMemcpyAsync(s.off, h + 64, sizeof(int64_t), cudaMemcpyHostToDevice, stream_);
-        cudaMemcpyAsync(s.size, h + 128, sizeof(int32_t), cudaMemcpyHostToDevice, stream_);
+        cudaMemcpyAsync(s.size, h + 128, 2 * sizeof(int32_t), cudaMemcpyHostToDevice, stream_);
         s.counted = false;
         s.score = 0;
         return true;
@@ -822,6 +900,7 @@ struct ExpPlan {
     void *out_pts;
     int64_t *out_off;
     int32_t *out_size;
+    uint8_t *out_sorted;  // per destination: written in lexicographic order (after the tile plan)
     void *big_mem;    // oversized-destination scratch (one block, carved per use)
     int64_t big_total;
     int64_t cand;       // candidates of this expansion (trace / statistics)
@@ -853,27 +932,58 @@ int Engine::step() {
         ~LaunchTally() { g_total_launches += n - start; }
     } tally{launches_, launches_};
     // ---------------------------------------------------------------- admission
+    // A queued request is admitted when its predicted peak footprint fits beside what the
+    // running requests hold and are predicted to grow by; a request that does not fit
+    // stays queued and smaller ones behind it may pass, until it has been passed over
+    // kMaxPassOver times, after which nothing behind it is admitted before it.  With
+    // nothing running a request is always tried (its prediction may be pessimistic).  A
+    // request whose DD alone exceeds the budget is rejected at once.
+    constexpr int32_t kMaxPassOver = 32;
     std::vector<CountPlan> counts;
-    while (!queued_.empty() && static_cast<int>(active_.size()) < max_slots_) {
-        Instance &I = *queued_.front();
-        const bool room = static_cast<int64_t>(arena_.used()) + I.est_bytes <= static_cast<int64_t>(arena_.capacity());
-        if (!room && !active_.empty()) break;
-        if (!admit(I)) {
-            if (!ok_) return -1;
-            if (!active_.empty()) break;  // wait for memory to free up
-            fail(I, PMDD_ERR_OOM, "request does not fit the device memory budget");
+    const int64_t cap_bytes = static_cast<int64_t>(arena_.capacity());
+    int64_t reserved = reserved_growth();
+    for (auto it = queued_.begin(); it != queued_.end() && static_cast<int>(active_.size()) < max_slots_;) {
+        Instance &I = **it;
+        auto reject = [&](const std::string &msg) {
+            fail(I, PMDD_ERR_OOM, msg);
             I.finish_s = now_s();
-            finished_.push_back(std::move(queued_.front()));
-            queued_.pop_front();
+            record_finish(I);
+            finished_.push_back(std::move(*it));
+            it = queued_.erase(it);
+        };
+        if (I.min_bytes > cap_bytes) {
+            reject("request needs at least " + std::to_string(I.min_bytes) + " device bytes for its DD, above the "
+                   "memory budget of " + std::to_string(cap_bytes));
             continue;
         }
+        const int64_t pred = predicted_bytes(I);
+        const bool fits = static_cast<int64_t>(arena_.used()) + reserved + pred <= cap_bytes;
+        if (!fits && !active_.empty()) {
+            if (++I.skipped > kMaxPassOver) break;
+            ++it;
+            continue;
+        }
+        if (!admit(I)) {
+            if (!ok_) return -1;
+            if (!active_.empty()) {  // wait for memory to free up
+                if (++I.skipped > kMaxPassOver) break;
+                ++it;
+                continue;
+            }
+            reject("request does not fit the device memory budget");
+            continue;
+        }
+        counters_.admitted++;
+        reserved += std::max<int64_t>(0, pred - current_bytes(I));
         if (I.phase == Instance::RUNNING) {
             counts.push_back({&I, true, false});
             if (I.opts.method == 3) counts.push_back({&I, false, false});
         }
-        active_.push_back(std::move(queued_.front()));
-        queued_.pop_front();
+        active_.push_back(std::move(*it));
+        it = queued_.erase(it);
     }
+    counters_.running_peak = std::max<int64_t>(counters_.running_peak, static_cast<int64_t>(active_.size()));
+    counters_.queued_peak = std::max<int64_t>(counters_.queued_peak, static_cast<int64_t>(queued_.size()));
 
     // ------------------------------------------------------------ expansions
     std::vector<ExpPlan> exps;
@@ -902,13 +1012,14 @@ int Engine::step() {
         const int nl = is_td ? s.layer + 1 : s.layer - 1;
         const int64_t C = s.res.total;
         const int32_t V = I.nodes_in(nl);
-        ExpPlan e{&I, is_td, nl, nullptr, nullptr, nullptr, nullptr, 0, C, s.res.max_item, s.res.num_big};
+        ExpPlan e{&I, is_td, nl, nullptr, nullptr, nullptr, nullptr, nullptr, 0, C, s.res.max_item, s.res.num_big};
         const size_t pts_bytes = static_cast<size_t>(std::max<int64_t>(C, 1)) * I.d * I.elem();
         e.out_pts = arena_.alloc(pts_bytes);
         e.out_off = static_cast<int64_t *>(arena_.alloc(sizeof(int64_t) * V));
         // sizes of the new frontier, followed by the tile plan of this expansion
         const int64_t ntiles = std::max<int64_t>(1, (C + window - 1) / window);
-        e.out_size = static_cast<int32_t *>(arena_.alloc(sizeof(int32_t) * (V + ntiles + 1)));
+        e.out_size = static_cast<int32_t *>(arena_.alloc(sizeof(int32_t) * (V + ntiles + 1) + static_cast<size_t>(V)));
+        if (e.out_size) e.out_sorted = reinterpret_cast<uint8_t *>(e.out_size + V + ntiles + 1);
         bool okay = e.out_pts && e.out_off && e.out_size;
         if (okay && s.res.num_big > 0) {
             const int64_t bt = s.res.big_total;
@@ -997,6 +1108,9 @@ int Engine::step() {
                 J.tile_window = window;
                 J.num_tiles = std::max<int64_t>(1, (s.res.total + window - 1) / window);
                 J.tile_first = e.out_size + J.num_items;
+                J.prev_sorted = s.sorted;
+                J.out_sorted = e.out_sorted;
+                J.pair_max = lex_pair_max_;
                 J.tile_base = gl.tiles;
                 tile_bases[pos] = gl.tiles;
                 item_bases[pos] = gl.items;
@@ -1046,6 +1160,7 @@ int Engine::step() {
     std::vector<int64_t> sd_bases;
     std::vector<Instance *> sd_inst;
     std::vector<SdGroup> sdg;
+    bool sd_alloc_failed = false;
     {
         std::vector<size_t> pick;
         size_t keep_bytes = 0;
@@ -1058,13 +1173,9 @@ int Engine::step() {
                 keep_bytes += align256(static_cast<size_t>(std::max<int64_t>(e.cand, 1)));
             }
         }
-        if (!pick.empty()) {
-            char *keep = static_cast<char *>(scratch(keep_bytes));
-            if (!keep) {
-                error_ = "engine bookkeeping allocation failed";
-                ok_ = false;
-                return -1;
-            }
+        char *keep = pick.empty() ? nullptr : static_cast<char *>(scratch(keep_bytes));
+        if (!pick.empty() && !keep) sd_alloc_failed = true;  // rolled back below, before any launch
+        if (keep) {
             for (size_t k = 0; k < pick.size(); ++k) {
                 const ExpPlan &e = exps[pick[k]];
                 Instance &I = *e.I;
@@ -1130,7 +1241,7 @@ int Engine::step() {
         xjobs[k].err = d_err_step;
     }
     for (size_t k = 0; k < sdjobs.size(); ++k) sdjobs[k].removed = d_removed ? d_removed + k : nullptr;
-    bool count_alloc_ok = d_fixed != nullptr;
+    bool count_alloc_ok = d_fixed != nullptr && !sd_alloc_failed;
     // the expansion's new frontier is what the count reads; resolve per plan below
 
     // ------------------------------------------------------------- staging
@@ -1191,36 +1302,6 @@ int Engine::step() {
         J.big_list = new_big[k];
         J.result = d_results + k;
     }
-    if (!count_alloc_ok) {
-        // Out of device memory for bookkeeping: give everything back and fail the
-        // largest blocked request so the others can progress next step.
-        for (size_t k = 0; k < counts.size(); ++k) {
-            arena_.release(new_arc_off[k]);
-            arena_.release(new_big[k]);
-        }
-        for (const ExpPlan &e : exps) {
-            for (void *q : {e.out_pts, static_cast<void *>(e.out_off), static_cast<void *>(e.out_size), e.big_mem})
-                arena_.release(q);
-        }
-        for (void *q : step_scratch_) arena_.release(q);
-        step_scratch_.clear();
-        Instance *victim = exps.empty() ? (counts.empty() ? nullptr : counts.back().I) : exps.back().I;
-        if (victim) fail(*victim, PMDD_ERR_OOM, "device memory budget exhausted");
-        int done = 0;
-        for (auto it = active_.begin(); it != active_.end();) {
-            if ((*it)->phase == Instance::DONE) {
-                release_instance(**it);
-                (*it)->finish_s = now_s();
-                finished_.push_back(std::move(*it));
-                it = active_.erase(it);
-                ++done;
-            } else {
-                ++it;
-            }
-        }
-        return done;
-    }
-
     // requests whose sides meet this step enter coupling now
     std::vector<Instance *> entering;
     for (const ExpPlan &e : exps) {
@@ -1236,11 +1317,76 @@ int Engine::step() {
     const size_t off_u = off_k;  // CoupleJob array
     const size_t off_ctrinit = align256(off_u + sizeof(dev::CoupleJob) * n_couple_max);
     stage_bytes = align256(off_ctrinit + sizeof(int64_t) * dev::kCtrCount * n_couple_max);
-    if (!h_desc_.reserve(stage_bytes)) {
-        error_ = "cudaMallocHost failed";
-        ok_ = false;
-        return -1;
+    // Every device and pinned allocation of the step is made here, before any side moves
+    // or launch, so that running out of memory rolls the step back and fails one request
+    // instead of the engine.
+    char *d_stage = nullptr;
+    // host summary (D2H): the summary block | coupling ctrs | finishing sizes (bounds:
+    // every coupler, every expansion finishing)
+    const size_t s_counts = 0, s_ts = f_ts, s_sd = f_sd, s_err = f_err;
+    const size_t s_ctr = align256(f_total);
+    const size_t s_fin = align256(s_ctr + sizeof(int64_t) * dev::kCtrCount * n_couple_max);
+    const size_t s_total = s_fin + sizeof(int32_t) * exps.size();
+    // oversized path: per group, the size-order list and the mark-path plan
+    std::vector<int32_t *> big_order(glaunch.size(), nullptr);
+    std::vector<void *> big_plan(glaunch.size(), nullptr);
+    if (count_alloc_ok) {
+        if (stage_bytes) d_stage = static_cast<char *>(scratch(stage_bytes));
+        if ((stage_bytes && !d_stage) || !h_desc_.reserve(stage_bytes) || !h_summary_.reserve(s_total))
+            count_alloc_ok = false;
+        for (size_t g = 0; g < glaunch.size() && count_alloc_ok; ++g) {
+            const GroupLaunch &gl = glaunch[g];
+            if (gl.big_count == 0) continue;
+            const int64_t nw = static_cast<int64_t>(gl.big_count);
+            if (nw > sms_ * 3 && nw <= dev::kBigOrderMax) {
+                big_order[g] = static_cast<int32_t *>(scratch(sizeof(int32_t) * static_cast<size_t>(nw)));
+                if (!big_order[g]) count_alloc_ok = false;
+            }
+            const int mark_cap = static_cast<int>(std::min<int64_t>(gl.mark_cap, nw));
+            if (count_alloc_ok && mark_cap > 0) {
+                big_plan[g] = scratch(dev::big_plan_bytes(mark_cap));
+                if (!big_plan[g]) count_alloc_ok = false;
+            }
+        }
     }
+    if (!count_alloc_ok) {
+        // Out of device memory for bookkeeping: give everything back and fail the
+        // largest blocked request so the others can progress next step.
+        for (size_t k = 0; k < counts.size(); ++k) {
+            arena_.release(new_arc_off[k]);
+            arena_.release(new_big[k]);
+        }
+        for (const ExpPlan &e : exps) {
+            for (void *q : {e.out_pts, static_cast<void *>(e.out_off), static_cast<void *>(e.out_size), e.big_mem})
+                arena_.release(q);
+        }
+        for (void *q : step_scratch_) arena_.release(q);
+        step_scratch_.clear();
+        // the request with the largest expansion of this step (else the last one counted)
+        Instance *victim = counts.empty() ? nullptr : counts.back().I;
+        int64_t most = -1;
+        for (const ExpPlan &e : exps)
+            if (e.cand > most) {
+                most = e.cand;
+                victim = e.I;
+            }
+        if (victim) fail(*victim, PMDD_ERR_OOM, "device memory budget exhausted");
+        int done = 0;
+        for (auto it = active_.begin(); it != active_.end();) {
+            if ((*it)->phase == Instance::DONE) {
+                release_instance(**it);
+                (*it)->finish_s = now_s();
+                record_finish(**it);
+                finished_.push_back(std::move(*it));
+                it = active_.erase(it);
+                ++done;
+            } else {
+                ++it;
+            }
+        }
+        return done;
+    }
+
     char *hs = static_cast<char *>(h_desc_.p);
     if (!xjobs.empty()) std::memcpy(hs + off_x, xjobs.data(), sizeof(dev::ExpandJob) * xjobs.size());
     if (!bigwork.empty()) std::memcpy(hs + off_b, bigwork.data(), sizeof(dev::BigWork) * bigwork.size());
@@ -1270,9 +1416,12 @@ int Engine::step() {
         to_release.push_back(e.big_mem);
         I.stats.work_candidates_total += s.res.total;
         I.stats.work_candidates_peak = std::max(I.stats.work_candidates_peak, s.res.total);
+        I.peak_cand = std::max(I.peak_cand, s.res.total);
+        s.slot_points = std::max<int64_t>(e.cand, 1);
         s.pts = e.out_pts;
         s.off = e.out_off;
         s.size = e.out_size;
+        s.sorted = e.out_sorted;
         s.arc_off = nullptr;
         s.big_list = nullptr;
         s.counted = false;
@@ -1331,17 +1480,6 @@ int Engine::step() {
     if (!ujobs.empty()) std::memcpy(hs + off_u, ujobs.data(), sizeof(dev::CoupleJob) * ujobs.size());
 
     // ----------------------------------------------------------- device work
-    char *d_stage = stage_bytes ? static_cast<char *>(scratch(stage_bytes)) : nullptr;
-    // host summary (D2H): the summary block | coupling ctrs | finishing sizes
-    const size_t s_counts = 0, s_ts = f_ts, s_sd = f_sd, s_err = f_err;
-    const size_t s_ctr = align256(f_total);
-    const size_t s_fin = align256(s_ctr + sizeof(int64_t) * dev::kCtrCount * ujobs.size());
-    const size_t s_total = s_fin + sizeof(int32_t) * finishing.size();
-    if ((stage_bytes && !d_stage) || !h_summary_.reserve(s_total)) {
-        error_ = "engine bookkeeping allocation failed";
-        ok_ = false;
-        return -1;
-    }
     cudaEvent_t ev0 = ev_[0], ev1 = ev_[1], ev2 = ev_[2], ev3 = ev_[3];
     if (stage_bytes && !cuda_ok(cudaMemcpyAsync(d_stage, hs, stage_bytes, cudaMemcpyHostToDevice, stream_), "H2D"))
         return -1;
@@ -1360,15 +1498,17 @@ int Engine::step() {
         if (!cuda_ok(dev::launch_tile_plan(dj, dib, static_cast<int>(gl.count), gl.items, stream_), "tile_plan_kernel"))
             return -1;
         const int grid = sms_ * 8;
-        if (!cuda_ok(dev::launch_expand_tiles(gl.d, gl.wide, dj, dtb, static_cast<int>(gl.count), gl.tiles, grid,
-                                              stream_),
-                     "expand_tile_kernel"))
-            return -1;
+        const bool lex = gl.d == 3 && lex_tiles_;
+        const cudaError_t te =
+            lex ? dev::launch_expand_tiles_lex(gl.wide, dj, dtb, static_cast<int>(gl.count), gl.tiles, grid, stream_)
+                : dev::launch_expand_tiles(gl.d, gl.wide, dj, dtb, static_cast<int>(gl.count), gl.tiles, grid, stream_);
+        if (!cuda_ok(te, lex ? "expand_tile_lex_kernel" : "expand_tile_kernel")) return -1;
         launches_ += 2;
         ktimes_.tile_launches += 1;
     }
     cudaEventRecord(ev1, stream_);
-    for (const GroupLaunch &gl : glaunch) {
+    for (size_t g = 0; g < glaunch.size(); ++g) {
+        const GroupLaunch &gl = glaunch[g];
         if (gl.big_count == 0) continue;
         const dev::ExpandJob *dj = reinterpret_cast<const dev::ExpandJob *>(d_stage + off_x) + gl.first;
         dev::BigLaunch L;
@@ -1383,24 +1523,9 @@ int Engine::step() {
         L.mark_cap = static_cast<int>(std::min<int64_t>(gl.mark_cap, static_cast<int64_t>(gl.big_count)));
         L.plan = nullptr;
         // more SFS blocks than fit the SMs at once: start the largest destinations first
-        L.order = nullptr;
-        const bool ordered = L.num_work > sms_ * 3 && L.num_work <= dev::kBigOrderMax;
-        if (ordered) {
-            L.order = static_cast<int32_t *>(scratch(sizeof(int32_t) * static_cast<size_t>(L.num_work)));
-            if (!L.order) {
-                error_ = "engine bookkeeping allocation failed";
-                ok_ = false;
-                return -1;
-            }
-        }
-        if (L.mark_cap > 0) {
-            L.plan = scratch(dev::big_plan_bytes(L.mark_cap));
-            if (!L.plan) {
-                error_ = "engine bookkeeping allocation failed";
-                ok_ = false;
-                return -1;
-            }
-        }
+        L.order = big_order[g];
+        const bool ordered = L.order != nullptr;
+        L.plan = big_plan[g];
         for (int64_t pass = 0; pass < gl.big_passes; ++pass) {
             L.pass = pass;
             if (!cuda_ok(dev::launch_big(gl.d, gl.wide, L, stream_), "oversized-destination kernels")) return -1;
@@ -1590,6 +1715,7 @@ int Engine::step() {
             I.stats.gpu_mem_peak_reserved_bytes = static_cast<int64_t>(arena_.reserved());
             release_instance(I);
             I.finish_s = now_s();
+            record_finish(I);
             finished_.push_back(std::move(*it));
             it = active_.erase(it);
             ++done;

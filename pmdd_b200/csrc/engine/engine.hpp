@@ -47,9 +47,17 @@ class Arena {
     size_t peak() const { return peak_; }
     void reset_peak() { peak_ = used_; }
     double grow_seconds() const { return grow_s_; }  // host time spent in cudaMalloc
+    // Fault injection for tests of the failure paths: after `after` more allocation
+    // calls, the next `count` calls fail as if the device were out of memory.
+    void inject_failures(int64_t after, int64_t count) {
+        inj_after_ = after;
+        inj_count_ = count;
+    }
+    int64_t injected_failures() const { return injected_; }
 
   private:
     bool grow(size_t at_least);
+    int64_t inj_after_ = 0, inj_count_ = 0, injected_ = 0;
     size_t cap_ = 0, reserved_ = 0, used_ = 0, peak_ = 0;
     double grow_s_ = 0;
     std::map<uintptr_t, size_t> chunks_;            // cudaMalloc base -> bytes
@@ -64,12 +72,14 @@ struct Side {
     void *pts = nullptr;
     int64_t *off = nullptr;
     int32_t *size = nullptr;
+    uint8_t *sorted = nullptr;     // per node: frontier in descending lexicographic order (in the size block)
     // counts for the next layer in this direction
     bool counted = false;
     int64_t *arc_off = nullptr;
     int64_t *big_list = nullptr;
     dev::CountResult res{};
     int64_t score = 0;
+    int64_t slot_points = 0;       // candidate slots of the current frontier (its memory)
 };
 
 // The shared part of every TSP MDD of n cities (tspbuild.cuh): all arrays but the
@@ -133,7 +143,12 @@ struct Instance {
     int64_t result_n = 0;
     pmdd_stats stats{};
     double submit_s = 0, admit_s = 0, finish_s = 0;
-    int64_t est_bytes = 0;              // admission estimate
+    // admission: the exact minimum (the DD's device copy) and what the footprint
+    // prediction uses -- the largest layers seen so far and the DD's shape
+    int64_t min_bytes = 0;
+    int64_t peak_cand = 0;              // largest expansion (candidates) so far, either side
+    int64_t max_layer_arcs = 0, max_layer_nodes = 0;
+    int32_t skipped = 0;                // admission passes this request was passed over
     bool external_dd = false;           // DD already resident (owned by a pmdd_resident set)
     const TspStructure *tsp = nullptr;  // TSP MDD: structure shared, I.dd holds the weight table only
     bool with_out_csr = false;          // device copy carries the bottom-up CSR
@@ -202,6 +217,14 @@ class Engine {
     size_t queued() const { return queued_.size(); }
     size_t running() const { return active_.size(); }
     std::deque<std::unique_ptr<Instance>> &finished() { return finished_; }
+    // Hands a request that failed before reaching the queue (its status and error set)
+    // straight to the finished list, counting it as rejected.
+    void finish_rejected(std::unique_ptr<Instance> I) {
+        I->phase = Instance::DONE;
+        I->finish_s = now_s();
+        counters_.rejected++;
+        finished_.push_back(std::move(I));
+    }
     bool cancel(uint64_t id);
     int64_t launches() const { return launches_; }
     const Arena &arena() const { return arena_; }
@@ -209,6 +232,21 @@ class Engine {
     void reset_mem_peak() { arena_.reset_peak(); }
     int device() const { return device_; }
     cudaStream_t stream() const { return stream_; }
+    // Serving counters (requests since the engine started).
+    struct Counters {
+        int64_t admitted = 0, rejected = 0, completed = 0, failed = 0, cancelled = 0;
+        int64_t queued_peak = 0, running_peak = 0;
+    };
+    const Counters &counters() const { return counters_; }
+    // Device bytes the admission model predicts for the request at its peak (its DD, two
+    // layers of frontier slots at the predicted largest layer, per-layer bookkeeping,
+    // and for method 3 the other side's frontier and the coupling block), and the
+    // bytes it holds now.
+    int64_t predicted_bytes(const Instance &I) const;
+    int64_t current_bytes(const Instance &I) const;
+    // Predicted growth of the running requests (sum of predicted minus current bytes).
+    int64_t reserved_growth() const;
+    void inject_alloc_failures(int64_t after, int64_t count) { arena_.inject_failures(after, count); }
     KernelTimes kernel_times() const { return ktimes_; }
     // Device copy of a prepared request's DD (with the bottom-up CSR) that stays in
     // the arena until release_dd(); requests then share it via external_dd.
@@ -279,8 +317,18 @@ class Engine {
     // destinations that leave the tiles for their arc count).
     int64_t mark_min_for(int d, int problem_type) const;
     void load_tuning();
+    // Three-objective tiles in lexicographic order (tile_lex.cu): on unless PMDD_LEX_TILES=0;
+    // destinations of at most lex_pair_max_ candidates are checked pairwise (PMDD_LEX_PAIR_MAX).
+    bool lex_tiles_ = true;
+    int32_t lex_pair_max_ = 48;
     int64_t big_mark_min_fixed_ = 0;
     std::map<std::pair<int, int>, int64_t> tuned_mark_min_;
+    // Footprint model: largest layer's candidates per DD arc, learned per (problem type,
+    // objectives, method) from finished requests (a max that decays by 5 % per finish).
+    std::map<std::tuple<int, int, int>, double> cand_per_arc_;
+    void learn_footprint(const Instance &I);
+    void record_finish(const Instance &I);
+    Counters counters_;
 };
 
 }  // namespace pmdd

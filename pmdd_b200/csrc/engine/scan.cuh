@@ -97,6 +97,17 @@ __device__ __forceinline__ int64_t item_start(const int32_t *item_arc_off, const
     return arc_cand_off[item_arc_off[item_base + i] - arc_base];
 }
 
+// First index in bases[0..n) with bases[idx] <= x < bases[idx+1] (bases ascending).
+__device__ __forceinline__ int find_base(const int64_t *__restrict__ bases, int n, int64_t x) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(bases + mid) <= x) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
 #define PMDD_DISPATCH_D(D_, CALL)                  \
     switch (D_) {                                  \
     case 1: { constexpr int DD = 1; return CALL; } \

@@ -56,17 +56,6 @@ struct TileSmem {
     int32_t chunk;                      // next 32-candidate chunk to filter
 };
 
-// First index in bases[0..n) with bases[idx] <= x < bases[idx+1] (bases ascending).
-__device__ __forceinline__ int find_base(const int64_t *__restrict__ bases, int n, int64_t x) {
-    int lo = 0, hi = n - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (__ldg(bases + mid) <= x) lo = mid;
-        else hi = mid - 1;
-    }
-    return lo;
-}
-
 // ------------------------------------------------------------------ tile plan
 __global__ void tile_plan_kernel(const ExpandJob *__restrict__ jobs, const int64_t *__restrict__ item_bases,
                                  int num_jobs, int64_t total_items) {
@@ -181,6 +170,7 @@ __global__ void __launch_bounds__(kTT) expand_tile_kernel(const ExpandJob *__res
                     const int64_t c = J.arc_cand_off[a1 - J.arc_base] - s;
                     J.out_off[i] = s;
                     if (c == 0) J.out_size[i] = 0;
+                    if (J.out_sorted) J.out_sorted[i] = c == 0 ? 1 : 0;  // written in arc order
                     S.item_c0[k] = s;
                     S.item_a0g[k] = a0;
                     if (c > 0 && tile_resident(c, a1 - a0)) {

@@ -1,0 +1,524 @@
+// Fused expand + dominance filter for three objectives, in lexicographic order.
+//
+// Every node's frontier is kept in descending lexicographic order (objective 0, then 1,
+// then 2).  Adding an arc's weight vector to every point of a frontier keeps that order,
+// so the candidates of one arc ("a run") arrive sorted, and a destination's candidates
+// are a few sorted runs.  In that order a point can only be dominated by a point before
+// it, and since every point before q has objective 0 >= q's, q is dominated (or a later
+// copy of an equal point) iff some earlier point has objectives 1 and 2 both >= q's: a
+// two-dimensional "staircase" question.  The staircase of a destination's first points
+// -- the two-dimensional maxima of (objective 1, objective 2) among them -- stays small
+// (a few to a few dozen entries on the workloads measured), so one warp can answer it
+// for a whole destination in one ordered pass.
+//
+//   stage:   as the pairwise tile kernel (tile.cu): destinations and their arcs, with
+//            each arc's parent flag "frontier sorted";
+//   expand:  candidate = parent point + arc weight, in run order;
+//   merge:   each candidate's position in its destination's lexicographic order is its
+//            index in its run plus, per other run, a binary search for how many of that
+//            run's points come before it (equal points: the lower run first); a
+//            destination with more than kMergeMaxArcs runs or an unsorted run counts
+//            the points before it instead;
+//   filter:  destinations of at most J.pair_max candidates: each candidate is checked
+//            against the points before it in the merged order; larger destinations:
+//            one warp walks the merged order 32 candidates at a time -- each candidate
+//            is looked up in the staircase so far (a binary search over objective 1),
+//            the chunk's survivors are checked against each other with warp ballots and
+//            shuffles, and the staircase is rebuilt from its survivors and the chunk's
+//            new two-dimensional maxima;
+//   write:   survivors go to the destination's slot in merged order, so the next
+//            layer's runs are sorted again (out_sorted = 1).
+//
+// The keep rule is the reference GPU filter's (src/pmdd/enum/gpu/dominance_utils.cuh:
+// 10-23): q is dropped iff another candidate p of the destination has p >= q on every
+// objective and (p != q or p comes first).  Of equal points the first in the merged order
+// stays; which copy stays does not change the frontier.  Oversized destinations are
+// left to big.cu, whose output is not in this order (out_sorted = 0): their children
+// merge by counting.
+#include "kernels.cuh"
+#include "scan.cuh"
+
+#include <algorithm>
+
+namespace pmdd {
+namespace dev {
+
+namespace {
+
+constexpr int kLT = kTileThreads;
+constexpr int kLexWarps = kLT / 32;
+constexpr int kStairCap = 64;      // staircase entries a warp keeps; beyond it: pairwise
+constexpr int kMergeMaxArcs = 16;  // more runs in a destination: rank by counting
+constexpr unsigned kFull = 0xffffffffu;
+
+template <typename T>
+struct LexSmem {
+    PackedPt<3, T> pts[kTileCap];        // candidates in run order; staircases after the merge
+    PackedPt<3, T> mpts[kTileCap];       // candidates in merged (descending lexicographic) order
+    int16_t tag[kTileCap];               // staged arc of each run-order candidate
+    uint16_t item_of[kTileCap];          // staged destination of each candidate (either order)
+    uint8_t keep[kTileCap];              // by merged position
+    int16_t keep_ex[kTileCap + 1];       // exclusive scan of keep
+    int16_t item_s[kTileItemCap + 1];    // staged destination -> first candidate position
+    int16_t item_arc0[kTileItemCap + 1]; // staged destination -> first staged arc
+    int32_t item_a0g[kTileItemCap];      // staged destination -> first arc (global id)
+    int64_t item_c0[kTileItemCap];       // staged destination -> job-local candidate start
+    uint8_t item_count[kTileItemCap];    // 1: merge by counting
+    int16_t big[kTileItemCap];           // destinations filtered by a staircase warp
+    int16_t arc_pos[kTileArcCap + 1];    // staged arc -> first candidate position
+    int32_t arc_w[kTileArcCap];          // staged arc -> weight row
+    int64_t arc_src[kTileArcCap];        // staged arc -> parent slot start (points)
+    int32_t warp_i[32];
+    int32_t tot_i, tot_a, i0, i1, job;
+    int32_t n_big, next_big, next_chunk;
+};
+
+// Per-warp staircase storage, laid over pts once the merge has read it: two buffers
+// (current, next) of objective-1 and objective-2 values.
+template <typename T>
+struct Stair {
+    T v1[2][kStairCap];
+    T v2[2][kStairCap];
+};
+
+template <typename T>
+__device__ __forceinline__ bool lex_gt(const PackedPt<3, T> &a, const PackedPt<3, T> &b) {
+    if (a.v[0] != b.v[0]) return a.v[0] > b.v[0];
+    if (a.v[1] != b.v[1]) return a.v[1] > b.v[1];
+    return a.v[2] > b.v[2];
+}
+
+template <typename T>
+__device__ __forceinline__ bool lex_eq(const PackedPt<3, T> &a, const PackedPt<3, T> &b) {
+    return a.v[0] == b.v[0] && a.v[1] == b.v[1] && a.v[2] == b.v[2];
+}
+
+// Candidates of one big destination, merged positions [s, e), walked by one warp.
+template <typename T>
+__device__ void stair_filter(LexSmem<T> &S, Stair<T> &st, int s, int e, int lane) {
+    int cur = 0;        // staircase buffer in use
+    int m = 0;          // staircase entries (warp-uniform), objective 1 descending
+    bool overflow = false;
+    const unsigned lt_mask = (1u << lane) - 1u;
+    for (int c0 = s; c0 < e; c0 += 32) {
+        const int p = c0 + lane;
+        const bool valid = p < e;
+        T q1 = 0, q2 = 0;
+        if (valid) {
+            q1 = S.mpts[p].v[1];
+            q2 = S.mpts[p].v[2];
+        }
+        bool dom = !valid;
+        if (overflow) {
+            // staircase given up: every point before p, chunk-mates included
+            const int hi = min(e, c0 + 32) - 1;
+            for (int j = s; j < hi; ++j) {
+                const PackedPt<3, T> c = S.mpts[j];
+                if (j < p) dom |= (c.v[1] >= q1) & (c.v[2] >= q2);
+                if (((j - s) & 15) == 15 && __all_sync(kFull, dom)) break;
+            }
+            if (valid) S.keep[p] = dom ? 0 : 1;
+            continue;
+        }
+        // staircase lookup: cnt = entries with objective 1 >= q1; the last of them holds
+        // the largest objective 2 among them
+        int cnt = 0;
+        if (valid && m > 0) {
+            int a = 0, b = m;
+            while (a < b) {
+                const int mid = (a + b) >> 1;
+                if (st.v1[cur][mid] >= q1) a = mid + 1;
+                else b = mid;
+            }
+            cnt = a;
+            dom = cnt > 0 && st.v2[cur][cnt - 1] >= q2;
+        }
+        // the chunk's surviving candidates against each other: an earlier one dominates;
+        // a later one that is larger in both (and not equal) removes it from the staircase
+        const unsigned alive = __ballot_sync(kFull, !dom);
+        bool rem = false;
+        unsigned mm = alive;
+        while (mm) {
+            const int j = __ffs(mm) - 1;
+            mm &= mm - 1;
+            const T a1 = __shfl_sync(kFull, q1, j), a2 = __shfl_sync(kFull, q2, j);
+            const bool ge = (a1 >= q1) & (a2 >= q2);
+            dom |= ge & (j < lane);
+            rem |= ge & (j > lane) & ((a1 != q1) | (a2 != q2));
+        }
+        if (valid) S.keep[p] = dom ? 0 : 1;
+        if (c0 + 32 >= e) break;
+        // next staircase: surviving entries and the chunk's new maxima, objective 1 descending
+        const bool fresh = !dom && !rem;
+        const unsigned nmask = __ballot_sync(kFull, fresh);
+        T eA1 = 0, eA2 = 0, eB1 = 0, eB2 = 0;
+        const bool hasA = lane < m, hasB = lane + 32 < m;
+        if (hasA) {
+            eA1 = st.v1[cur][lane];
+            eA2 = st.v2[cur][lane];
+        }
+        if (hasB) {
+            eB1 = st.v1[cur][lane + 32];
+            eB2 = st.v2[cur][lane + 32];
+        }
+        bool killA = false, killB = false;
+        int gtA = 0, gtB = 0, gtq = 0;
+        unsigned nn = nmask;
+        while (nn) {
+            const int j = __ffs(nn) - 1;
+            nn &= nn - 1;
+            const T n1 = __shfl_sync(kFull, q1, j), n2 = __shfl_sync(kFull, q2, j);
+            killA |= hasA & (n1 >= eA1) & (n2 >= eA2);
+            killB |= hasB & (n1 >= eB1) & (n2 >= eB2);
+            gtA += (n1 > eA1) ? 1 : 0;
+            gtB += (n1 > eB1) ? 1 : 0;
+            gtq += (n1 > q1) ? 1 : 0;
+        }
+        const unsigned survA = __ballot_sync(kFull, hasA && !killA);
+        const unsigned survB = __ballot_sync(kFull, hasB && !killB);
+        const int nsA = __popc(survA);
+        const int m_next = nsA + __popc(survB) + __popc(nmask);
+        if (m_next > kStairCap) {
+            overflow = true;
+            continue;
+        }
+        const int nxt = cur ^ 1;
+        if (hasA && !killA) {
+            const int pos = __popc(survA & lt_mask) + gtA;
+            st.v1[nxt][pos] = eA1;
+            st.v2[nxt][pos] = eA2;
+        }
+        if (hasB && !killB) {
+            const int pos = nsA + __popc(survB & lt_mask) + gtB;
+            st.v1[nxt][pos] = eB1;
+            st.v2[nxt][pos] = eB2;
+        }
+        if (fresh) {
+            // surviving entries before q: those among the first cnt (objective 1 >= q1);
+            // an entry with objective 1 == q1 is dominated by q and did not survive
+            const int ca = min(cnt, 32), cb = max(cnt - 32, 0);
+            const unsigned ma = ca >= 32 ? kFull : ((1u << ca) - 1u);
+            const unsigned mb = cb >= 32 ? kFull : ((1u << cb) - 1u);
+            const int pos = __popc(survA & ma) + __popc(survB & mb) + gtq;
+            st.v1[nxt][pos] = q1;
+            st.v2[nxt][pos] = q2;
+        }
+        __syncwarp();
+        cur = nxt;
+        m = m_next;
+    }
+}
+
+}  // namespace
+
+template <typename T>
+__global__ void __launch_bounds__(kLT) expand_tile_lex_kernel(const ExpandJob *__restrict__ jobs,
+                                                              const int64_t *__restrict__ tile_bases, int num_jobs,
+                                                              int64_t total_tiles) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    LexSmem<T> &S = *reinterpret_cast<LexSmem<T> *>(smem_raw);
+    Stair<T> *stairs = reinterpret_cast<Stair<T> *>(&S.pts[0]);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int64_t tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
+        if (tid == 0) {
+            const int j = find_base(tile_bases, num_jobs, tile);
+            const ExpandJob &J = jobs[j];
+            const int64_t t = tile - tile_bases[j];
+            S.job = j;
+            S.i0 = J.tile_first[t];
+            S.i1 = J.tile_first[t + 1];
+        }
+        __syncthreads();
+        const ExpandJob &J = jobs[S.job];
+        const int32_t i0 = S.i0, i1 = S.i1;
+        const T *__restrict__ prev = static_cast<const T *>(J.prev_pts);
+        T *__restrict__ outp = static_cast<T *>(J.out_pts);
+        const int pair_max = J.pair_max;
+        int32_t ic = i0;
+        while (ic < i1) {
+            const int n_stage = min(kTileItemCap, i1 - ic);
+            // --- stage destinations: candidate starts and sizes, arc ranges
+            constexpr int PER = kTileItemCap / kLT;
+            static_assert(PER >= 1, "one destination per thread at least");
+            int32_t cnt[PER], narc[PER];
+            int32_t local = 0, local_a = 0;
+#pragma unroll
+            for (int r = 0; r < PER; ++r) {
+                const int k = tid * PER + r;
+                cnt[r] = 0;
+                narc[r] = 0;
+                if (k < n_stage) {
+                    const int32_t i = ic + k;
+                    const int32_t v = J.item_base + i;
+                    const int32_t a0 = J.item_arc_off[v], a1 = J.item_arc_off[v + 1];
+                    const int64_t s = J.arc_cand_off[a0 - J.arc_base];
+                    const int64_t c = J.arc_cand_off[a1 - J.arc_base] - s;
+                    J.out_off[i] = s;
+                    const bool resident = c > 0 && tile_resident(c, a1 - a0);
+                    if (c == 0) J.out_size[i] = 0;
+                    if (J.out_sorted) J.out_sorted[i] = (c == 0 || resident) ? 1 : 0;
+                    S.item_c0[k] = s;
+                    S.item_a0g[k] = a0;
+                    S.item_count[k] = 0;
+                    if (resident) {
+                        cnt[r] = static_cast<int32_t>(c);
+                        narc[r] = a1 - a0;
+                    }
+                }
+                local += cnt[r];
+                local_a += narc[r];
+            }
+            const int32_t ex = block_exclusive_scan<int32_t, kLT>(local, S.warp_i, &S.tot_i);
+            const int32_t exa = block_exclusive_scan<int32_t, kLT>(local_a, S.warp_i, &S.tot_a);
+            // this pass takes the longest prefix of staged destinations whose arcs fit
+            int32_t fit = 0;
+            {
+                int32_t run = ex, runa = exa;
+#pragma unroll
+                for (int r = 0; r < PER; ++r) {
+                    const int k = tid * PER + r;
+                    if (k < n_stage) {
+                        S.item_s[k] = static_cast<int16_t>(run);
+                        S.item_arc0[k] = static_cast<int16_t>(runa);
+                        if (runa + narc[r] <= kTileArcCap) ++fit;
+                        if (narc[r] > kMergeMaxArcs) S.item_count[k] = 1;
+                    }
+                    run += cnt[r];
+                    runa += narc[r];
+                }
+            }
+            (void)block_exclusive_scan<int32_t, kLT>(fit, S.warp_i, &S.tot_i);
+            const int n_it = S.tot_i;  // >= 1: one destination has at most kTileArcCap / 2 arcs
+            if (n_it == 0) {           // impossible for well-formed plans; skip defensively
+                if (tid == 0) atomicOr(J.err, kErrBounds);
+                break;
+            }
+            __syncthreads();
+            if (tid == 0) {
+                int32_t e = S.item_s[n_it - 1], ea = S.item_arc0[n_it - 1];
+                const int32_t v = J.item_base + ic + n_it - 1;
+                const int32_t a0 = J.item_arc_off[v], a1 = J.item_arc_off[v + 1];
+                const int64_t c = J.arc_cand_off[a1 - J.arc_base] - J.arc_cand_off[a0 - J.arc_base];
+                if (c > 0 && tile_resident(c, a1 - a0)) {
+                    e += static_cast<int32_t>(c);
+                    ea += a1 - a0;
+                }
+                S.item_s[n_it] = static_cast<int16_t>(e);
+                S.item_arc0[n_it] = static_cast<int16_t>(ea);
+                S.tot_i = e;
+                S.tot_a = ea;
+                S.n_big = 0;
+                S.next_big = 0;
+                S.next_chunk = 0;
+            }
+            __syncthreads();
+            const int32_t total = S.tot_i, total_a = S.tot_a;
+            if (total > kTileCap || total_a > kTileArcCap) {  // impossible for well-formed offsets
+                if (tid == 0) atomicOr(J.err, kErrBounds);
+                break;
+            }
+            // --- stage the arcs of the small destinations (and whether each parent is sorted)
+            for (int x = tid; x < total_a; x += kLT) {
+                int lo = 0, hi = n_it - 1;  // destination owning staged arc x
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (S.item_arc0[mid] <= x) lo = mid;
+                    else hi = mid - 1;
+                }
+                const int k = lo;
+                const int32_t a = S.item_a0g[k] + (x - S.item_arc0[k]);
+                const int64_t c0 = J.arc_cand_off[a - J.arc_base];
+                const int32_t nb = J.arc_nbr[a] - J.prev_base;
+                S.arc_pos[x] = static_cast<int16_t>(S.item_s[k] + (c0 - S.item_c0[k]));
+                S.arc_src[x] = J.prev_off[nb];
+                S.arc_w[x] = J.arc_wrow[a];
+                if (J.prev_sorted == nullptr || J.prev_sorted[nb] == 0) S.item_count[k] = 1;
+            }
+            if (tid == 0) S.arc_pos[total_a] = static_cast<int16_t>(total);
+            __syncthreads();
+            // --- expand: candidate = parent point + arc weight (run order)
+            for (int q = tid; q < total; q += kLT) {
+                int lo = 0, hi = n_it - 1;
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (S.item_s[mid] <= q) lo = mid;
+                    else hi = mid - 1;
+                }
+                const int k = lo;
+                int alo = S.item_arc0[k], ahi = S.item_arc0[k + 1] - 1;
+                while (alo < ahi) {
+                    const int mid = (alo + ahi + 1) >> 1;
+                    if (S.arc_pos[mid] <= q) alo = mid;
+                    else ahi = mid - 1;
+                }
+                const int x = alo;
+                const int64_t idx = q - S.arc_pos[x];
+                const T *src = prev + (S.arc_src[x] + idx) * 3;
+                const int32_t *w = J.weights + static_cast<int64_t>(S.arc_w[x]) * 3;
+                PackedPt<3, T> pt;
+#pragma unroll
+                for (int o = 0; o < PackedPt<3, T>::kPad; ++o) pt.v[o] = o < 3 ? src[o] + static_cast<T>(w[o]) : T(0);
+                S.pts[q] = pt;
+                S.tag[q] = static_cast<int16_t>(x);
+                S.item_of[q] = static_cast<uint16_t>(k);
+            }
+            __syncthreads();
+            // --- merge: each candidate's position in its destination's lexicographic order
+            for (int q = tid; q < total; q += kLT) {
+                const int k = S.item_of[q];
+                const int x = S.tag[q];
+                const int js = S.item_s[k], je = S.item_s[k + 1];
+                const PackedPt<3, T> me = S.pts[q];
+                int rank = 0;
+                if (S.item_count[k] == 0) {
+                    rank = q - S.arc_pos[x];
+                    const int y0 = S.item_arc0[k], y1 = S.item_arc0[k + 1];
+                    for (int y = y0; y < y1; ++y) {
+                        if (y == x) continue;
+                        const int lo = S.arc_pos[y], hi = (y + 1 < y1) ? S.arc_pos[y + 1] : je;
+                        // points of run y before me: larger, or equal in a lower run; a prefix
+                        const bool tie_first = y < x;
+                        int a = lo, b = hi;
+                        while (a < b) {
+                            const int mid = (a + b) >> 1;
+                            const PackedPt<3, T> c = S.pts[mid];
+                            const bool before = lex_gt(c, me) || (tie_first && lex_eq(c, me));
+                            if (before) a = mid + 1;
+                            else b = mid;
+                        }
+                        rank += a - lo;
+                    }
+                } else {
+                    for (int j = js; j < je; ++j) {
+                        const PackedPt<3, T> c = S.pts[j];
+                        rank += (lex_gt(c, me) || (j < q && lex_eq(c, me))) ? 1 : 0;
+                    }
+                }
+                S.mpts[js + rank] = me;
+            }
+            // destinations for the staircase warps, largest first in three tiers
+            for (int tier = 0; tier < 3; ++tier) {
+                const int lo_c = tier == 0 ? 512 : (tier == 1 ? 128 : pair_max);
+                const int hi_c = tier == 0 ? kTileCap : (tier == 1 ? 512 : 128);
+                for (int k = tid; k < n_it; k += kLT) {
+                    const int c = S.item_s[k + 1] - S.item_s[k];
+                    if (c > lo_c && c <= hi_c && c > pair_max) S.big[atomicAdd(&S.n_big, 1)] = static_cast<int16_t>(k);
+                }
+                __syncthreads();
+            }
+            // --- filter, big destinations: one staircase warp each
+            while (true) {
+                int b = 0;
+                if (lane == 0) b = atomicAdd(&S.next_big, 1);
+                b = __shfl_sync(kFull, b, 0);
+                if (b >= S.n_big) break;
+                const int k = S.big[b];
+                stair_filter<T>(S, stairs[warp], S.item_s[k], S.item_s[k + 1], lane);
+            }
+            // --- filter, small destinations: every candidate against the points before it
+            while (true) {
+                int c0 = 0;
+                if (lane == 0) c0 = atomicAdd(&S.next_chunk, 1) * 32;
+                c0 = __shfl_sync(kFull, c0, 0);
+                if (c0 >= total) break;
+                const int q = c0 + lane;
+                int js = q, len = 0;
+                if (q < total) {
+                    const int k = S.item_of[q];
+                    const int s0 = S.item_s[k], s1 = S.item_s[k + 1];
+                    if (s1 - s0 <= pair_max) {
+                        js = s0;
+                        len = q - s0;
+                    }
+                }
+                const bool mine = q < total && (S.item_s[S.item_of[q] + 1] - S.item_s[S.item_of[q]]) <= pair_max;
+                if (!__any_sync(kFull, mine)) continue;
+                T q1 = 0, q2 = 0;
+                if (mine) {
+                    q1 = S.mpts[q].v[1];
+                    q2 = S.mpts[q].v[2];
+                }
+                bool dom = !mine;
+                const int maxlen = warp_max_i(len);
+                for (int t = 0; t < maxlen; ++t) {
+                    if (t < len) {
+                        const PackedPt<3, T> c = S.mpts[js + t];
+                        dom |= (c.v[1] >= q1) & (c.v[2] >= q2);
+                    }
+                    if ((t & 7) == 7 && __all_sync(kFull, dom)) break;
+                }
+                if (mine) S.keep[q] = dom ? 0 : 1;
+            }
+            __syncthreads();
+            // --- exclusive scan of keep flags (merged order)
+            constexpr int QPER = kTileCap / kLT;
+            int32_t kept_local = 0;
+#pragma unroll
+            for (int r = 0; r < QPER; ++r) {
+                const int q = tid * QPER + r;
+                if (q < total) kept_local += S.keep[q];
+            }
+            const int32_t kex = block_exclusive_scan<int32_t, kLT>(kept_local, S.warp_i, &S.tot_i);
+            {
+                int32_t run = kex;
+#pragma unroll
+                for (int r = 0; r < QPER; ++r) {
+                    const int q = tid * QPER + r;
+                    if (q < total) {
+                        S.keep_ex[q] = static_cast<int16_t>(run);
+                        run += S.keep[q];
+                    }
+                }
+                if (tid == kLT - 1) S.keep_ex[total] = static_cast<int16_t>(run);
+            }
+            __syncthreads();
+            if (tid == 0 && J.tile_surv != nullptr && S.keep_ex[total] > 0)
+                atomicAdd(J.tile_surv, static_cast<unsigned long long>(S.keep_ex[total]));
+            // --- write survivors into each destination's slot, in merged order
+            for (int q = tid; q < total; q += kLT) {
+                if (!S.keep[q]) continue;
+                const int k = S.item_of[q];
+                const int64_t dst = S.item_c0[k] + (S.keep_ex[q] - S.keep_ex[S.item_s[k]]);
+                T *o_ = outp + dst * 3;
+                const PackedPt<3, T> me = S.mpts[q];
+#pragma unroll
+                for (int o = 0; o < 3; ++o) o_[o] = me.v[o];
+            }
+            for (int k = tid; k < n_it; k += kLT) {
+                const int js = S.item_s[k], je = S.item_s[k + 1];
+                if (je > js) J.out_size[ic + k] = S.keep_ex[je] - S.keep_ex[js];
+            }
+            __syncthreads();
+            ic += n_it;
+        }
+        __syncthreads();  // tile bookkeeping in shared memory is rewritten next iteration
+    }
+}
+
+namespace {
+
+template <typename T>
+cudaError_t launch_lex_t(const ExpandJob *jobs, const int64_t *tile_bases, int num_jobs, int64_t total_tiles, int grid,
+                         cudaStream_t stream) {
+    static_assert(sizeof(Stair<T>) * kLexWarps <= sizeof(PackedPt<3, T>) * kTileCap, "staircases fit over pts");
+    const size_t smem = sizeof(LexSmem<T>);
+    const cudaError_t e = ensure_smem_limit(reinterpret_cast<const void *>(expand_tile_lex_kernel<T>), smem);
+    if (e != cudaSuccess) return e;
+    if (total_tiles <= 0) return cudaSuccess;
+    const int64_t g = std::min<int64_t>(total_tiles, grid);
+    expand_tile_lex_kernel<T><<<static_cast<unsigned>(g), kLT, smem, stream>>>(jobs, tile_bases, num_jobs, total_tiles);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+size_t lex_tile_smem_bytes(bool wide) { return wide ? sizeof(LexSmem<int64_t>) : sizeof(LexSmem<int32_t>); }
+
+cudaError_t launch_expand_tiles_lex(bool wide, const ExpandJob *jobs, const int64_t *tile_bases, int num_jobs,
+                                    int64_t total_tiles, int grid, cudaStream_t stream) {
+    if (wide) return launch_lex_t<int64_t>(jobs, tile_bases, num_jobs, total_tiles, grid, stream);
+    return launch_lex_t<int32_t>(jobs, tile_bases, num_jobs, total_tiles, grid, stream);
+}
+
+}  // namespace dev
+}  // namespace pmdd

@@ -83,6 +83,17 @@ class Server:
     def pending(self) -> int:
         return self._lib.pmdd_server_pending(self._h)
 
+    def info(self) -> dict:
+        """Serving counters and memory figures (pmdd_server_info)."""
+        inf = _native.PmddServerInfo()
+        self._lib.pmdd_server_get_info(self._h, ctypes.byref(inf))
+        return {name: getattr(inf, name) for name, _ in inf._fields_}
+
+    def inject_alloc_failures(self, after: int, count: int) -> None:
+        """Test hook: after `after` more device allocations, the next `count` fail."""
+        if self._lib.pmdd_server_inject_alloc_failures(self._h, int(after), int(count)) != 0:
+            raise ValueError("after and count must be >= 0")
+
     def close(self):
         if self._h:
             self._lib.pmdd_server_destroy(self._h)
