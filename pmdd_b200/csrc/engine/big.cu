@@ -24,6 +24,7 @@
 // the batched knapsack / set-packing stream as on single 5-objective TSPs), so by default
 // it takes every destination above kSmallMax candidates; SFS blocks keep those that leave
 // the tiles for their arc count, and whatever a fixed or tuned crossover assigns them.
+#include "big_common.cuh"
 #include "kernels.cuh"
 #include "sfs.cuh"
 
@@ -33,6 +34,8 @@ namespace pmdd {
 namespace dev {
 
 namespace {
+
+using namespace big;
 
 constexpr int kFlatThreads = 256;
 constexpr int kMarkThreads = 256;
@@ -44,88 +47,6 @@ template <int D, typename T>
 struct MarkCfg {
     static constexpr int kTile = 32768 / static_cast<int>(sizeof(PackedPt<D, T>));  // points per shared tile
 };
-
-struct BigItem {
-    int32_t item;      // job-local destination
-    int32_t a0, a1;    // its arcs (global ids)
-    int64_t soff;      // scratch offset (candidates) within this pass's window
-    int64_t c0;        // job-local candidate start (the slot start)
-    int64_t n;         // candidates
-};
-
-__device__ __forceinline__ void fill_item(const ExpandJob &J, int64_t k, int64_t lo, BigItem *b) {
-    b->item = static_cast<int32_t>(J.big_list[2 * k]);
-    b->soff = J.big_list[2 * k + 1] - lo;
-    const int32_t v = J.item_base + b->item;
-    b->a0 = J.item_arc_off[v];
-    b->a1 = J.item_arc_off[v + 1];
-    b->c0 = J.arc_cand_off[b->a0 - J.arc_base];
-    b->n = J.arc_cand_off[b->a1 - J.arc_base] - b->c0;
-}
-
-// The destination of work item W, if pass `pass` takes it (its scratch offset lies in the
-// pass's window); its scratch offset is then re-based to the window.
-__device__ __forceinline__ bool big_item(const ExpandJob &J, const BigWork &W, int64_t pass, BigItem *b) {
-    const int64_t lo = pass * J.big_window;
-    const int64_t s = J.big_list[2 * W.big + 1];
-    if (s < lo || s >= lo + J.big_window) return false;
-    fill_item(J, W.big, lo, b);
-    return true;
-}
-
-__device__ __forceinline__ int find_job(const int64_t *bases, int n, int64_t g) {
-    int lo = 0, hi = n - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (bases[mid] <= g) lo = mid;
-        else hi = mid - 1;
-    }
-    return lo;
-}
-
-// Flat candidate g of a group's pass: its job, destination and position in it (false
-// if g falls past the pass's destinations or into another pass's).
-struct BigCand {
-    int job;
-    int64_t i;   // position within the destination
-    BigItem B;
-};
-
-__device__ __forceinline__ bool big_cand(const ExpandJob *jobs, const int64_t *job_bases, int num_jobs, int64_t g,
-                                         int64_t pass, BigCand *c) {
-    const int j = find_job(job_bases, num_jobs, g);
-    const ExpandJob &J = jobs[j];
-    const int64_t cl = g - job_bases[j];
-    if (J.num_big <= 0 || cl >= J.big_rows) return false;
-    const int64_t lo = pass * J.big_window;
-    const int64_t s = lo + cl;  // index in the job's whole oversized candidate order
-    int a = 0, b = J.num_big - 1;
-    while (a < b) {
-        const int mid = (a + b + 1) >> 1;
-        if (J.big_list[2 * mid + 1] <= s) a = mid;
-        else b = mid - 1;
-    }
-    const int64_t soff = J.big_list[2 * a + 1];
-    if (soff > s || soff < lo || soff >= lo + J.big_window) return false;
-    fill_item(J, a, lo, &c->B);
-    c->i = s - soff;
-    if (c->i >= c->B.n) return false;
-    c->job = j;
-    return true;
-}
-
-// Arc run [rs, re) (destination-local) of position i, and its arc.
-__device__ __forceinline__ int32_t run_of(const ExpandJob &J, const BigItem &B, int64_t i, int64_t *rs, int64_t *re) {
-    int lo = B.a0, hi = B.a1 - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (J.arc_cand_off[mid - J.arc_base] - B.c0 <= i) lo = mid;
-        else hi = mid - 1;
-    }
-    *rs = J.arc_cand_off[lo - J.arc_base] - B.c0;
-    *re = J.arc_cand_off[lo + 1 - J.arc_base] - B.c0;
-    return lo;
-}
 
 // The destinations that take the mark path in one pass.  Destination h is work item
 // work_idx[h]; its candidates form chunks [chunk_base[h], chunk_base[h + 1]) of 256, its
@@ -625,9 +546,15 @@ static cudaError_t launch_big_t(const BigLaunch &L, cudaStream_t stream) {
         const cudaError_t e = ensure_smem_limit(reinterpret_cast<const void *>(big_sfs_kernel<D, T>), Cfg::kSmem);
         if (e != cudaSuccess) return e;
     }
-    const int64_t want = (L.total + kFlatThreads - 1) / kFlatThreads;
-    const unsigned grid = static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>(want, int64_t(L.sms) * 32)));
-    big_expand_kernel<D, T><<<grid, kFlatThreads, 0, stream>>>(L.jobs, L.job_bases, L.num_jobs, L.total, L.pass);
+    const bool lex = D == 3 && L.lex_big;
+    if (lex) {
+        const cudaError_t e = launch_big_lex_rank(sizeof(T) == 8, L, stream);
+        if (e != cudaSuccess) return e;
+    } else {
+        const int64_t want = (L.total + kFlatThreads - 1) / kFlatThreads;
+        const unsigned grid = static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>(want, int64_t(L.sms) * 32)));
+        big_expand_kernel<D, T><<<grid, kFlatThreads, 0, stream>>>(L.jobs, L.job_bases, L.num_jobs, L.total, L.pass);
+    }
     if (L.with_sfs) {
         const int32_t *order = nullptr;
         if (L.order && L.num_work <= kBigOrderMax) {
@@ -648,6 +575,7 @@ static cudaError_t launch_big_t(const BigLaunch &L, cudaStream_t stream) {
         big_mark_kernel<D, T><<<chunks, kMarkThreads, 0, stream>>>(L.jobs, L.work, L.pass, plan, L.mark_cap);
         big_write_kernel<D, T><<<L.mark_cap, kWriteThreads, 0, stream>>>(L.jobs, L.work, L.pass, plan, L.mark_cap);
     }
+    if (lex) return launch_big_lex_filter(sizeof(T) == 8, L, stream);
     return cudaGetLastError();
 }
 

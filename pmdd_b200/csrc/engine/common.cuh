@@ -104,7 +104,7 @@ struct ExpandJob {
     uint8_t *out_sorted;
     int32_t pair_max;              // lexicographic tiles: destinations of at most this many
                                    // candidates are checked pairwise, larger ones by a staircase warp
-    int32_t pad1;
+    int32_t lex_big;               // 1: oversized destinations with sorted runs take big_lex.cu
 };
 
 // Bytes of oversized-destination scratch per candidate point.

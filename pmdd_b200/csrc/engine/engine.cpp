@@ -1111,6 +1111,7 @@ int Engine::step() {
                 J.prev_sorted = s.sorted;
                 J.out_sorted = e.out_sorted;
                 J.pair_max = lex_pair_max_;
+                J.lex_big = (I.d == 3 && lex_tiles_) ? 1 : 0;
                 J.tile_base = gl.tiles;
                 tile_bases[pos] = gl.tiles;
                 item_bases[pos] = gl.items;
@@ -1520,6 +1521,7 @@ int Engine::step() {
         L.total = gl.big_rows;
         L.sms = sms_;
         L.with_sfs = true;
+        L.lex_big = gl.d == 3 && lex_tiles_;
         L.mark_cap = static_cast<int>(std::min<int64_t>(gl.mark_cap, static_cast<int64_t>(gl.big_count)));
         L.plan = nullptr;
         // more SFS blocks than fit the SMs at once: start the largest destinations first
@@ -1529,7 +1531,7 @@ int Engine::step() {
         for (int64_t pass = 0; pass < gl.big_passes; ++pass) {
             L.pass = pass;
             if (!cuda_ok(dev::launch_big(gl.d, gl.wide, L, stream_), "oversized-destination kernels")) return -1;
-            launches_ += (L.mark_cap > 0 ? 9 : 2) + (ordered ? 1 : 0);
+            launches_ += (L.mark_cap > 0 ? 9 : 2) + (ordered ? 1 : 0) + (L.lex_big ? 1 : 0);
         }
     }
     if (!sdjobs.empty()) {

@@ -33,11 +33,16 @@ struct BigLaunch {
     void *plan;                  // big_plan_bytes(mark_cap) of scratch for the mark path
     int mark_cap;                // upper bound on mark-path destinations in the pass; 0: none
     int32_t *order;              // num_work ints: SFS blocks largest destination first; nullptr: list order
+    bool lex_big;                // three objectives: destinations with sorted runs take big_lex.cu
 };
 // Most oversized destinations whose SFS blocks are put in size order (one block sorts them).
 constexpr int kBigOrderMax = 4096;
 size_t big_plan_bytes(int cap);
 cudaError_t launch_big(int d, bool wide, const BigLaunch &L, cudaStream_t stream);
+// The lexicographic oversized path (big_lex.cu), three objectives: the rank kernel takes
+// the place of the materialising expansion, the filter runs after the other paths.
+cudaError_t launch_big_lex_rank(bool wide, const BigLaunch &L, cudaStream_t stream);
+cudaError_t launch_big_lex_filter(bool wide, const BigLaunch &L, cudaStream_t stream);
 
 }  // namespace dev
 }  // namespace pmdd

@@ -37,6 +37,7 @@
 // merge by counting.
 #include "kernels.cuh"
 #include "scan.cuh"
+#include "stair.cuh"
 
 #include <algorithm>
 
@@ -73,13 +74,9 @@ struct LexSmem {
     int32_t n_big, next_big, next_chunk;
 };
 
-// Per-warp staircase storage, laid over pts once the merge has read it: two buffers
-// (current, next) of objective-1 and objective-2 values.
+// Per-warp staircase storage, laid over pts once the merge has read it.
 template <typename T>
-struct Stair {
-    T v1[2][kStairCap];
-    T v2[2][kStairCap];
-};
+using Stair = StairBuf<T, kStairCap>;
 
 template <typename T>
 __device__ __forceinline__ bool lex_gt(const PackedPt<3, T> &a, const PackedPt<3, T> &b) {
@@ -95,11 +92,8 @@ __device__ __forceinline__ bool lex_eq(const PackedPt<3, T> &a, const PackedPt<3
 
 // Candidates of one big destination, merged positions [s, e), walked by one warp.
 template <typename T>
-__device__ void stair_filter(LexSmem<T> &S, Stair<T> &st, int s, int e, int lane) {
-    int cur = 0;        // staircase buffer in use
-    int m = 0;          // staircase entries (warp-uniform), objective 1 descending
-    bool overflow = false;
-    const unsigned lt_mask = (1u << lane) - 1u;
+__device__ void stair_filter(LexSmem<T> &S, Stair<T> &sb, int s, int e, int lane) {
+    StairState st;
     for (int c0 = s; c0 < e; c0 += 32) {
         const int p = c0 + lane;
         const bool valid = p < e;
@@ -109,7 +103,7 @@ __device__ void stair_filter(LexSmem<T> &S, Stair<T> &st, int s, int e, int lane
             q2 = S.mpts[p].v[2];
         }
         bool dom = !valid;
-        if (overflow) {
+        if (st.overflow) {
             // staircase given up: every point before p, chunk-mates included
             const int hi = min(e, c0 + 32) - 1;
             for (int j = s; j < hi; ++j) {
@@ -117,95 +111,10 @@ __device__ void stair_filter(LexSmem<T> &S, Stair<T> &st, int s, int e, int lane
                 if (j < p) dom |= (c.v[1] >= q1) & (c.v[2] >= q2);
                 if (((j - s) & 15) == 15 && __all_sync(kFull, dom)) break;
             }
-            if (valid) S.keep[p] = dom ? 0 : 1;
-            continue;
-        }
-        // staircase lookup: cnt = entries with objective 1 >= q1; the last of them holds
-        // the largest objective 2 among them
-        int cnt = 0;
-        if (valid && m > 0) {
-            int a = 0, b = m;
-            while (a < b) {
-                const int mid = (a + b) >> 1;
-                if (st.v1[cur][mid] >= q1) a = mid + 1;
-                else b = mid;
-            }
-            cnt = a;
-            dom = cnt > 0 && st.v2[cur][cnt - 1] >= q2;
-        }
-        // the chunk's surviving candidates against each other: an earlier one dominates;
-        // a later one that is larger in both (and not equal) removes it from the staircase
-        const unsigned alive = __ballot_sync(kFull, !dom);
-        bool rem = false;
-        unsigned mm = alive;
-        while (mm) {
-            const int j = __ffs(mm) - 1;
-            mm &= mm - 1;
-            const T a1 = __shfl_sync(kFull, q1, j), a2 = __shfl_sync(kFull, q2, j);
-            const bool ge = (a1 >= q1) & (a2 >= q2);
-            dom |= ge & (j < lane);
-            rem |= ge & (j > lane) & ((a1 != q1) | (a2 != q2));
+        } else {
+            dom = stair_chunk<T, kStairCap>(sb, st, valid, q1, q2, c0 + 32 < e);
         }
         if (valid) S.keep[p] = dom ? 0 : 1;
-        if (c0 + 32 >= e) break;
-        // next staircase: surviving entries and the chunk's new maxima, objective 1 descending
-        const bool fresh = !dom && !rem;
-        const unsigned nmask = __ballot_sync(kFull, fresh);
-        T eA1 = 0, eA2 = 0, eB1 = 0, eB2 = 0;
-        const bool hasA = lane < m, hasB = lane + 32 < m;
-        if (hasA) {
-            eA1 = st.v1[cur][lane];
-            eA2 = st.v2[cur][lane];
-        }
-        if (hasB) {
-            eB1 = st.v1[cur][lane + 32];
-            eB2 = st.v2[cur][lane + 32];
-        }
-        bool killA = false, killB = false;
-        int gtA = 0, gtB = 0, gtq = 0;
-        unsigned nn = nmask;
-        while (nn) {
-            const int j = __ffs(nn) - 1;
-            nn &= nn - 1;
-            const T n1 = __shfl_sync(kFull, q1, j), n2 = __shfl_sync(kFull, q2, j);
-            killA |= hasA & (n1 >= eA1) & (n2 >= eA2);
-            killB |= hasB & (n1 >= eB1) & (n2 >= eB2);
-            gtA += (n1 > eA1) ? 1 : 0;
-            gtB += (n1 > eB1) ? 1 : 0;
-            gtq += (n1 > q1) ? 1 : 0;
-        }
-        const unsigned survA = __ballot_sync(kFull, hasA && !killA);
-        const unsigned survB = __ballot_sync(kFull, hasB && !killB);
-        const int nsA = __popc(survA);
-        const int m_next = nsA + __popc(survB) + __popc(nmask);
-        if (m_next > kStairCap) {
-            overflow = true;
-            continue;
-        }
-        const int nxt = cur ^ 1;
-        if (hasA && !killA) {
-            const int pos = __popc(survA & lt_mask) + gtA;
-            st.v1[nxt][pos] = eA1;
-            st.v2[nxt][pos] = eA2;
-        }
-        if (hasB && !killB) {
-            const int pos = nsA + __popc(survB & lt_mask) + gtB;
-            st.v1[nxt][pos] = eB1;
-            st.v2[nxt][pos] = eB2;
-        }
-        if (fresh) {
-            // surviving entries before q: those among the first cnt (objective 1 >= q1);
-            // an entry with objective 1 == q1 is dominated by q and did not survive
-            const int ca = min(cnt, 32), cb = max(cnt - 32, 0);
-            const unsigned ma = ca >= 32 ? kFull : ((1u << ca) - 1u);
-            const unsigned mb = cb >= 32 ? kFull : ((1u << cb) - 1u);
-            const int pos = __popc(survA & ma) + __popc(survB & mb) + gtq;
-            st.v1[nxt][pos] = q1;
-            st.v2[nxt][pos] = q2;
-        }
-        __syncwarp();
-        cur = nxt;
-        m = m_next;
     }
 }
 
