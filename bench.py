@@ -319,6 +319,39 @@ def config1_filter(P, dds, device, peak, flush=None):
             "device_s": st1["device_elapsed_s"]}
 
 
+SINGLE_CASES = {
+    "kp3_n40": (1, 3, lambda I: I.knapsack_text(40, 3, 0)),
+    "kp4_n60": (1, 4, lambda I: I.knapsack_text(60, 4, 0)),
+    "kp7_n25": (1, 7, lambda I: I.knapsack_text(25, 7, 0)),
+    "sp3_n100_m20": (2, 3, lambda I: I.setpacking_text(100, 20, 3, 0)),
+}
+
+
+def instance_only(args):
+    """`--instance NAME --method M`: one single-instance configuration (seed 0) through
+    pmdd_enumerate, `--warmup` untimed runs then `--steps` timed ones; one JSON line with
+    the device time and work counters of each timed run.  The command the committed
+    single-instance profiles run under ncu."""
+    import torch
+
+    import pmdd_b200 as P
+    from pmdd_b200 import instances
+
+    torch.cuda.set_device(0)
+    ptype, d, make = SINGLE_CASES[args.instance]
+    dd = P.DecisionDiagram.from_text(make(instances), ptype, d)
+    for _ in range(args.warmup):
+        P.enumerate_dd(dd, method=args.method)
+    runs = []
+    for _ in range(max(1, args.steps)):
+        st = {}
+        pts = P.enumerate_dd(dd, method=args.method, stats=st)
+        runs.append({"device_s": st["device_elapsed_s"], "solutions": int(len(pts)),
+                     "candidates": int(st["work_candidates_total"]), "join_products": int(st["work_join_products_total"]),
+                     "launches": int(st["gpu_launches"])})
+    print(json.dumps({"instance": args.instance, "method": args.method, "runs": runs}))
+
+
 def config1_only(args):
     """`--config1 N`: the config-1 filter leg alone (N x KP d=3 n=40, seeds 0..N-1,
     method 1), `--warmup` untimed resident enumerations then `--steps` timed ones; one
@@ -357,9 +390,16 @@ def main():
     ap.add_argument("--config1", type=int, default=0,
                     help="only the config-1 filter leg on this many KP d=3 n=40 instances (profiling aid; "
                          "prints its own JSON line, not a bench line)")
+    ap.add_argument("--instance", default="",
+                    help="only one single-instance configuration (kp3_n40, kp4_n60, kp7_n25, sp3_n100_m20) by "
+                         "--method, `--warmup` untimed then `--steps` timed runs (profiling aid; own JSON line)")
+    ap.add_argument("--method", type=int, default=1)
     args = ap.parse_args()
     if args.config1 > 0:
         config1_only(args)
+        return
+    if args.instance:
+        instance_only(args)
         return
 
     rank = int(os.environ.get("RANK", "0"))
