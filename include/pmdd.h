@@ -139,6 +139,9 @@ typedef struct pmdd_stats {
     int64_t work_tile_candidates_total;  /* candidates filtered in shared-memory tiles */
     int64_t work_tile_survivors_total;   /* survivors the tile kernel wrote */
     int64_t tile_launches;               /* expand+filter tile kernels this call launched */
+    int64_t work_stair_candidates_total; /* three objectives: candidates of destinations filtered by a
+                                            staircase warp (tiles above the pairwise limit, and
+                                            oversized destinations with sorted runs) */
 } pmdd_stats;
 
 /* ------------------------------------------------------------ one-shot entry
@@ -318,6 +321,12 @@ int64_t pmdd_launch_count(void);
  * engines read at start-up (PMDD_TUNING_FILE, else the per-user cache written by
  * pmdd_b200.autotune).  No counterpart in the reference, which has one filter path. */
 int64_t pmdd_tuned_mark_min(const char *path, int32_t nobjs, int32_t problem_type);
+/* The three-objective crossover between the pairwise check and the staircase warp
+ * (destinations of at most this many candidates are checked pairwise) that the tuning
+ * file holds for (nobjs, problem_type), or -1 if none (engines then use 48).  Same file
+ * rules as pmdd_tuned_mark_min.  No counterpart in the reference, whose filter is
+ * pairwise at every size (src/pmdd/enum/gpu/topdown.cu:163-240). */
+int64_t pmdd_tuned_lex_pair_max(const char *path, int32_t nobjs, int32_t problem_type);
 
 #ifdef __cplusplus
 }

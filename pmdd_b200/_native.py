@@ -104,6 +104,7 @@ class PmddStats(ctypes.Structure):
         ("work_tile_candidates_total", c_i64),
         ("work_tile_survivors_total", c_i64),
         ("tile_launches", c_i64),
+        ("work_stair_candidates_total", c_i64),
     ]
 
     def as_dict(self) -> dict:
@@ -227,6 +228,7 @@ GPU_SYMBOLS = {
     "pmdd_version": (ctypes.c_char_p, []),
     "pmdd_launch_count": (c_i64, []),
     "pmdd_tuned_mark_min": (c_i64, [ctypes.c_char_p, c_i32, c_i32]),
+    "pmdd_tuned_lex_pair_max": (c_i64, [ctypes.c_char_p, c_i32, c_i32]),
 }
 
 _host = None

@@ -1,4 +1,4 @@
-"""Autotuner for the oversized-destination crossover, cached per (objectives, problem type).
+"""Autotuner for the filter crossovers, cached per (objectives, problem type).
 
 Destinations too large for a shared-memory tile are filtered one of two ways: one
 sort-filter-skyline block each (one SM per destination) or the GPU-wide pass that drops
@@ -15,6 +15,12 @@ choice to the tuning file the engine reads at start-up:
 
 A family for which the built-in behaviour is as fast as the best size gets an entry
 without "big_mark_min" ({"builtin": true, ...}), which the engine reads as untuned.
+
+Three-objective families also get "lex_pair_max": in the lexicographic tiles,
+destinations of at most that many candidates are checked pairwise against the points
+before them and larger ones by a staircase warp.  It is timed over PAIR_MAX_SIZES with the
+chosen oversized crossover in place (PMDD_LEX_PAIR_MAX in a fresh process); sizes within
+2 % of the fastest tie and the default (48) wins a tie, else the smallest.
 
     python -m pmdd_b200.autotune --nobjs 3 5 --ptype 1 3 [--out PATH]
 
@@ -34,6 +40,8 @@ from . import instances
 
 CANDIDATE_SIZES = (1025, 4096, 16384, 65536, 1 << 40)
 DEFAULT_MARK_MIN = 1025
+PAIR_MAX_SIZES = (0, 16, 32, 48, 96, 256, 1024)
+DEFAULT_PAIR_MAX = 48
 
 
 def tuning_path() -> str:
@@ -71,10 +79,11 @@ print(json.dumps({{"seconds": best}}))
 
 
 def time_in_child(path: str, nobjs: int, problem_type: int, method: int, mark_min: Optional[int],
-                  repeats: int = 3, timeout: float = 600.0) -> Optional[float]:
+                  repeats: int = 3, timeout: float = 600.0, pair_max: Optional[int] = None) -> Optional[float]:
     """Best device time of `repeats` enumerations in a fresh process with the given
-    crossover (None: the engine's built-in behaviour, no tuning file); None if the run
-    fails or times out."""
+    oversized crossover (None: the engine's built-in behaviour, no tuning file) and
+    three-objective pairwise limit (None: the built-in 48); None if the run fails or times
+    out."""
     root = os.path.abspath(os.path.join(os.path.dirname(__file__), ".."))
     code = _CHILD.format(root=root, path=path, ptype=problem_type, nobjs=nobjs, method=method, repeats=repeats)
     env = dict(os.environ, PMDD_TUNING_FILE=path + ".no-tuning.json")
@@ -82,6 +91,10 @@ def time_in_child(path: str, nobjs: int, problem_type: int, method: int, mark_mi
         env.pop("PMDD_BIG_MARK_MIN", None)
     else:
         env["PMDD_BIG_MARK_MIN"] = str(int(mark_min))
+    if pair_max is None:
+        env.pop("PMDD_LEX_PAIR_MAX", None)
+    else:
+        env["PMDD_LEX_PAIR_MAX"] = str(int(pair_max))
     try:
         p = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=timeout)
     except subprocess.TimeoutExpired:
@@ -110,6 +123,17 @@ def choose(times: Dict[int, Optional[float]], builtin: Optional[float] = None) -
     return DEFAULT_MARK_MIN if DEFAULT_MARK_MIN in tied else max(tied)
 
 
+def choose_pair_max(times: Dict[int, Optional[float]]) -> int:
+    """Fastest pairwise limit; sizes within 2 % of the fastest tie, the default wins a
+    tie, else the smallest; no usable timing -> the default."""
+    ok = {k: v for k, v in times.items() if v is not None}
+    if not ok:
+        return DEFAULT_PAIR_MAX
+    best = min(ok.values())
+    tied = [k for k, v in ok.items() if v <= best * 1.02]
+    return DEFAULT_PAIR_MAX if DEFAULT_PAIR_MAX in tied else min(tied)
+
+
 def tune(families: Iterable[tuple], sizes: Sequence[int] = CANDIDATE_SIZES, method: int = 1,
          timer: Optional[Callable[..., Optional[float]]] = None, workdir: Optional[str] = None) -> Dict[str, dict]:
     """Tunes every (nobjs, problem_type) of `families`; returns the entries to store."""
@@ -129,6 +153,10 @@ def tune(families: Iterable[tuple], sizes: Sequence[int] = CANDIDATE_SIZES, meth
         seconds["builtin"] = builtin
         pick = choose(times, builtin)
         entry = {"builtin": True} if pick is None else {"big_mark_min": pick}
+        if nobjs == 3:
+            pt = {int(k): timer(path, nobjs, ptype, method, pick, pair_max=int(k)) for k in PAIR_MAX_SIZES}
+            entry["lex_pair_max"] = choose_pair_max(pt)
+            entry["pair_max_seconds"] = {str(k): v for k, v in pt.items()}
         entry.update({"seconds": seconds, "instance": desc})
         out[f"d{nobjs}_p{ptype}"] = entry
     return out
@@ -163,7 +191,7 @@ def main(argv=None):
     entries = tune([(d, p) for d in args.nobjs for p in args.ptype])
     path = write(entries, args.out)
     for k, v in entries.items():
-        print(k, v.get("big_mark_min", "built-in"), v["seconds"])
+        print(k, v.get("big_mark_min", "built-in"), v.get("lex_pair_max", "-"), v["seconds"])
     print("written", path)
 
 

@@ -161,6 +161,7 @@ __global__ void __launch_bounds__(FilterCfg<T>::kThreads) big_lex_filter_kernel(
         if (lane == 0) {
             J.out_size[B.item] = static_cast<int32_t>(kept);
             if (J.out_sorted) J.out_sorted[B.item] = 1;
+            if (J.tile_surv) atomicAdd(J.tile_surv + 1, static_cast<unsigned long long>(B.n));
         }
     }
 }

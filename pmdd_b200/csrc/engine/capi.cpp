@@ -303,6 +303,7 @@ int collect_batch(std::vector<std::unique_ptr<pmdd::Instance>> &reqs, pmdd_front
             stats->dominance_filtered_total += st.dominance_filtered_total;
             stats->work_tile_candidates_total += st.work_tile_candidates_total;
             stats->work_tile_survivors_total += st.work_tile_survivors_total;
+            stats->work_stair_candidates_total += st.work_stair_candidates_total;
             stats->gpu_mem_peak_used_bytes = std::max(stats->gpu_mem_peak_used_bytes, st.gpu_mem_peak_used_bytes);
             stats->gpu_mem_peak_reserved_bytes = st.gpu_mem_peak_reserved_bytes;
         }
@@ -1021,9 +1022,15 @@ const char *pmdd_version(void) { return "pmdd_b200 0.1 (sm_100a)"; }
 int64_t pmdd_launch_count(void) { return pmdd::g_total_launches.load(); }
 
 int64_t pmdd_tuned_mark_min(const char *path, int32_t nobjs, int32_t problem_type) {
-    const auto table = pmdd::read_tuning(path ? std::string(path) : pmdd::default_tuning_path());
+    const auto table = pmdd::read_tuning(path ? std::string(path) : pmdd::default_tuning_path(), "big_mark_min");
     auto it = table.find({nobjs, problem_type});
     return it != table.end() ? it->second : 0;
+}
+
+int64_t pmdd_tuned_lex_pair_max(const char *path, int32_t nobjs, int32_t problem_type) {
+    const auto table = pmdd::read_tuning(path ? std::string(path) : pmdd::default_tuning_path(), "lex_pair_max");
+    auto it = table.find({nobjs, problem_type});
+    return it != table.end() ? it->second : -1;
 }
 
 }  // extern "C"

@@ -95,7 +95,8 @@ struct ExpandJob {
                                    // [p * big_window, (p + 1) * big_window) (--max-cand)
     int64_t big_rows;              // scratch rows (candidates) one pass can use
     uint32_t *err;
-    unsigned long long *tile_surv; // survivors written by the tile kernel (added to)
+    unsigned long long *tile_surv; // [0]: survivors written by the tile kernel, [1]: candidates of
+                                   // destinations filtered by staircase warps (both added to)
     // Lexicographic order (three objectives): a node whose flag is 1 holds its frontier in
     // descending lexicographic order.  prev_sorted is indexed like prev_size; the tile
     // kernels write out_sorted for every destination they stage (1 only when they wrote

@@ -577,7 +577,7 @@ Engine::Engine(int device, int64_t budget_bytes, int max_slots) : device_(device
     const char *lx = std::getenv("PMDD_LEX_TILES");
     if (lx && lx[0] == '0') lex_tiles_ = false;
     const char *pm = std::getenv("PMDD_LEX_PAIR_MAX");
-    if (pm && *pm && std::atoi(pm) >= 0) lex_pair_max_ = std::atoi(pm);
+    if (pm && *pm && std::atoi(pm) >= 0) lex_pair_max_fixed_ = std::atoi(pm);
     ok_ = true;
 }
 
@@ -608,7 +608,7 @@ std::string default_tuning_path() {
     return std::string();
 }
 
-std::map<std::pair<int, int>, int64_t> read_tuning(const std::string &path) {
+std::map<std::pair<int, int>, int64_t> read_tuning(const std::string &path, const char *key) {
     std::map<std::pair<int, int>, int64_t> out;
     if (path.empty()) return out;
     FILE *f = std::fopen(path.c_str(), "rb");
@@ -618,31 +618,51 @@ std::map<std::pair<int, int>, int64_t> read_tuning(const std::string &path) {
     size_t got;
     while ((got = std::fread(buf, 1, sizeof(buf), f)) > 0 && text.size() < (1u << 20)) text.append(buf, got);
     std::fclose(f);
+    const std::string quoted = std::string("\"") + key + "\"";
+    // entry keys "d<objectives>_p<problem type>"; an entry runs to the next entry key
+    std::vector<std::pair<size_t, std::pair<int, int>>> entries;
     size_t pos = 0;
     while ((pos = text.find("\"d", pos)) != std::string::npos) {
         int d = 0, p = 0, used = 0;
-        if (std::sscanf(text.c_str() + pos, "\"d%d_p%d\"%n", &d, &p, &used) != 2 || used == 0) {
+        if (std::sscanf(text.c_str() + pos, "\"d%d_p%d\"%n", &d, &p, &used) == 2 && used > 0) {
+            entries.push_back({pos, {d, p}});
+            pos += used;
+        } else {
             ++pos;
-            continue;
         }
-        const size_t end = text.find('}', pos);
-        const size_t key = text.find("\"big_mark_min\"", pos);
-        if (key != std::string::npos && key < end) {
-            long long v = 0;
-            if (std::sscanf(text.c_str() + key + 14, " : %lld", &v) == 1 && v > 0 && d >= 1 && d <= 8)
-                out[{d, p}] = v;
-        }
-        pos += used;
+    }
+    for (size_t i = 0; i < entries.size(); ++i) {
+        const size_t begin = entries[i].first;
+        const size_t end = i + 1 < entries.size() ? entries[i + 1].first : text.size();
+        const size_t k = text.find(quoted, begin);
+        if (k == std::string::npos || k >= end) continue;
+        long long v = 0;
+        const int d = entries[i].second.first;
+        if (std::sscanf(text.c_str() + k + quoted.size(), " : %lld", &v) == 1 && v >= 0 && d >= 1 && d <= 8)
+            out[entries[i].second] = v;
     }
     return out;
 }
 
-void Engine::load_tuning() { tuned_mark_min_ = read_tuning(default_tuning_path()); }
+void Engine::load_tuning() {
+    const std::string path = default_tuning_path();
+    tuned_mark_min_ = read_tuning(path, "big_mark_min");
+    for (auto it = tuned_mark_min_.begin(); it != tuned_mark_min_.end();)  // 0 is not a crossover
+        it = it->second > 0 ? std::next(it) : tuned_mark_min_.erase(it);
+    tuned_pair_max_ = read_tuning(path, "lex_pair_max");
+}
 
 int64_t Engine::mark_min_for(int d, int problem_type) const {
     if (big_mark_min_fixed_ > 0) return big_mark_min_fixed_;
     auto it = tuned_mark_min_.find({d, problem_type});
     return it != tuned_mark_min_.end() ? it->second : static_cast<int64_t>(dev::kSmallMax) + 1;
+}
+
+int32_t Engine::pair_max_for(int d, int problem_type) const {
+    if (lex_pair_max_fixed_ >= 0) return lex_pair_max_fixed_;
+    auto it = tuned_pair_max_.find({d, problem_type});
+    return it != tuned_pair_max_.end() ? static_cast<int32_t>(std::min<int64_t>(it->second, dev::kSmallMax))
+                                       : kDefaultPairMax;
 }
 
 void *Engine::scratch(size_t bytes) {
@@ -1110,7 +1130,7 @@ int Engine::step() {
                 J.tile_first = e.out_size + J.num_items;
                 J.prev_sorted = s.sorted;
                 J.out_sorted = e.out_sorted;
-                J.pair_max = lex_pair_max_;
+                J.pair_max = pair_max_for(I.d, I.opts.problem_type);
                 J.lex_big = (I.d == 3 && lex_tiles_) ? 1 : 0;
                 J.tile_base = gl.tiles;
                 tile_bases[pos] = gl.tiles;
@@ -1229,7 +1249,7 @@ int Engine::step() {
     // labels removed by state dominance per job | error word.  All but the count
     // results start at zero (one memset).
     const size_t f_ts = sizeof(dev::CountResult) * counts.size();
-    const size_t f_sd = f_ts + sizeof(unsigned long long) * exps.size();
+    const size_t f_sd = f_ts + 2 * sizeof(unsigned long long) * exps.size();  // (survivors, staircase) per expansion
     const size_t f_err = f_sd + sizeof(int64_t) * sdjobs.size();
     const size_t f_total = f_err + sizeof(uint64_t);
     char *d_fixed = static_cast<char *>(scratch(f_total));
@@ -1238,7 +1258,7 @@ int Engine::step() {
     int64_t *d_removed = d_fixed ? reinterpret_cast<int64_t *>(d_fixed + f_sd) : nullptr;
     uint32_t *d_err_step = d_fixed ? reinterpret_cast<uint32_t *>(d_fixed + f_err) : nullptr;
     for (size_t k = 0; k < xjobs.size(); ++k) {
-        xjobs[k].tile_surv = d_tile_surv ? d_tile_surv + k : nullptr;
+        xjobs[k].tile_surv = d_tile_surv ? d_tile_surv + 2 * k : nullptr;
         xjobs[k].err = d_err_step;
     }
     for (size_t k = 0; k < sdjobs.size(); ++k) sdjobs[k].removed = d_removed ? d_removed + k : nullptr;
@@ -1617,7 +1637,7 @@ int Engine::step() {
         }
         unsigned long long tile_surv = 0;
         for (size_t k = 0; k < exps.size(); ++k)
-            tile_surv += reinterpret_cast<const unsigned long long *>(static_cast<char *>(h_summary_.p) + s_ts)[k];
+            tile_surv += reinterpret_cast<const unsigned long long *>(static_cast<char *>(h_summary_.p) + s_ts)[2 * k];
         std::fprintf(stderr,
                      "[pmdd step] jobs=%zu counts=%zu couple=%zu cand=%lld big_items=%lld big_cand=%lld max_item=%lld "
                      "tile_cand=%lld tile_surv=%llu tiles_ms=%.3f big_ms=%.3f rest_ms=%.3f host_to_sync_us=%.1f "
@@ -1643,7 +1663,9 @@ int Engine::step() {
         e.I->stats.kernel_total_s += (ms_expand + ms_big + ms_rest) * 1e-3;
         e.I->stats.work_tile_candidates_total += e.cand - e.big_total;
         e.I->stats.work_tile_survivors_total +=
-            static_cast<int64_t>(reinterpret_cast<const unsigned long long *>(hsum + s_ts)[k]);
+            static_cast<int64_t>(reinterpret_cast<const unsigned long long *>(hsum + s_ts)[2 * k]);
+        e.I->stats.work_stair_candidates_total +=
+            static_cast<int64_t>(reinterpret_cast<const unsigned long long *>(hsum + s_ts)[2 * k + 1]);
     }
     for (size_t k = 0; k < sdjobs.size(); ++k)
         sd_inst[k]->stats.dominance_filtered_total += reinterpret_cast<const int64_t *>(hsum + s_sd)[k];

@@ -186,7 +186,7 @@ void prepare_tsp_instance(const TspStructure &S, int nobjs, const int32_t *cost,
 // Tuned oversized-path crossovers, (objectives, problem type) -> big_mark_min, from the
 // tuning file pmdd_b200.autotune writes (see Engine::mark_min_for); empty when absent.
 std::string default_tuning_path();
-std::map<std::pair<int, int>, int64_t> read_tuning(const std::string &path);
+std::map<std::pair<int, int>, int64_t> read_tuning(const std::string &path, const char *key = "big_mark_min");
 
 // Runs fn(i) for i in [0, n) on up to `threads` host threads (PMDD_HOST_THREADS caps
 // the default, which is the hardware concurrency, at most 32).
@@ -317,10 +317,15 @@ class Engine {
     // destinations that leave the tiles for their arc count).
     int64_t mark_min_for(int d, int problem_type) const;
     void load_tuning();
-    // Three-objective tiles in lexicographic order (tile_lex.cu): on unless PMDD_LEX_TILES=0;
-    // destinations of at most lex_pair_max_ candidates are checked pairwise (PMDD_LEX_PAIR_MAX).
+    // Three-objective tiles in lexicographic order (tile_lex.cu): on unless PMDD_LEX_TILES=0.
+    // Destinations of at most pair_max_for(d, problem type) candidates are checked
+    // pairwise, larger ones by a staircase warp: PMDD_LEX_PAIR_MAX if set, else the tuned
+    // value ("lex_pair_max" in the tuning file), else kDefaultPairMax.
+    static constexpr int32_t kDefaultPairMax = 48;
     bool lex_tiles_ = true;
-    int32_t lex_pair_max_ = 48;
+    int32_t lex_pair_max_fixed_ = -1;
+    std::map<std::pair<int, int>, int64_t> tuned_pair_max_;
+    int32_t pair_max_for(int d, int problem_type) const;
     int64_t big_mark_min_fixed_ = 0;
     std::map<std::pair<int, int>, int64_t> tuned_mark_min_;
     // Footprint model: largest layer's candidates per DD arc, learned per (problem type,

@@ -322,6 +322,8 @@ __global__ void __launch_bounds__(kLT) expand_tile_lex_kernel(const ExpandJob *_
                 b = __shfl_sync(kFull, b, 0);
                 if (b >= S.n_big) break;
                 const int k = S.big[b];
+                if (lane == 0 && J.tile_surv != nullptr)
+                    atomicAdd(J.tile_surv + 1, static_cast<unsigned long long>(S.item_s[k + 1] - S.item_s[k]));
                 stair_filter<T>(S, stairs[warp], S.item_s[k], S.item_s[k + 1], lane);
             }
             // --- filter, small destinations: every candidate against the points before it

@@ -21,9 +21,12 @@ def test_choose_picks_fastest_and_breaks_ties_upward():
 def test_tune_with_a_fake_timer(tmp_path):
     calls = []
 
-    def timer(path, nobjs, ptype, method, mark_min):
-        calls.append((nobjs, ptype, mark_min))
+    def timer(path, nobjs, ptype, method, mark_min, pair_max=None):
+        calls.append((nobjs, ptype, mark_min, pair_max))
         assert os.path.exists(path)
+        if pair_max is not None:  # three objectives: the staircase pays from 96 candidates up
+            assert nobjs == 3 and mark_min == 16384
+            return 1.0 + abs(pair_max - 96) / 1e3
         if mark_min is None:  # the built-in behaviour: slower for d=3, fastest for d=5
             return 2.0 if nobjs == 3 else 0.5
         return 1.0 + abs(mark_min - 16384) / 1e6
@@ -31,13 +34,25 @@ def test_tune_with_a_fake_timer(tmp_path):
     entries = autotune.tune([(3, 1), (5, 3)], sizes=(4096, 16384, 65536), timer=timer, workdir=str(tmp_path))
     assert set(entries) == {"d3_p1", "d5_p3"}
     assert entries["d3_p1"]["big_mark_min"] == 16384
+    assert entries["d3_p1"]["lex_pair_max"] == 96
     assert entries["d5_p3"]["builtin"] is True and "big_mark_min" not in entries["d5_p3"]
-    assert len(calls) == 8
+    assert "lex_pair_max" not in entries["d5_p3"]
+    assert len(calls) == 8 + len(autotune.PAIR_MAX_SIZES)
     # the engine reads a built-in entry as untuned, the other one as tuned
     path = autotune.write(entries, str(tmp_path / "t.json"))
     lib = _native.gpu_lib()
     assert lib.pmdd_tuned_mark_min(path.encode(), 3, 1) == 16384
     assert lib.pmdd_tuned_mark_min(path.encode(), 5, 3) == 0
+    assert lib.pmdd_tuned_lex_pair_max(path.encode(), 3, 1) == 96
+    assert lib.pmdd_tuned_lex_pair_max(path.encode(), 5, 3) == -1
+
+
+def test_choose_pair_max():
+    assert autotune.choose_pair_max({0: 2.0, 48: 1.5, 96: 1.0}) == 96
+    assert autotune.choose_pair_max({0: 1.0, 48: 1.01, 96: 1.3}) == 48  # within 2 %: the default
+    assert autotune.choose_pair_max({0: 1.0, 16: 1.01, 48: 1.5}) == 0   # else the smallest
+    assert autotune.choose_pair_max({0: None}) == autotune.DEFAULT_PAIR_MAX
+    assert autotune.DEFAULT_PAIR_MAX in autotune.PAIR_MAX_SIZES
 
 
 def test_default_is_among_the_timed_sizes():
@@ -129,3 +144,47 @@ def test_engine_applies_the_tuned_crossover(tmp_path):
     plain = run({"PMDD_TUNING_FILE": never})
     assert tuned["ok"] and plain["ok"]
     assert tuned["launches"] > plain["launches"]
+
+
+LEX_CHILD = r"""
+import sys, json
+sys.path.insert(0, {root!r})
+import numpy as np
+import oracle
+import pmdd_b200 as P
+from pmdd_b200 import instances
+dd = P.DecisionDiagram.from_text(instances.knapsack_text(40, 3, 0), 1, 3)
+st = {{}}
+got = P.enumerate_dd(dd, method=1, stats=st)
+ok = np.array_equal(oracle.sorted_set(got), oracle.sorted_set(oracle.enumerate(dd, 1)))
+print(json.dumps({{"ok": bool(ok), "stair": st["work_stair_candidates_total"],
+                   "cand": st["work_candidates_total"]}}))
+"""
+
+
+@pytest.mark.gpu
+def test_engine_applies_the_tuned_pair_max(tmp_path):
+    """A tuning file whose three-objective knapsack entry sends every tile destination to
+    the staircase warps (lex_pair_max 0) makes them filter far more candidates than one
+    that keeps every tile destination pairwise (1024: only oversized destinations are
+    left to staircases); the frontier is the same."""
+    import subprocess
+    import sys
+
+    from conftest import ROOT
+
+    def run(pair_max):
+        path = str(tmp_path / f"t{pair_max}.json")
+        autotune.write({"d3_p1": {"lex_pair_max": pair_max}}, path)
+        env = dict(os.environ, PMDD_TUNING_FILE=path)
+        env.pop("PMDD_LEX_PAIR_MAX", None)
+        env.pop("PMDD_LEX_TILES", None)
+        p = subprocess.run([sys.executable, "-c", LEX_CHILD.format(root=ROOT)], env=env, capture_output=True,
+                           text=True, timeout=600)
+        assert p.returncode == 0, p.stdout + p.stderr
+        return json.loads(p.stdout.strip().splitlines()[-1])
+
+    all_stair, all_pair = run(0), run(1024)
+    assert all_stair["ok"] and all_pair["ok"]
+    assert all_stair["stair"] > 0.9 * all_stair["cand"]
+    assert all_pair["stair"] < 0.05 * all_pair["cand"]
