@@ -67,6 +67,7 @@ struct LexSmem {
     uint8_t item_count[kTileItemCap];    // 1: merge by counting
     int16_t big[kTileItemCap];           // destinations filtered by a staircase warp
     int16_t arc_pos[kTileArcCap + 1];    // staged arc -> first candidate position
+    int16_t arc_item[kTileArcCap];       // staged arc -> staged destination
     int32_t arc_w[kTileArcCap];          // staged arc -> weight row
     int64_t arc_src[kTileArcCap];        // staged arc -> parent slot start (points)
     int32_t warp_i[32];
@@ -77,6 +78,38 @@ struct LexSmem {
 // Per-warp staircase storage, laid over pts once the merge has read it.
 template <typename T>
 using Stair = StairBuf<T, kStairCap>;
+
+// Largest x over the threads before this one (-1 for thread 0); every thread calls it.
+template <int THREADS>
+__device__ __forceinline__ int32_t block_exclusive_max(int32_t x, int32_t *warp_buf) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int32_t inc = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int32_t y = __shfl_up_sync(kFull, inc, o);
+        if (lane >= o) inc = max(inc, y);
+    }
+    int32_t exc = __shfl_up_sync(kFull, inc, 1);
+    if (lane == 0) exc = -1;
+    if (lane == 31) warp_buf[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        const int32_t w = lane < THREADS / 32 ? warp_buf[lane] : -1;
+        int32_t winc = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int32_t y = __shfl_up_sync(kFull, winc, o);
+            if (lane >= o) winc = max(winc, y);
+        }
+        int32_t wexc = __shfl_up_sync(kFull, winc, 1);
+        if (lane == 0) wexc = -1;
+        if (lane < THREADS / 32) warp_buf[lane] = wexc;
+    }
+    __syncthreads();
+    const int32_t r = max(exc, warp_buf[warp]);
+    __syncthreads();  // warp_buf may be reused right after
+    return r;
+}
 
 template <typename T>
 __device__ __forceinline__ bool lex_gt(const PackedPt<3, T> &a, const PackedPt<3, T> &b) {
@@ -241,26 +274,38 @@ __global__ void __launch_bounds__(kLT) expand_tile_lex_kernel(const ExpandJob *_
                 S.arc_pos[x] = static_cast<int16_t>(S.item_s[k] + (c0 - S.item_c0[k]));
                 S.arc_src[x] = J.prev_off[nb];
                 S.arc_w[x] = J.arc_wrow[a];
+                S.arc_item[x] = static_cast<int16_t>(k);
                 if (J.prev_sorted == nullptr || J.prev_sorted[nb] == 0) S.item_count[k] = 1;
             }
             if (tid == 0) S.arc_pos[total_a] = static_cast<int16_t>(total);
+            for (int q = tid; q < total; q += kLT) S.tag[q] = -1;
+            __syncthreads();
+            // --- each candidate's arc: mark every non-empty run's first position, then a
+            // block-wide running maximum carries the arc over its run
+            for (int x = tid; x < total_a; x += kLT)
+                if (S.arc_pos[x + 1] > S.arc_pos[x]) S.tag[S.arc_pos[x]] = static_cast<int16_t>(x);
+            __syncthreads();
+            {
+                constexpr int QP = kTileCap / kLT;
+                int32_t run = -1, seen[QP];
+#pragma unroll
+                for (int r = 0; r < QP; ++r) {
+                    const int q = tid * QP + r;
+                    if (q < total) run = max(run, static_cast<int32_t>(S.tag[q]));
+                    seen[r] = run;
+                }
+                const int32_t before = block_exclusive_max<kLT>(run, S.warp_i);
+#pragma unroll
+                for (int r = 0; r < QP; ++r) {
+                    const int q = tid * QP + r;
+                    if (q < total) S.tag[q] = static_cast<int16_t>(max(before, seen[r]));
+                }
+            }
             __syncthreads();
             // --- expand: candidate = parent point + arc weight (run order)
             for (int q = tid; q < total; q += kLT) {
-                int lo = 0, hi = n_it - 1;
-                while (lo < hi) {
-                    const int mid = (lo + hi + 1) >> 1;
-                    if (S.item_s[mid] <= q) lo = mid;
-                    else hi = mid - 1;
-                }
-                const int k = lo;
-                int alo = S.item_arc0[k], ahi = S.item_arc0[k + 1] - 1;
-                while (alo < ahi) {
-                    const int mid = (alo + ahi + 1) >> 1;
-                    if (S.arc_pos[mid] <= q) alo = mid;
-                    else ahi = mid - 1;
-                }
-                const int x = alo;
+                const int x = S.tag[q];
+                const int k = S.arc_item[x];
                 const int64_t idx = q - S.arc_pos[x];
                 const T *src = prev + (S.arc_src[x] + idx) * 3;
                 const int32_t *w = J.weights + static_cast<int64_t>(S.arc_w[x]) * 3;
@@ -268,7 +313,6 @@ __global__ void __launch_bounds__(kLT) expand_tile_lex_kernel(const ExpandJob *_
 #pragma unroll
                 for (int o = 0; o < PackedPt<3, T>::kPad; ++o) pt.v[o] = o < 3 ? src[o] + static_cast<T>(w[o]) : T(0);
                 S.pts[q] = pt;
-                S.tag[q] = static_cast<int16_t>(x);
                 S.item_of[q] = static_cast<uint16_t>(k);
             }
             __syncthreads();
