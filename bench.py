@@ -225,7 +225,9 @@ def single_instances(P, instances, device, with_ref):
 # --------------------------------------------------------------- served loop
 def served_loop(rate, n_req, seed, P, instances, device=0):
     """Poisson arrivals at `rate` req/s; KP (n~U{20..60}) / SP (n~U{60..100}) method 1 and
-    TSP (n~U{9..13}, method 3); latency = finish - arrival on the host clock.  Knapsack
+    TSP (n~U{9..13}, method 3); latency = finish - arrival on the host clock.  Afterwards
+    every request runs alone on an idle server (submit -> result); the slowdown of a
+    request is its served latency over its lone one.  Knapsack
     and set-packing DDs are built on the host before the loop; a TSP request goes in by
     its cost matrices (the server's shared n-city MDD on the device).  Every
     result's frontier CSV.gz and stats record are handed to the asynchronous writer as it
@@ -268,7 +270,7 @@ def served_loop(rate, n_req, seed, P, instances, device=0):
             if r.status != 0:
                 raise RuntimeError(f"served request {r.req_id} failed: {r.error}")
             # finish_s is the engine's steady clock; arrival is relative to t0
-            lat.append((r.finish_s - (t0_mono + arrivals[r.req_id])) * 1e3)
+            lat.append((r.req_id, (r.finish_s - (t0_mono + arrivals[r.req_id])) * 1e3))
             finished += 1
             rec = json.dumps({"request": int(r.req_id), "problem_type": specs[r.req_id][0],
                               "method": specs[r.req_id][2], "num_solutions": int(len(r.frontier))})
@@ -282,9 +284,26 @@ def served_loop(rate, n_req, seed, P, instances, device=0):
     tail_ms = (time.perf_counter() - tw) * 1e3
     writer.close()
     shutil.rmtree(outdir, ignore_errors=True)
-    lat = np.array(lat)
+    # each request alone: a server with nothing else to do, submit -> result
+    alone = np.zeros(n_req)
+    lone = P.Server(device=device)
+    for i in range(n_req):
+        if specs[i][0] == 3:
+            lone.submit_tsp(dds[i], i, method=specs[i][2])
+        else:
+            lone.submit(dds[i], i, method=specs[i][2])
+        while lone.pending() > 0:
+            lone.run(0)
+        r = lone.poll()
+        alone[i] = (r.finish_s - r.submit_s) * 1e3
+    lone.close()
+    ids = np.array([i for i, _ in lat])
+    lat = np.array([x for _, x in lat])
+    slow = lat / np.maximum(alone[ids], 1e-3)
     return {"rate_rps": rate, "requests": n_req, "p50_ms": float(np.percentile(lat, 50)),
             "p99_ms": float(np.percentile(lat, 99)), "solves_per_s": n_req / wall,
+            "alone_p50_ms": float(np.percentile(alone, 50)), "alone_p99_ms": float(np.percentile(alone, 99)),
+            "slowdown_p50": float(np.percentile(slow, 50)), "slowdown_p99": float(np.percentile(slow, 99)),
             "outputs_written": written, "writer_tail_ms": tail_ms,
             "admission": {k: int(info[k]) for k in ("admitted", "completed", "rejected", "failed", "queued_peak",
                                                      "running_peak", "budget_bytes", "peak_used_bytes")}}
@@ -522,7 +541,9 @@ def main():
     alg_per_launch = alg_bytes / max(1, tile_launches)
     traffic = None
     issue = None
-    tpath = os.path.join(ROOT, "profiles", "expand_tile_kernel_stream_traffic.json")
+    lex = os.environ.get("PMDD_LEX_TILES", "1") != "0"  # three objectives: the lexicographic tiles
+    kname = "expand_tile_lex_kernel" if lex else "expand_tile_kernel"
+    tpath = os.path.join(ROOT, "profiles", f"{kname}_stream_traffic.json")
     if os.path.exists(tpath):
         try:
             tj = json.load(open(tpath))
@@ -560,7 +581,9 @@ def main():
         "clocks": clocks,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak if peak else None, "traffic": traffic,
-                     "kernel": "expand_tile_kernel<3,int32> (fused expand + dominance filter)",
+                     "kernel": (f"{kname}<int32> (fused expand + lexicographic merge + staircase filter)" if lex
+                                else f"{kname}<3,int32> (fused expand + pairwise dominance filter)"),
+                     "traffic_source": os.path.relpath(tpath, ROOT) if traffic is not None else None,
                      "peak_kind": peak_kind,
                      "launches": int(tile_launches),
                      "algorithmic_bytes_per_launch": int(alg_per_launch),
