@@ -57,6 +57,7 @@ constexpr int kBigJTile = 1024;       // candidates per shared-memory comparison
 // Device error word bits (written with atomicOr; read back once per step).
 constexpr uint32_t kErrBounds = 1u;        // an index check failed (work skipped)
 constexpr uint32_t kErrCoupleOverflow = 2u;
+constexpr uint32_t kErrTimeout = 4u;       // a bounded wait (bulk-copy barrier) gave up
 
 // One layer expansion of one instance in one direction.  "Items" are the destination
 // nodes of the layer; each has a contiguous range of arcs whose neighbour (the arc's
@@ -106,6 +107,8 @@ struct ExpandJob {
     int32_t pair_max;              // lexicographic tiles: destinations of at most this many
                                    // candidates are checked pairwise, larger ones by a staircase warp
     int32_t lex_big;               // 1: oversized destinations with sorted runs take big_lex.cu
+    int32_t lex_bulk;              // 1: lexicographic tiles stage parent runs by bulk copies
+    int32_t pad2;
 };
 
 // Bytes of oversized-destination scratch per candidate point.

@@ -576,6 +576,8 @@ Engine::Engine(int device, int64_t budget_bytes, int max_slots) : device_(device
     *(static_cast<unsigned char *>(h_init_.p) + 132) = 1;                   // one point is sorted
     const char *lx = std::getenv("PMDD_LEX_TILES");
     if (lx && lx[0] == '0') lex_tiles_ = false;
+    const char *lb = std::getenv("PMDD_LEX_BULK");
+    if (lb && *lb) lex_bulk_ = lb[0] == '1';
     const char *pm = std::getenv("PMDD_LEX_PAIR_MAX");
     if (pm && *pm && std::atoi(pm) >= 0) lex_pair_max_fixed_ = std::atoi(pm);
     ok_ = true;
@@ -1132,6 +1134,7 @@ int Engine::step() {
                 J.out_sorted = e.out_sorted;
                 J.pair_max = pair_max_for(I.d, I.opts.problem_type);
                 J.lex_big = (I.d == 3 && lex_tiles_) ? 1 : 0;
+                J.lex_bulk = lex_bulk_ ? 1 : 0;
                 J.tile_base = gl.tiles;
                 tile_bases[pos] = gl.tiles;
                 item_bases[pos] = gl.items;
@@ -1653,8 +1656,12 @@ int Engine::step() {
     // ----------------------------------------------------------- host updates
     const uint32_t errw = *reinterpret_cast<uint32_t *>(hsum + s_err);
     if (errw != 0) {
+        const bool timeout = (errw & dev::kErrTimeout) != 0 && (errw & ~dev::kErrTimeout) == 0;
         for (auto &p : active_)
-            if (p->phase != Instance::DONE) fail(*p, PMDD_ERR_INTERNAL, "device-side index check failed");
+            if (p->phase != Instance::DONE) {
+                if (timeout) fail(*p, PMDD_ERR_TIMEOUT, "a bounded device wait gave up (bulk-copy staging)");
+                else fail(*p, PMDD_ERR_INTERNAL, "device-side index check failed");
+            }
     }
     for (size_t k = 0; k < exps.size(); ++k) {
         const ExpPlan &e = exps[k];

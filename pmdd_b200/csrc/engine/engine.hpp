@@ -323,6 +323,9 @@ class Engine {
     // value ("lex_pair_max" in the tuning file), else kDefaultPairMax.
     static constexpr int32_t kDefaultPairMax = 48;
     bool lex_tiles_ = true;
+    // Lexicographic tiles stage each arc's parent run into shared memory with one bulk copy
+    // (cp.async.bulk on an mbarrier) instead of per-thread loads: PMDD_LEX_BULK=1 / 0.
+    bool lex_bulk_ = false;
     int32_t lex_pair_max_fixed_ = -1;
     std::map<std::pair<int, int>, int64_t> tuned_pair_max_;
     int32_t pair_max_for(int d, int problem_type) const;

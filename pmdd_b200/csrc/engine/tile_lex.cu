@@ -35,6 +35,7 @@
 // stays; which copy stays does not change the frontier.  Oversized destinations are
 // left to big.cu, whose output is not in this order (out_sorted = 0): their children
 // merge by counting.
+#include "bulk.cuh"
 #include "kernels.cuh"
 #include "scan.cuh"
 #include "stair.cuh"
@@ -51,6 +52,7 @@ constexpr int kLexWarps = kLT / 32;
 constexpr int kStairCap = 64;      // staircase entries a warp keeps; beyond it: pairwise
 constexpr int kMergeMaxArcs = 16;  // more runs in a destination: rank by counting
 constexpr unsigned kFull = 0xffffffffu;
+constexpr int kWaitIters = 1 << 22;  // bulk-copy barrier: try_wait rounds before giving up
 
 template <typename T>
 struct LexSmem {
@@ -70,9 +72,11 @@ struct LexSmem {
     int16_t arc_item[kTileArcCap];       // staged arc -> staged destination
     int32_t arc_w[kTileArcCap];          // staged arc -> weight row
     int64_t arc_src[kTileArcCap];        // staged arc -> parent slot start (points)
+    int32_t arc_stage[kTileArcCap];      // bulk staging: byte offset of the run's first point (in mpts)
+    uint64_t bar;                        // bulk staging barrier
     int32_t warp_i[32];
     int32_t tot_i, tot_a, i0, i1, job;
-    int32_t n_big, next_big, next_chunk;
+    int32_t n_big, next_big, next_chunk, tot_stage;
 };
 
 // Per-warp staircase storage, laid over pts once the merge has read it.
@@ -161,7 +165,11 @@ __global__ void __launch_bounds__(kLT) expand_tile_lex_kernel(const ExpandJob *_
     LexSmem<T> &S = *reinterpret_cast<LexSmem<T> *>(smem_raw);
     Stair<T> *stairs = reinterpret_cast<Stair<T> *>(&S.pts[0]);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (int64_t tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
+    unsigned bar_phase = 0;
+    bool aborted = false;
+    if (tid == 0) mbar_init(&S.bar, 1);
+    __syncthreads();
+    for (int64_t tile = blockIdx.x; tile < total_tiles && !aborted; tile += gridDim.x) {
         if (tid == 0) {
             const int j = find_base(tile_bases, num_jobs, tile);
             const ExpandJob &J = jobs[j];
@@ -280,6 +288,64 @@ __global__ void __launch_bounds__(kLT) expand_tile_lex_kernel(const ExpandJob *_
             if (tid == 0) S.arc_pos[total_a] = static_cast<int16_t>(total);
             for (int q = tid; q < total; q += kLT) S.tag[q] = -1;
             __syncthreads();
+            // --- bulk staging (J.lex_bulk): each parent run, widened to 16-byte boundaries,
+            // goes to shared memory (the mpts area, unused until the merge) by one
+            // cp.async.bulk completing on the block's barrier, while the arc assignment
+            // below runs.  Frontier blocks are arena blocks (256-byte aligned, sizes
+            // rounded up to 256 bytes), so the widened range stays inside the block.
+            unsigned char *stage = reinterpret_cast<unsigned char *>(&S.mpts[0]);
+            bool bulk = false;
+            if (J.lex_bulk) {
+                constexpr int AP = kTileArcCap / kLT;
+                int32_t padded[AP];
+                uintptr_t lo_addr[AP];
+                int32_t local = 0;
+#pragma unroll
+                for (int r = 0; r < AP; ++r) {
+                    const int x = tid * AP + r;
+                    padded[r] = 0;
+                    lo_addr[r] = 0;
+                    if (x < total_a) {
+                        const int len = S.arc_pos[x + 1] - S.arc_pos[x];
+                        if (len > 0) {
+                            const uintptr_t a = reinterpret_cast<uintptr_t>(prev + S.arc_src[x] * 3);
+                            const uintptr_t lo = a & ~static_cast<uintptr_t>(15);
+                            const uintptr_t hi = (a + static_cast<uintptr_t>(len) * 3 * sizeof(T) + 15) &
+                                                 ~static_cast<uintptr_t>(15);
+                            padded[r] = static_cast<int32_t>(hi - lo);
+                            lo_addr[r] = lo;
+                        }
+                    }
+                    local += padded[r];
+                }
+                const int32_t ex = block_exclusive_scan<int32_t, kLT>(local, S.warp_i, &S.tot_stage);
+                bulk = S.tot_stage <= static_cast<int32_t>(sizeof(S.mpts));
+                if (bulk) {
+                    int32_t run = ex;
+#pragma unroll
+                    for (int r = 0; r < AP; ++r) {
+                        const int x = tid * AP + r;
+                        if (x < total_a && padded[r] > 0) {
+                            const uintptr_t a = reinterpret_cast<uintptr_t>(prev + S.arc_src[x] * 3);
+                            S.arc_stage[x] = run + static_cast<int32_t>(a - lo_addr[r]);
+                        }
+                        run += padded[r];
+                    }
+                    fence_proxy_async_smem();  // the last pass's reads and writes of mpts come first
+                    __syncthreads();
+                    if (tid == 0) mbar_arrive_expect_tx(&S.bar, static_cast<unsigned>(S.tot_stage));
+                    __syncthreads();
+                    run = ex;
+#pragma unroll
+                    for (int r = 0; r < AP; ++r) {
+                        const int x = tid * AP + r;
+                        if (x < total_a && padded[r] > 0)
+                            bulk_g2s(stage + run, reinterpret_cast<const void *>(lo_addr[r]),
+                                     static_cast<unsigned>(padded[r]), &S.bar);
+                        run += padded[r];
+                    }
+                }
+            }
             // --- each candidate's arc: mark every non-empty run's first position, then a
             // block-wide running maximum carries the arc over its run
             for (int x = tid; x < total_a; x += kLT)
@@ -302,12 +368,25 @@ __global__ void __launch_bounds__(kLT) expand_tile_lex_kernel(const ExpandJob *_
                 }
             }
             __syncthreads();
+            if (bulk) {
+                bool ok = false;
+                for (int it = 0; it < kWaitIters && !ok; ++it) ok = mbar_try_wait(&S.bar, bar_phase);
+                bar_phase ^= 1u;
+                if (__syncthreads_or(!ok)) {
+                    // the copies did not arrive: report, give them one more bounded wait, stop
+                    if (tid == 0) atomicOr(J.err, kErrTimeout);
+                    for (int it = 0; it < kWaitIters && !ok; ++it) ok = mbar_try_wait(&S.bar, bar_phase ^ 1u);
+                    aborted = true;
+                    break;
+                }
+            }
             // --- expand: candidate = parent point + arc weight (run order)
             for (int q = tid; q < total; q += kLT) {
                 const int x = S.tag[q];
                 const int k = S.arc_item[x];
                 const int64_t idx = q - S.arc_pos[x];
-                const T *src = prev + (S.arc_src[x] + idx) * 3;
+                const T *src = bulk ? reinterpret_cast<const T *>(stage + S.arc_stage[x]) + idx * 3
+                                    : prev + (S.arc_src[x] + idx) * 3;
                 const int32_t *w = J.weights + static_cast<int64_t>(S.arc_w[x]) * 3;
                 PackedPt<3, T> pt;
 #pragma unroll

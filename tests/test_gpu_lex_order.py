@@ -6,7 +6,8 @@
   oversized path's 256.  Both fall back to checking every earlier point; the frontiers
   must equal the oracle's.
 * Both ends of the pairwise / staircase crossover (PMDD_LEX_PAIR_MAX 0: every
-  destination by a staircase warp; 1024: every destination pairwise) and the pairwise tile
+  destination by a staircase warp; 1024: every destination pairwise), the parent runs
+  staged by bulk copies or loaded directly (PMDD_LEX_BULK 1 / 0), and the pairwise tile
   kernel (PMDD_LEX_TILES=0) stay exact on the golden fixtures and seeded instances.  The
   engine reads these settings at start-up, so each runs in a child process.
 """
@@ -77,14 +78,15 @@ print(json.dumps({{"checked": n}}))
 """
 
 
-@pytest.mark.parametrize("env", [{"PMDD_LEX_PAIR_MAX": "0"}, {"PMDD_LEX_PAIR_MAX": "1024"}, {"PMDD_LEX_TILES": "0"}],
-                         ids=["all-staircase", "all-pairwise", "pairwise-kernel"])
+@pytest.mark.parametrize("env", [{"PMDD_LEX_PAIR_MAX": "0"}, {"PMDD_LEX_PAIR_MAX": "1024"}, {"PMDD_LEX_TILES": "0"},
+                                 {"PMDD_LEX_BULK": "1"}, {"PMDD_LEX_BULK": "0"}],
+                         ids=["all-staircase", "all-pairwise", "pairwise-kernel", "bulk-staging", "direct-loads"])
 def test_filter_paths_stay_exact(env):
     from conftest import ROOT
 
     e = dict(os.environ)
-    e.pop("PMDD_LEX_PAIR_MAX", None)
-    e.pop("PMDD_LEX_TILES", None)
+    for k in ("PMDD_LEX_PAIR_MAX", "PMDD_LEX_TILES", "PMDD_LEX_BULK"):
+        e.pop(k, None)
     e.update(env)
     p = subprocess.run([sys.executable, "-c", CHILD.format(root=ROOT, tests=os.path.join(ROOT, "tests"))], env=e,
                        capture_output=True, text=True, timeout=900)
