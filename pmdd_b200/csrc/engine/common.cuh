@@ -109,6 +109,7 @@ struct ExpandJob {
     int32_t lex_big;               // 1: oversized destinations with sorted runs take big_lex.cu
     int32_t lex_bulk;              // 1: lexicographic tiles stage parent runs by bulk copies
     int32_t pad2;
+    unsigned long long *phase_clk; // diagnostic: cycles per tile phase (lexicographic tiles), or nullptr
 };
 
 // Bytes of oversized-destination scratch per candidate point.

@@ -1254,7 +1254,8 @@ int Engine::step() {
     const size_t f_ts = sizeof(dev::CountResult) * counts.size();
     const size_t f_sd = f_ts + 2 * sizeof(unsigned long long) * exps.size();  // (survivors, staircase) per expansion
     const size_t f_err = f_sd + sizeof(int64_t) * sdjobs.size();
-    const size_t f_total = f_err + sizeof(uint64_t);
+    const size_t f_clk = f_err + sizeof(uint64_t);  // PMDD_TRACE: tile phase cycles (8 counters)
+    const size_t f_total = f_clk + (trace_ ? 8 * sizeof(unsigned long long) : 0);
     char *d_fixed = static_cast<char *>(scratch(f_total));
     dev::CountResult *d_results = counts.empty() ? nullptr : reinterpret_cast<dev::CountResult *>(d_fixed);
     unsigned long long *d_tile_surv = d_fixed ? reinterpret_cast<unsigned long long *>(d_fixed + f_ts) : nullptr;
@@ -1263,6 +1264,7 @@ int Engine::step() {
     for (size_t k = 0; k < xjobs.size(); ++k) {
         xjobs[k].tile_surv = d_tile_surv ? d_tile_surv + 2 * k : nullptr;
         xjobs[k].err = d_err_step;
+        xjobs[k].phase_clk = (trace_ && d_fixed) ? reinterpret_cast<unsigned long long *>(d_fixed + f_clk) : nullptr;
     }
     for (size_t k = 0; k < sdjobs.size(); ++k) sdjobs[k].removed = d_removed ? d_removed + k : nullptr;
     bool count_alloc_ok = d_fixed != nullptr && !sd_alloc_failed;
@@ -1641,14 +1643,16 @@ int Engine::step() {
         unsigned long long tile_surv = 0;
         for (size_t k = 0; k < exps.size(); ++k)
             tile_surv += reinterpret_cast<const unsigned long long *>(static_cast<char *>(h_summary_.p) + s_ts)[2 * k];
+        const unsigned long long *pc = reinterpret_cast<const unsigned long long *>(static_cast<char *>(h_summary_.p) + f_clk);
         std::fprintf(stderr,
                      "[pmdd step] jobs=%zu counts=%zu couple=%zu cand=%lld big_items=%lld big_cand=%lld max_item=%lld "
                      "tile_cand=%lld tile_surv=%llu tiles_ms=%.3f big_ms=%.3f rest_ms=%.3f host_to_sync_us=%.1f "
-                     "arena_reserved_mb=%.0f arena_grow_ms=%.1f\n",
+                     "arena_reserved_mb=%.0f arena_grow_ms=%.1f phase_mcyc=%.2f,%.2f,%.2f,%.2f,%.2f,%.2f,%.2f\n",
                      exps.size(), counts.size(), ujobs.size(), static_cast<long long>(cand),
                      static_cast<long long>(nbig), static_cast<long long>(big_cand), static_cast<long long>(max_item),
                      static_cast<long long>(cand - big_cand), tile_surv, ms_expand, ms_big, ms_rest,
-                     (now_s() - step_t0) * 1e6, arena_.reserved() / 1e6, arena_.grow_seconds() * 1e3);
+                     (now_s() - step_t0) * 1e6, arena_.reserved() / 1e6, arena_.grow_seconds() * 1e3,
+                     pc[0] * 1e-6, pc[1] * 1e-6, pc[2] * 1e-6, pc[3] * 1e-6, pc[4] * 1e-6, pc[5] * 1e-6, pc[6] * 1e-6);
     }
     for (void *q : step_scratch_) arena_.release(q);
     step_scratch_.clear();

@@ -79,6 +79,24 @@ struct LexSmem {
     int32_t n_big, next_big, next_chunk, tot_stage;
 };
 
+// Phase clock (J.phase_clk, a diagnostic): thread 0 adds the cycles its block spent in
+// each phase of a pass (stage destinations, stage arcs, arc assignment, expand, merge,
+// filter, scan and write) to the job's counters.
+struct PhaseClock {
+    unsigned long long *out;
+    long long t;
+    __device__ __forceinline__ void start() {
+        if (out) t = clock64();
+    }
+    __device__ __forceinline__ void lap(int phase) {
+        if (out) {
+            const long long now = clock64();
+            atomicAdd(out + phase, static_cast<unsigned long long>(now - t));
+            t = now;
+        }
+    }
+};
+
 // Per-warp staircase storage, laid over pts once the merge has read it.
 template <typename T>
 using Stair = StairBuf<T, kStairCap>;
@@ -184,6 +202,8 @@ __global__ void __launch_bounds__(kLT) expand_tile_lex_kernel(const ExpandJob *_
         const T *__restrict__ prev = static_cast<const T *>(J.prev_pts);
         T *__restrict__ outp = static_cast<T *>(J.out_pts);
         const int pair_max = J.pair_max;
+        PhaseClock clk{tid == 0 ? J.phase_clk : nullptr, 0};
+        clk.start();
         int32_t ic = i0;
         while (ic < i1) {
             const int n_stage = min(kTileItemCap, i1 - ic);
@@ -267,6 +287,7 @@ __global__ void __launch_bounds__(kLT) expand_tile_lex_kernel(const ExpandJob *_
                 if (tid == 0) atomicOr(J.err, kErrBounds);
                 break;
             }
+            clk.lap(0);
             // --- stage the arcs of the small destinations (and whether each parent is sorted)
             for (int x = tid; x < total_a; x += kLT) {
                 int lo = 0, hi = n_it - 1;  // destination owning staged arc x
@@ -346,6 +367,7 @@ __global__ void __launch_bounds__(kLT) expand_tile_lex_kernel(const ExpandJob *_
                     }
                 }
             }
+            clk.lap(1);
             // --- each candidate's arc: mark every non-empty run's first position, then a
             // block-wide running maximum carries the arc over its run
             for (int x = tid; x < total_a; x += kLT)
@@ -380,6 +402,7 @@ __global__ void __launch_bounds__(kLT) expand_tile_lex_kernel(const ExpandJob *_
                     break;
                 }
             }
+            clk.lap(2);
             // --- expand: candidate = parent point + arc weight (run order)
             for (int q = tid; q < total; q += kLT) {
                 const int x = S.tag[q];
@@ -395,6 +418,7 @@ __global__ void __launch_bounds__(kLT) expand_tile_lex_kernel(const ExpandJob *_
                 S.item_of[q] = static_cast<uint16_t>(k);
             }
             __syncthreads();
+            clk.lap(3);
             // --- merge: each candidate's position in its destination's lexicographic order
             for (int q = tid; q < total; q += kLT) {
                 const int k = S.item_of[q];
@@ -438,6 +462,7 @@ __global__ void __launch_bounds__(kLT) expand_tile_lex_kernel(const ExpandJob *_
                 }
                 __syncthreads();
             }
+            clk.lap(4);
             // --- filter, big destinations: one staircase warp each
             while (true) {
                 int b = 0;
@@ -484,6 +509,7 @@ __global__ void __launch_bounds__(kLT) expand_tile_lex_kernel(const ExpandJob *_
                 if (mine) S.keep[q] = dom ? 0 : 1;
             }
             __syncthreads();
+            clk.lap(5);
             // --- exclusive scan of keep flags (merged order)
             constexpr int QPER = kTileCap / kLT;
             int32_t kept_local = 0;
@@ -523,6 +549,7 @@ __global__ void __launch_bounds__(kLT) expand_tile_lex_kernel(const ExpandJob *_
                 if (je > js) J.out_size[ic + k] = S.keep_ex[je] - S.keep_ex[js];
             }
             __syncthreads();
+            clk.lap(6);
             ic += n_it;
         }
         __syncthreads();  // tile bookkeeping in shared memory is rewritten next iteration
