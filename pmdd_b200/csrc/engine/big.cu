@@ -548,7 +548,8 @@ static cudaError_t launch_big_t(const BigLaunch &L, cudaStream_t stream) {
     }
     const bool lex = D == 3 && L.lex_big;
     if (lex) {
-        const cudaError_t e = launch_big_lex_rank(sizeof(T) == 8, L, stream);
+        cudaError_t e = launch_big_lex_rank(sizeof(T) == 8, L, stream);
+        for (int r = 0; e == cudaSuccess && r < L.lex_rounds; ++r) e = launch_big_lex_merge(sizeof(T) == 8, L, r, stream);
         if (e != cudaSuccess) return e;
     } else {
         const int64_t want = (L.total + kFlatThreads - 1) / kFlatThreads;

@@ -1,7 +1,7 @@
 // Oversized destinations of three objectives, in lexicographic order.
 //
 // A destination too large for a tile (tile_resident()) whose arc runs all come from
-// frontiers kept in descending lexicographic order, at most kBigMergeMaxArcs of them, is
+// frontiers kept in descending lexicographic order, at most kBigLexMaxArcs of them, is
 // filtered here instead of by big.cu's sort-filter-skyline or pivot/mark passes:
 //
 //   big_lex_rank_kernel:   thread per candidate of the scratch pass (the flat space of
@@ -12,6 +12,10 @@
 //       points: the lower run first); it is written to scratch at that position.
 //       Candidates of destinations this path does not take are written in run order, as
 //       big_expand_kernel writes them;
+//   big_lex_merge_kernel:  destinations of more than kBigDirectArcs runs are written in run
+//       order by the rank kernel and sorted by ceil(log2(runs)) rounds that merge
+//       neighbouring groups of runs (thread per candidate, a binary search into the
+//       sibling group), alternating between the two scratch buffers;
 //   big_lex_filter_kernel: one warp per destination walks the sorted candidates 32 at a
 //       time with the staircase of stair.cuh and writes the survivors to the slot in
 //       order (so the destination's frontier is sorted, out_sorted = 1) -- its work is
@@ -82,7 +86,7 @@ __global__ void __launch_bounds__(kRankThreads) big_lex_rank_kernel(const Expand
         const T q0 = src[0] + static_cast<T>(w[0]), q1 = src[1] + static_cast<T>(w[1]),
                 q2 = src[2] + static_cast<T>(w[2]);
         int64_t pos = c.i;
-        if (J.lex_big && lex_eligible(J, c.B)) {
+        if (J.lex_big && c.B.a1 - c.B.a0 <= kBigDirectArcs && lex_eligible(J, c.B)) {
             pos = c.i - rs;
             for (int32_t b = c.B.a0; b < c.B.a1; ++b) {
                 if (b == a) continue;
@@ -112,6 +116,56 @@ __global__ void __launch_bounds__(kRankThreads) big_lex_rank_kernel(const Expand
     }
 }
 
+// Merge round `round` of the lexicographic destinations with more than kBigDirectArcs
+// runs: at round r the destination consists of sorted groups of 2^r consecutive runs
+// (in big_pts for even r, big_pts2 for odd r); each candidate moves to its place in the
+// union with its sibling group (a binary search there; equal points: the left group
+// first), in the other buffer.  Thread per candidate of the scratch pass.
+template <typename T>
+__global__ void __launch_bounds__(kRankThreads) big_lex_merge_kernel(const ExpandJob *__restrict__ jobs,
+                                                                     const int64_t *__restrict__ job_bases,
+                                                                     int num_jobs, int64_t total, int64_t pass,
+                                                                     int round) {
+    for (int64_t g = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; g < total;
+         g += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        BigCand c;
+        if (!big_cand(jobs, job_bases, num_jobs, g, pass, &c)) continue;
+        const ExpandJob &J = jobs[c.job];
+        const int K = c.B.a1 - c.B.a0;
+        if (!J.lex_big || round >= lex_merge_rounds(K) || !lex_eligible(J, c.B)) continue;
+        const T *src = static_cast<const T *>(round & 1 ? J.big_pts2 : J.big_pts) + c.B.soff * 3;
+        T *dst = static_cast<T *>(round & 1 ? J.big_pts : J.big_pts2) + c.B.soff * 3;
+        // start of run x of the destination (x <= K), destination-local
+        auto st = [&](int x) -> int64_t {
+            return x >= K ? c.B.n : J.arc_cand_off[c.B.a0 + x - J.arc_base] - c.B.c0;
+        };
+        int64_t rs, re;
+        const int32_t a = run_of(J, c.B, c.i, &rs, &re);
+        const int grp = (a - c.B.a0) >> round;
+        const int sib = grp ^ 1;
+        const int64_t my0 = st(grp << round);
+        const T q0 = src[c.i * 3], q1 = src[c.i * 3 + 1], q2 = src[c.i * 3 + 2];
+        int64_t cnt = 0;
+        const int64_t merged0 = st((grp >> 1) << (round + 1));
+        if ((sib << round) < K) {
+            const int64_t lo0 = st(sib << round), hi0 = st(min((sib + 1) << round, K));
+            const bool tie = sib < grp;  // the left group's equal points come first
+            int64_t lo = lo0, hi = hi0;
+            while (lo < hi) {
+                const int64_t mid = (lo + hi) >> 1;
+                const T *p = src + mid * 3;
+                if (before<T>(p[0], p[1], p[2], q0, q1, q2, tie)) lo = mid + 1;
+                else hi = mid;
+            }
+            cnt = lo - lo0;
+        }
+        T *o = dst + (merged0 + (c.i - my0) + cnt) * 3;
+        o[0] = q0;
+        o[1] = q1;
+        o[2] = q2;
+    }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(FilterCfg<T>::kThreads) big_lex_filter_kernel(const ExpandJob *__restrict__ jobs,
                                                                                 const BigWork *__restrict__ work,
@@ -125,7 +179,8 @@ __global__ void __launch_bounds__(FilterCfg<T>::kThreads) big_lex_filter_kernel(
         const ExpandJob &J = jobs[W.job];
         BigItem B;
         if (!J.lex_big || !big_item_any(J, W, pass, &B) || !lex_eligible(J, B)) continue;
-        const T *cand = static_cast<const T *>(J.big_pts) + B.soff * 3;
+        // sorted candidates: big_pts after an even number of merge rounds, else big_pts2
+        const T *cand = static_cast<const T *>(lex_merge_rounds(B.a1 - B.a0) & 1 ? J.big_pts2 : J.big_pts) + B.soff * 3;
         T *out = static_cast<T *>(J.out_pts) + B.c0 * 3;
         StairState st;
         int64_t kept = 0;
@@ -180,6 +235,18 @@ static cudaError_t launch_filter_t(const BigLaunch &L, cudaStream_t stream) {
     const unsigned grid = static_cast<unsigned>(
         std::max<int64_t>(1, std::min<int64_t>((L.num_work + Cfg::kWarps - 1) / Cfg::kWarps, int64_t(L.sms) * 16)));
     big_lex_filter_kernel<T><<<grid, Cfg::kThreads, 0, stream>>>(L.jobs, L.work, L.num_work, L.pass);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_big_lex_merge(bool wide, const BigLaunch &L, int round, cudaStream_t stream) {
+    const int64_t want = (L.total + kRankThreads - 1) / kRankThreads;
+    const unsigned grid = static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>(want, int64_t(L.sms) * 32)));
+    if (wide)
+        big_lex_merge_kernel<int64_t><<<grid, kRankThreads, 0, stream>>>(L.jobs, L.job_bases, L.num_jobs, L.total,
+                                                                         L.pass, round);
+    else
+        big_lex_merge_kernel<int32_t><<<grid, kRankThreads, 0, stream>>>(L.jobs, L.job_bases, L.num_jobs, L.total,
+                                                                         L.pass, round);
     return cudaGetLastError();
 }
 

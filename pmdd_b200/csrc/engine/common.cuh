@@ -50,6 +50,19 @@ __host__ __device__ constexpr bool tile_resident(int64_t candidates, int64_t arc
     return candidates <= kSmallMax && arcs <= kTileArcCap / 2;
 }
 
+// Oversized three-objective destinations in lexicographic order (big_lex.cu): up to
+// kBigDirectArcs runs each candidate is ranked against the other runs directly; beyond,
+// ceil(log2(runs)) merge rounds of neighbouring run groups sort the destination; more
+// than kBigLexMaxArcs runs take the pivot/mark path instead.
+constexpr int kBigDirectArcs = 16;
+constexpr int kBigLexMaxArcs = 4096;
+__host__ __device__ inline int lex_merge_rounds(int arcs) {
+    int r = 0;
+    if (arcs > kBigDirectArcs)
+        while ((1 << r) < arcs) ++r;
+    return r;
+}
+
 constexpr int kCountThreads = 1024;
 constexpr int kBigThreads = 256;
 constexpr int kBigJTile = 1024;       // candidates per shared-memory comparison tile
@@ -137,7 +150,7 @@ struct CountResult {
     int64_t big_total;   // candidates in destinations above kSmallMax
     int64_t cur_total;   // points of the current layer's frontiers (survivor statistics)
     int32_t num_big;
-    int32_t pad;
+    int32_t max_big_arcs;  // most arcs of an oversized destination
 };
 
 // Big-path work entry: one oversized destination of one job.

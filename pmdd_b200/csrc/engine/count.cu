@@ -14,11 +14,13 @@ __global__ void __launch_bounds__(kCountThreads) count_scan_kernel(const CountJo
     __shared__ int64_t s_carry;
     __shared__ unsigned long long s_max;
     __shared__ int s_nbig;
+    __shared__ int s_maxarcs;
     const int tid = threadIdx.x;
     if (tid == 0) {
         s_carry = 0;
         s_max = 0;
         s_nbig = 0;
+        s_maxarcs = 0;
     }
     __syncthreads();
     for (int base = 0; base < J.num_arcs; base += kCountThreads) {
@@ -40,6 +42,7 @@ __global__ void __launch_bounds__(kCountThreads) count_scan_kernel(const CountJo
         const int64_t c = e - b;
         atomicMax(&s_max, static_cast<unsigned long long>(c));
         if (c > 0 && !tile_resident(c, J.item_arc_off[v + 1] - J.item_arc_off[v])) {
+            atomicMax(&s_maxarcs, J.item_arc_off[v + 1] - J.item_arc_off[v]);
             const int k = atomicAdd(&s_nbig, 1);
             J.big_list[2 * k] = i;
             J.big_list[2 * k + 1] = c;
@@ -73,6 +76,7 @@ __global__ void __launch_bounds__(kCountThreads) count_scan_kernel(const CountJo
         J.result->big_total = s_carry;
         J.result->cur_total = cur_total;
         J.result->num_big = nbig;
+        J.result->max_big_arcs = s_maxarcs;
     }
 }
 

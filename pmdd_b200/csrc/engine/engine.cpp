@@ -1084,6 +1084,7 @@ int Engine::step() {
         int64_t tiles;
         size_t big_first, big_count;
         int64_t max_big;
+        int32_t max_big_arcs;      // most arcs of an oversized destination (merge rounds)
         int64_t items;             // destinations over the group's jobs
         int64_t big_passes;        // scratch passes of the oversized path
         int64_t big_rows;          // oversized candidate rows over the group's jobs (flat space)
@@ -1161,7 +1162,10 @@ int Engine::step() {
                 big_bases[pos] = gl.big_rows;
                 gl.big_rows += J.big_rows;
                 for (int b = 0; b < s.res.num_big; ++b) bigwork.push_back({static_cast<int32_t>(pos - gl.first), b});
-                if (s.res.num_big > 0) gl.max_big = std::max(gl.max_big, s.res.max_item);
+                if (s.res.num_big > 0) {
+                    gl.max_big = std::max(gl.max_big, s.res.max_item);
+                    gl.max_big_arcs = std::max(gl.max_big_arcs, s.res.max_big_arcs);
+                }
                 ordered.push_back(e);
                 ++pos;
             }
@@ -1547,6 +1551,7 @@ int Engine::step() {
         L.sms = sms_;
         L.with_sfs = true;
         L.lex_big = gl.d == 3 && lex_tiles_;
+        L.lex_rounds = L.lex_big ? dev::lex_merge_rounds(std::min(gl.max_big_arcs, dev::kBigLexMaxArcs)) : 0;
         L.mark_cap = static_cast<int>(std::min<int64_t>(gl.mark_cap, static_cast<int64_t>(gl.big_count)));
         L.plan = nullptr;
         // more SFS blocks than fit the SMs at once: start the largest destinations first
@@ -1556,7 +1561,7 @@ int Engine::step() {
         for (int64_t pass = 0; pass < gl.big_passes; ++pass) {
             L.pass = pass;
             if (!cuda_ok(dev::launch_big(gl.d, gl.wide, L, stream_), "oversized-destination kernels")) return -1;
-            launches_ += (L.mark_cap > 0 ? 9 : 2) + (ordered ? 1 : 0) + (L.lex_big ? 1 : 0);
+            launches_ += (L.mark_cap > 0 ? 9 : 2) + (ordered ? 1 : 0) + (L.lex_big ? 1 + L.lex_rounds : 0);
         }
     }
     if (!sdjobs.empty()) {

@@ -34,6 +34,7 @@ struct BigLaunch {
     int mark_cap;                // upper bound on mark-path destinations in the pass; 0: none
     int32_t *order;              // num_work ints: SFS blocks largest destination first; nullptr: list order
     bool lex_big;                // three objectives: destinations with sorted runs take big_lex.cu
+    int lex_rounds;              // merge rounds the destinations with the most runs need
 };
 // Most oversized destinations whose SFS blocks are put in size order (one block sorts them).
 constexpr int kBigOrderMax = 4096;
@@ -42,6 +43,7 @@ cudaError_t launch_big(int d, bool wide, const BigLaunch &L, cudaStream_t stream
 // The lexicographic oversized path (big_lex.cu), three objectives: the rank kernel takes
 // the place of the materialising expansion, the filter runs after the other paths.
 cudaError_t launch_big_lex_rank(bool wide, const BigLaunch &L, cudaStream_t stream);
+cudaError_t launch_big_lex_merge(bool wide, const BigLaunch &L, int round, cudaStream_t stream);
 cudaError_t launch_big_lex_filter(bool wide, const BigLaunch &L, cudaStream_t stream);
 
 }  // namespace dev
