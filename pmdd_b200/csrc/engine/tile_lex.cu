@@ -17,8 +17,8 @@
 //   merge:   each candidate's position in its destination's lexicographic order is its
 //            index in its run plus, per other run, a binary search for how many of that
 //            run's points come before it (equal points: the lower run first); a
-//            destination with more than kMergeMaxArcs runs or an unsorted run counts
-//            the points before it instead;
+//            destination with a run from an unsorted parent counts the points before it
+//            instead;
 //   filter:  destinations of at most J.pair_max candidates: each candidate is checked
 //            against the points before it in the merged order; larger destinations:
 //            one warp walks the merged order 32 candidates at a time -- each candidate
@@ -50,7 +50,6 @@ namespace {
 constexpr int kLT = kTileThreads;
 constexpr int kLexWarps = kLT / 32;
 constexpr int kStairCap = 64;      // staircase entries a warp keeps; beyond it: pairwise
-constexpr int kMergeMaxArcs = 16;  // more runs in a destination: rank by counting
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kWaitIters = 1 << 22;  // bulk-copy barrier: try_wait rounds before giving up
 
@@ -242,6 +241,7 @@ __global__ void __launch_bounds__(kLT) expand_tile_lex_kernel(const ExpandJob *_
             const int32_t exa = block_exclusive_scan<int32_t, kLT>(local_a, S.warp_i, &S.tot_a);
             // this pass takes the longest prefix of staged destinations whose arcs fit
             int32_t fit = 0;
+            int32_t end_s[PER], end_a[PER];  // where this thread's destinations end
             {
                 int32_t run = ex, runa = exa;
 #pragma unroll
@@ -251,10 +251,11 @@ __global__ void __launch_bounds__(kLT) expand_tile_lex_kernel(const ExpandJob *_
                         S.item_s[k] = static_cast<int16_t>(run);
                         S.item_arc0[k] = static_cast<int16_t>(runa);
                         if (runa + narc[r] <= kTileArcCap) ++fit;
-                        if (narc[r] > kMergeMaxArcs) S.item_count[k] = 1;
                     }
                     run += cnt[r];
                     runa += narc[r];
+                    end_s[r] = run;
+                    end_a[r] = runa;
                 }
             }
             (void)block_exclusive_scan<int32_t, kLT>(fit, S.warp_i, &S.tot_i);
@@ -264,19 +265,17 @@ __global__ void __launch_bounds__(kLT) expand_tile_lex_kernel(const ExpandJob *_
                 break;
             }
             __syncthreads();
-            if (tid == 0) {
-                int32_t e = S.item_s[n_it - 1], ea = S.item_arc0[n_it - 1];
-                const int32_t v = J.item_base + ic + n_it - 1;
-                const int32_t a0 = J.item_arc_off[v], a1 = J.item_arc_off[v + 1];
-                const int64_t c = J.arc_cand_off[a1 - J.arc_base] - J.arc_cand_off[a0 - J.arc_base];
-                if (c > 0 && tile_resident(c, a1 - a0)) {
-                    e += static_cast<int32_t>(c);
-                    ea += a1 - a0;
+            // end markers of this pass, from the thread that staged its last destination
+#pragma unroll
+            for (int r = 0; r < PER; ++r) {
+                if (tid * PER + r == n_it - 1) {
+                    S.item_s[n_it] = static_cast<int16_t>(end_s[r]);
+                    S.item_arc0[n_it] = static_cast<int16_t>(end_a[r]);
+                    S.tot_i = end_s[r];
+                    S.tot_a = end_a[r];
                 }
-                S.item_s[n_it] = static_cast<int16_t>(e);
-                S.item_arc0[n_it] = static_cast<int16_t>(ea);
-                S.tot_i = e;
-                S.tot_a = ea;
+            }
+            if (tid == 0) {
                 S.n_big = 0;
                 S.next_big = 0;
                 S.next_chunk = 0;
