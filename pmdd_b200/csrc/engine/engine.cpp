@@ -1551,6 +1551,7 @@ int Engine::step() {
         L.sms = sms_;
         L.with_sfs = true;
         L.lex_big = gl.d == 3 && lex_tiles_;
+        L.max_n = gl.max_big;
         L.lex_rounds = L.lex_big ? dev::lex_merge_rounds(std::min(gl.max_big_arcs, dev::kBigLexMaxArcs)) : 0;
         L.mark_cap = static_cast<int>(std::min<int64_t>(gl.mark_cap, static_cast<int64_t>(gl.big_count)));
         L.plan = nullptr;
@@ -1561,7 +1562,7 @@ int Engine::step() {
         for (int64_t pass = 0; pass < gl.big_passes; ++pass) {
             L.pass = pass;
             if (!cuda_ok(dev::launch_big(gl.d, gl.wide, L, stream_), "oversized-destination kernels")) return -1;
-            launches_ += (L.mark_cap > 0 ? 9 : 2) + (ordered ? 1 : 0) + (L.lex_big ? 1 + L.lex_rounds : 0);
+            launches_ += (L.mark_cap > 0 ? 9 : 2) + (ordered ? 1 : 0) + (L.lex_big ? 4 + L.lex_rounds : 0);
         }
     }
     if (!sdjobs.empty()) {

@@ -58,18 +58,17 @@ __device__ __forceinline__ bool stair_chunk(StairBuf<T, CAP> &sb, StairState &st
         cnt = a;
         dom = cnt > 0 && sb.v2[cur][cnt - 1] >= q2;
     }
-    // the chunk's survivors against each other: every lane against every surviving lane,
-    // unrolled so that the shuffles do not wait on one another
+    // the chunk's survivors against each other
     const unsigned alive = __ballot_sync(kAll, !dom);
     bool rem = false;
-    if (alive != 0u) {
-#pragma unroll
-        for (int j = 0; j < 32; ++j) {
-            const T a1 = __shfl_sync(kAll, q1, j), a2 = __shfl_sync(kAll, q2, j);
-            const bool ge = ((alive >> j) & 1u) & (a1 >= q1) & (a2 >= q2);
-            dom |= ge & (j < lane);
-            rem |= ge & (j > lane) & ((a1 != q1) | (a2 != q2));
-        }
+    unsigned mm = alive;
+    while (mm) {
+        const int j = __ffs(mm) - 1;
+        mm &= mm - 1;
+        const T a1 = __shfl_sync(kAll, q1, j), a2 = __shfl_sync(kAll, q2, j);
+        const bool ge = (a1 >= q1) & (a2 >= q2);
+        dom |= ge & (j < lane);
+        rem |= ge & (j > lane) & ((a1 != q1) | (a2 != q2));
     }
     if (!update) return dom;
     // next staircase: surviving entries and the chunk's new maxima, objective 1 descending.
