@@ -28,9 +28,9 @@ __device__ __forceinline__ void fill_item(const ExpandJob &J, int64_t k, int64_t
 }
 
 // Destinations of three objectives whose runs all come from sorted frontiers, at most
-// kBigLexMaxArcs of them: the lexicographic path (big_lex.cu) filters these.
+// J.lex_max_arcs of them: the lexicographic path (big_lex.cu) filters these.
 __device__ __forceinline__ bool lex_eligible(const ExpandJob &J, const BigItem &B) {
-    if (J.prev_sorted == nullptr || B.a1 - B.a0 > kBigLexMaxArcs) return false;
+    if (J.prev_sorted == nullptr || B.a1 - B.a0 > J.lex_max_arcs) return false;
     for (int32_t a = B.a0; a < B.a1; ++a)
         if (J.prev_sorted[J.arc_nbr[a] - J.prev_base] == 0) return false;
     return true;

@@ -1,7 +1,7 @@
 // Oversized destinations of three objectives, in lexicographic order.
 //
 // A destination too large for a tile (tile_resident()) whose arc runs all come from
-// frontiers kept in descending lexicographic order, at most kBigLexMaxArcs of them, is
+// frontiers kept in descending lexicographic order, at most ExpandJob::lex_max_arcs, is
 // filtered here instead of by big.cu's sort-filter-skyline or pivot/mark passes:
 //
 //   big_lex_rank_kernel:   thread per candidate of the scratch pass (the flat space of
@@ -16,11 +16,12 @@
 //       order by the rank kernel and sorted by ceil(log2(runs)) rounds that merge
 //       neighbouring groups of runs (thread per candidate, a binary search into the
 //       sibling group), alternating between the two scratch buffers;
-//   big_lex_seg_*_kernel:  the sorted candidates are walked with the staircase of
-//       stair.cuh in segments of kSeg, one warp each, the segments joined by prefix
-//       staircases, and the survivors written to the slot in order (so the destination's
-//       frontier is sorted, out_sorted = 1) -- work linear in the candidates instead of
-//       quadratic in what the pivots leave, spread over a warp per segment.
+//   big_lex_filter_kernel: one warp per destination walks the sorted candidates 32 at a
+//       time with the staircase of stair.cuh and writes the survivors to the slot in
+//       order (so the destination's frontier is sorted, out_sorted = 1) -- its work is
+//       linear in the candidates instead of quadratic in what the pivots leave.  If the
+//       staircase outgrows kStairBig entries the warp checks each remaining candidate
+//       against every point before it.
 //
 // Keep rule as everywhere (src/pmdd/enum/gpu/dominance_utils.cuh:10-23): of equal points
 // the first in the merged order stays.
@@ -165,259 +166,58 @@ __global__ void __launch_bounds__(kRankThreads) big_lex_merge_kernel(const Expan
     }
 }
 
-// ---------------------------------------------------------------- segmented filter
-// A destination's sorted candidates are cut into segments of kSeg.  A candidate is
-// dominated iff it is dominated within its segment or by the staircase of all earlier
-// segments, so:
-//   seg_local:  warp per segment walks it with a staircase from empty (local keep flags
-//               in big_idx) and stores the segment's final staircase SK_s;
-//   seg_prefix: warp per destination merges SK_0, SK_1, ... in order into the prefix
-//               staircases P_1, P_2, ... (P_s: everything before segment s);
-//   seg_final:  warp per segment drops its locally kept candidates that P_s dominates
-//               and counts the rest;
-//   seg_write:  warp per segment writes its survivors after those of earlier segments,
-//               so the destination's frontier comes out in order.
-// Scratch of a destination (pass offset soff, n candidates, S segments): keep flags
-// big_idx[soff + i]; big_surv_idx[soff + s*kSeg] = survivors of segment s, and for a
-// full segment t < S-1 also [+1] = |SK_t|, [+2] = |P_{t+1}|; big_surv_idx[soff + 3] = 1
-// when a staircase outgrew kStairBig (then one warp walks the whole destination, checking
-// every earlier candidate once the staircase is given up); segment t's 3*kSeg values of
-// big_surv hold SK_t and P_{t+1}.
-constexpr int kSeg = 1024;
-
 template <typename T>
-struct SegView {
-    const T *cand;   // sorted candidates, 3 values each
-    int32_t *flag;
-    int32_t *meta;
-    T *reg;          // segment t's region: reg + t * kSeg * 3
-    int64_t n;
-    int S;
-    __device__ T *sk1(int t) const { return reg + static_cast<int64_t>(t) * kSeg * 3; }
-    __device__ T *sk2(int t) const { return sk1(t) + kStairBig; }
-    __device__ T *p1(int t) const { return sk1(t) + 2 * kStairBig; }
-    __device__ T *p2(int t) const { return sk1(t) + 3 * kStairBig; }
-    __device__ bool overflow() const { return S > 1 && meta[3] != 0; }
-};
-
-template <typename T>
-__device__ __forceinline__ bool seg_view(const ExpandJob &J, const BigWork &W, int64_t pass, SegView<T> *v) {
-    BigItem B;
-    if (!J.lex_big || !big_item_any(J, W, pass, &B) || !lex_eligible(J, B)) return false;
-    v->cand = static_cast<const T *>(lex_merge_rounds(B.a1 - B.a0) & 1 ? J.big_pts2 : J.big_pts) + B.soff * 3;
-    v->flag = J.big_idx + B.soff;
-    v->meta = J.big_surv_idx + B.soff;
-    v->reg = static_cast<T *>(J.big_surv) + B.soff * 3;
-    v->n = B.n;
-    v->S = static_cast<int>((B.n + kSeg - 1) / kSeg);
-    return true;
-}
-
-// One warp: candidates [b, e) against the points before them in [lo, e) (pairwise).
-template <typename T>
-__device__ void pairwise_walk(const T *cand, int32_t *flag, int64_t lo, int64_t b, int64_t e, int lane) {
-    for (int64_t c0 = b; c0 < e; c0 += 32) {
-        const int64_t p = c0 + lane;
-        const bool valid = p < e;
-        T q1 = 0, q2 = 0;
-        if (valid) {
-            q1 = cand[p * 3 + 1];
-            q2 = cand[p * 3 + 2];
-        }
-        bool dom = !valid;
-        const int64_t hi = min(e, c0 + 32) - 1;
-        for (int64_t j = lo; j < hi; ++j) {
-            if (j < p) dom |= (cand[j * 3 + 1] >= q1) & (cand[j * 3 + 2] >= q2);
-            if (((j - lo) & 31) == 31 && __all_sync(kAll, dom)) break;
-        }
-        if (valid) flag[p] = dom ? 0 : 1;
-    }
-}
-
-// One warp: candidates [b, e) with a staircase from empty (keep flags); returns false if
-// the staircase outgrew kStairBig (the rest of [b, e) is then checked pairwise against
-// [b, e)).  `keep_last` keeps the staircase after the last chunk.
-template <typename T>
-__device__ bool stair_walk(const T *cand, int32_t *flag, int64_t b, int64_t e, bool keep_last,
-                           StairBuf<T, kStairBig> &buf, StairState &st, int lane) {
-    for (int64_t c0 = b; c0 < e; c0 += 32) {
-        const int64_t p = c0 + lane;
-        const bool valid = p < e;
-        if (st.overflow) {
-            pairwise_walk<T>(cand, flag, b, c0, e, lane);
-            return false;
-        }
-        T q1 = 0, q2 = 0;
-        if (valid) {
-            q1 = cand[p * 3 + 1];
-            q2 = cand[p * 3 + 2];
-        }
-        const bool dom = stair_chunk<T, kStairBig>(buf, st, valid, q1, q2, keep_last || c0 + 32 < e);
-        if (valid) flag[p] = dom ? 0 : 1;
-    }
-    return !st.overflow;
-}
-
-template <typename T>
-__global__ void __launch_bounds__(FilterCfg<T>::kThreads) big_lex_seg_local_kernel(const ExpandJob *__restrict__ jobs,
-                                                                                   const BigWork *__restrict__ work,
-                                                                                   int64_t pass) {
-    constexpr int NW = FilterCfg<T>::kWarps;
-    __shared__ StairBuf<T, kStairBig> bufs[NW];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const BigWork W = work[blockIdx.x];
-    SegView<T> v;
-    if (!seg_view<T>(jobs[W.job], W, pass, &v)) return;
-    const int s = blockIdx.y * NW + warp;
-    if (s >= v.S) return;
-    const int64_t b = static_cast<int64_t>(s) * kSeg, e = min(v.n, b + kSeg);
-    StairState st;
-    const bool ok = stair_walk<T>(v.cand, v.flag, b, e, s < v.S - 1, bufs[warp], st, lane);
-    if (s < v.S - 1) {
-        if (!ok) {
-            if (lane == 0) v.meta[3] = 1;
-            return;
-        }
-        for (int i = lane; i < st.m; i += 32) {
-            v.sk1(s)[i] = bufs[warp].v1[st.cur][i];
-            v.sk2(s)[i] = bufs[warp].v2[st.cur][i];
-        }
-        if (lane == 0) v.meta[static_cast<int64_t>(s) * kSeg + 1] = st.m;
-    }
-}
-
-template <typename T>
-__global__ void __launch_bounds__(FilterCfg<T>::kThreads) big_lex_seg_prefix_kernel(const ExpandJob *__restrict__ jobs,
-                                                                                    const BigWork *__restrict__ work,
-                                                                                    int num_work, int64_t pass) {
-    constexpr int NW = FilterCfg<T>::kWarps;
-    __shared__ StairBuf<T, kStairBig> bufs[NW];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int wi = blockIdx.x * NW + warp;
-    if (wi >= num_work) return;
-    const BigWork W = work[wi];
-    SegView<T> v;
-    if (!seg_view<T>(jobs[W.job], W, pass, &v) || v.S <= 1 || v.overflow()) return;
-    StairState P;  // the staircase of everything before the next segment
-    for (int t = 0; t + 1 < v.S; ++t) {
-        const int m = v.meta[static_cast<int64_t>(t) * kSeg + 1];
-        for (int c0 = 0; c0 < m; c0 += 32) {
-            const bool valid = c0 + lane < m;
-            T e1 = 0, e2 = 0;
-            if (valid) {
-                e1 = v.sk1(t)[c0 + lane];
-                e2 = v.sk2(t)[c0 + lane];
-            }
-            (void)stair_chunk<T, kStairBig>(bufs[warp], P, valid, e1, e2, true);
-            if (P.overflow) {
-                if (lane == 0) v.meta[3] = 1;
-                return;
-            }
-        }
-        for (int i = lane; i < P.m; i += 32) {
-            v.p1(t)[i] = bufs[warp].v1[P.cur][i];
-            v.p2(t)[i] = bufs[warp].v2[P.cur][i];
-        }
-        if (lane == 0) v.meta[static_cast<int64_t>(t) * kSeg + 2] = P.m;
-    }
-}
-
-template <typename T>
-__global__ void __launch_bounds__(FilterCfg<T>::kThreads) big_lex_seg_final_kernel(const ExpandJob *__restrict__ jobs,
-                                                                                   const BigWork *__restrict__ work,
-                                                                                   int64_t pass) {
-    constexpr int NW = FilterCfg<T>::kWarps;
-    __shared__ StairBuf<T, kStairBig> bufs[NW];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const BigWork W = work[blockIdx.x];
-    SegView<T> v;
-    if (!seg_view<T>(jobs[W.job], W, pass, &v)) return;
-    const int s = blockIdx.y * NW + warp;
-    if (s >= v.S) return;
-    if (v.overflow()) {
-        // a staircase outgrew its buffer: one warp walks the whole destination again
-        if (s != 0) return;
-        StairState st;
-        (void)stair_walk<T>(v.cand, v.flag, 0, v.n, false, bufs[warp], st, lane);
-        for (int t = 0; t < v.S; ++t) {
-            const int64_t b = static_cast<int64_t>(t) * kSeg, e = min(v.n, b + kSeg);
-            int cnt = 0;
-            for (int64_t c0 = b; c0 < e; c0 += 32)
-                cnt += __popc(__ballot_sync(kAll, c0 + lane < e && v.flag[c0 + lane] != 0));
-            if (lane == 0) v.meta[b] = cnt;
-        }
-        return;
-    }
-    const int64_t b = static_cast<int64_t>(s) * kSeg, e = min(v.n, b + kSeg);
-    int m = 0;
-    if (s > 0) {  // P_s, kept in the region of segment s-1
-        m = v.meta[static_cast<int64_t>(s - 1) * kSeg + 2];
-        for (int i = lane; i < m; i += 32) {
-            bufs[warp].v1[0][i] = v.p1(s - 1)[i];
-            bufs[warp].v2[0][i] = v.p2(s - 1)[i];
-        }
-        __syncwarp();
-    }
-    int cnt = 0;
-    for (int64_t c0 = b; c0 < e; c0 += 32) {
-        const int64_t p = c0 + lane;
-        bool keep = p < e && v.flag[p] != 0;
-        if (keep && m > 0) {
-            const T q1 = v.cand[p * 3 + 1], q2 = v.cand[p * 3 + 2];
-            int lo = 0, hi = m;  // entries with objective 1 >= q1
-            while (lo < hi) {
-                const int mid = (lo + hi) >> 1;
-                if (bufs[warp].v1[0][mid] >= q1) lo = mid + 1;
-                else hi = mid;
-            }
-            if (lo > 0 && bufs[warp].v2[0][lo - 1] >= q2) {
-                keep = false;
-                v.flag[p] = 0;
-            }
-        }
-        cnt += __popc(__ballot_sync(kAll, keep));
-    }
-    if (lane == 0) v.meta[b] = cnt;
-}
-
-template <typename T>
-__global__ void __launch_bounds__(FilterCfg<T>::kThreads) big_lex_seg_write_kernel(const ExpandJob *__restrict__ jobs,
-                                                                                   const BigWork *__restrict__ work,
-                                                                                   int64_t pass) {
-    constexpr int NW = FilterCfg<T>::kWarps;
+__global__ void __launch_bounds__(FilterCfg<T>::kThreads) big_lex_filter_kernel(const ExpandJob *__restrict__ jobs,
+                                                                                const BigWork *__restrict__ work,
+                                                                                int num_work, int64_t pass) {
+    constexpr int kFilterWarps = FilterCfg<T>::kWarps;
+    __shared__ StairBuf<T, kStairBig> bufs[kFilterWarps];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned lt_mask = (1u << lane) - 1u;
-    const BigWork W = work[blockIdx.x];
-    const ExpandJob &J = jobs[W.job];
-    SegView<T> v;
-    if (!seg_view<T>(J, W, pass, &v)) return;
-    const int s = blockIdx.y * NW + warp;
-    if (s >= v.S) return;
-    int64_t before = 0;  // survivors of the earlier segments
-    for (int t = lane; t < s; t += 32) before += v.meta[static_cast<int64_t>(t) * kSeg];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) before += __shfl_xor_sync(kAll, before, o);
-    BigItem B;
-    fill_item(J, W.big, pass * J.big_window, &B);
-    T *out = static_cast<T *>(J.out_pts) + B.c0 * 3;
-    const int64_t b = static_cast<int64_t>(s) * kSeg, e = min(v.n, b + kSeg);
-    int64_t kept = before;
-    for (int64_t c0 = b; c0 < e; c0 += 32) {
-        const int64_t p = c0 + lane;
-        const bool keep = p < e && v.flag[p] != 0;
-        const unsigned k = __ballot_sync(kAll, keep);
-        if (keep) {
-            T *o = out + (kept + __popc(k & lt_mask)) * 3;
-            o[0] = v.cand[p * 3];
-            o[1] = v.cand[p * 3 + 1];
-            o[2] = v.cand[p * 3 + 2];
+    for (int wi = blockIdx.x * kFilterWarps + warp; wi < num_work; wi += gridDim.x * kFilterWarps) {
+        const BigWork W = work[wi];
+        const ExpandJob &J = jobs[W.job];
+        BigItem B;
+        if (!J.lex_big || !big_item_any(J, W, pass, &B) || !lex_eligible(J, B)) continue;
+        // sorted candidates: big_pts after an even number of merge rounds, else big_pts2
+        const T *cand = static_cast<const T *>(lex_merge_rounds(B.a1 - B.a0) & 1 ? J.big_pts2 : J.big_pts) + B.soff * 3;
+        T *out = static_cast<T *>(J.out_pts) + B.c0 * 3;
+        StairState st;
+        int64_t kept = 0;
+        for (int64_t c0 = 0; c0 < B.n; c0 += 32) {
+            const int64_t p = c0 + lane;
+            const bool valid = p < B.n;
+            T q0 = 0, q1 = 0, q2 = 0;
+            if (valid) {
+                q0 = cand[p * 3];
+                q1 = cand[p * 3 + 1];
+                q2 = cand[p * 3 + 2];
+            }
+            bool dom = !valid;
+            if (st.overflow) {
+                // staircase given up: every candidate before p, chunk-mates included
+                const int64_t hi = min(B.n, c0 + 32) - 1;
+                for (int64_t j = 0; j < hi; ++j) {
+                    if (j < p) dom |= (cand[j * 3 + 1] >= q1) & (cand[j * 3 + 2] >= q2);
+                    if ((j & 31) == 31 && __all_sync(kAll, dom)) break;
+                }
+            } else {
+                dom = stair_chunk<T, kStairBig>(bufs[warp], st, valid, q1, q2, c0 + 32 < B.n);
+            }
+            const unsigned keep = __ballot_sync(kAll, !dom);
+            if (!dom) {
+                T *o = out + (kept + __popc(keep & lt_mask)) * 3;
+                o[0] = q0;
+                o[1] = q1;
+                o[2] = q2;
+            }
+            kept += __popc(keep);
         }
-        kept += __popc(k);
-    }
-    if (s == v.S - 1 && lane == 0) {
-        J.out_size[B.item] = static_cast<int32_t>(kept);
-        if (J.out_sorted) J.out_sorted[B.item] = 1;
-        if (J.tile_surv) atomicAdd(J.tile_surv + 1, static_cast<unsigned long long>(v.n));
+        if (lane == 0) {
+            J.out_size[B.item] = static_cast<int32_t>(kept);
+            if (J.out_sorted) J.out_sorted[B.item] = 1;
+            if (J.tile_surv) atomicAdd(J.tile_surv + 1, static_cast<unsigned long long>(B.n));
+        }
     }
 }
 
@@ -432,14 +232,9 @@ cudaError_t launch_big_lex_rank(bool wide, const BigLaunch &L, cudaStream_t stre
 template <typename T>
 static cudaError_t launch_filter_t(const BigLaunch &L, cudaStream_t stream) {
     using Cfg = FilterCfg<T>;
-    if (L.num_work <= 0) return cudaSuccess;
-    const int64_t max_seg = std::max<int64_t>(1, (L.max_n + kSeg - 1) / kSeg);
-    const dim3 grid(static_cast<unsigned>(L.num_work), static_cast<unsigned>((max_seg + Cfg::kWarps - 1) / Cfg::kWarps));
-    const unsigned pgrid = static_cast<unsigned>((L.num_work + Cfg::kWarps - 1) / Cfg::kWarps);
-    big_lex_seg_local_kernel<T><<<grid, Cfg::kThreads, 0, stream>>>(L.jobs, L.work, L.pass);
-    big_lex_seg_prefix_kernel<T><<<pgrid, Cfg::kThreads, 0, stream>>>(L.jobs, L.work, L.num_work, L.pass);
-    big_lex_seg_final_kernel<T><<<grid, Cfg::kThreads, 0, stream>>>(L.jobs, L.work, L.pass);
-    big_lex_seg_write_kernel<T><<<grid, Cfg::kThreads, 0, stream>>>(L.jobs, L.work, L.pass);
+    const unsigned grid = static_cast<unsigned>(
+        std::max<int64_t>(1, std::min<int64_t>((L.num_work + Cfg::kWarps - 1) / Cfg::kWarps, int64_t(L.sms) * 16)));
+    big_lex_filter_kernel<T><<<grid, Cfg::kThreads, 0, stream>>>(L.jobs, L.work, L.num_work, L.pass);
     return cudaGetLastError();
 }
 

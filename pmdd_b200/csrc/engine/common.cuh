@@ -53,7 +53,7 @@ __host__ __device__ constexpr bool tile_resident(int64_t candidates, int64_t arc
 // Oversized three-objective destinations in lexicographic order (big_lex.cu): up to
 // kBigDirectArcs runs each candidate is ranked against the other runs directly; beyond,
 // ceil(log2(runs)) merge rounds of neighbouring run groups sort the destination; more
-// than kBigLexMaxArcs runs take the pivot/mark path instead.
+// than ExpandJob::lex_max_arcs (at most kBigLexMaxArcs) runs take the pivot/mark path.
 constexpr int kBigDirectArcs = 16;
 constexpr int kBigLexMaxArcs = 4096;
 __host__ __device__ inline int lex_merge_rounds(int arcs) {
@@ -121,7 +121,8 @@ struct ExpandJob {
                                    // candidates are checked pairwise, larger ones by a staircase warp
     int32_t lex_big;               // 1: oversized destinations with sorted runs take big_lex.cu
     int32_t lex_bulk;              // 1: lexicographic tiles stage parent runs by bulk copies
-    int32_t pad2;
+    int32_t lex_max_arcs;          // oversized destinations of at most this many runs (and at
+                                   // most kBigLexMaxArcs) take big_lex.cu
     unsigned long long *phase_clk; // diagnostic: cycles per tile phase (lexicographic tiles), or nullptr
 };
 

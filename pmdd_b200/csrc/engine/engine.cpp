@@ -578,6 +578,8 @@ Engine::Engine(int device, int64_t budget_bytes, int max_slots) : device_(device
     if (lx && lx[0] == '0') lex_tiles_ = false;
     const char *lb = std::getenv("PMDD_LEX_BULK");
     if (lb && *lb) lex_bulk_ = lb[0] == '1';
+    const char *la = std::getenv("PMDD_BIG_LEX_MAX_ARCS");
+    if (la && *la) lex_max_arcs_ = std::max(0, std::min(std::atoi(la), dev::kBigLexMaxArcs));
     const char *pm = std::getenv("PMDD_LEX_PAIR_MAX");
     if (pm && *pm && std::atoi(pm) >= 0) lex_pair_max_fixed_ = std::atoi(pm);
     ok_ = true;
@@ -1098,7 +1100,7 @@ int Engine::step() {
         std::vector<ExpPlan> ordered;
         ordered.reserve(exps.size());
         for (auto &g : groups) {
-            GroupLaunch gl{g.first.first, g.first.second, pos, g.second.size(), 0, bigwork.size(), 0, 0, 0, 0, 0, 0};
+            GroupLaunch gl{g.first.first, g.first.second, pos, g.second.size(), 0, bigwork.size(), 0, 0, 0, 0, 0, 0, 0};
             for (size_t idx : g.second) {
                 const ExpPlan &e = exps[idx];
                 Instance &I = *e.I;
@@ -1136,6 +1138,7 @@ int Engine::step() {
                 J.pair_max = pair_max_for(I.d, I.opts.problem_type);
                 J.lex_big = (I.d == 3 && lex_tiles_) ? 1 : 0;
                 J.lex_bulk = lex_bulk_ ? 1 : 0;
+                J.lex_max_arcs = lex_max_arcs_;
                 J.tile_base = gl.tiles;
                 tile_bases[pos] = gl.tiles;
                 item_bases[pos] = gl.items;
@@ -1259,7 +1262,7 @@ int Engine::step() {
     const size_t f_sd = f_ts + 2 * sizeof(unsigned long long) * exps.size();  // (survivors, staircase) per expansion
     const size_t f_err = f_sd + sizeof(int64_t) * sdjobs.size();
     const size_t f_clk = f_err + sizeof(uint64_t);  // PMDD_TRACE: tile phase cycles (8 counters)
-    const size_t f_total = f_clk + (trace_ ? 8 * sizeof(unsigned long long) : 0);
+    const size_t f_total = f_clk + (trace_ ? 10 * sizeof(unsigned long long) : 0);
     char *d_fixed = static_cast<char *>(scratch(f_total));
     dev::CountResult *d_results = counts.empty() ? nullptr : reinterpret_cast<dev::CountResult *>(d_fixed);
     unsigned long long *d_tile_surv = d_fixed ? reinterpret_cast<unsigned long long *>(d_fixed + f_ts) : nullptr;
@@ -1551,8 +1554,7 @@ int Engine::step() {
         L.sms = sms_;
         L.with_sfs = true;
         L.lex_big = gl.d == 3 && lex_tiles_;
-        L.max_n = gl.max_big;
-        L.lex_rounds = L.lex_big ? dev::lex_merge_rounds(std::min(gl.max_big_arcs, dev::kBigLexMaxArcs)) : 0;
+        L.lex_rounds = L.lex_big ? dev::lex_merge_rounds(std::min(gl.max_big_arcs, lex_max_arcs_)) : 0;
         L.mark_cap = static_cast<int>(std::min<int64_t>(gl.mark_cap, static_cast<int64_t>(gl.big_count)));
         L.plan = nullptr;
         // more SFS blocks than fit the SMs at once: start the largest destinations first
@@ -1562,7 +1564,7 @@ int Engine::step() {
         for (int64_t pass = 0; pass < gl.big_passes; ++pass) {
             L.pass = pass;
             if (!cuda_ok(dev::launch_big(gl.d, gl.wide, L, stream_), "oversized-destination kernels")) return -1;
-            launches_ += (L.mark_cap > 0 ? 9 : 2) + (ordered ? 1 : 0) + (L.lex_big ? 4 + L.lex_rounds : 0);
+            launches_ += (L.mark_cap > 0 ? 9 : 2) + (ordered ? 1 : 0) + (L.lex_big ? 1 + L.lex_rounds : 0);
         }
     }
     if (!sdjobs.empty()) {
@@ -1653,12 +1655,13 @@ int Engine::step() {
         std::fprintf(stderr,
                      "[pmdd step] jobs=%zu counts=%zu couple=%zu cand=%lld big_items=%lld big_cand=%lld max_item=%lld "
                      "tile_cand=%lld tile_surv=%llu tiles_ms=%.3f big_ms=%.3f rest_ms=%.3f host_to_sync_us=%.1f "
-                     "arena_reserved_mb=%.0f arena_grow_ms=%.1f phase_mcyc=%.2f,%.2f,%.2f,%.2f,%.2f,%.2f,%.2f\n",
+                     "arena_reserved_mb=%.0f arena_grow_ms=%.1f phase_mcyc=%.2f,%.2f,%.2f,%.2f,%.2f,%.2f,%.2f warp_mcyc=%.2f,%.2f\n",
                      exps.size(), counts.size(), ujobs.size(), static_cast<long long>(cand),
                      static_cast<long long>(nbig), static_cast<long long>(big_cand), static_cast<long long>(max_item),
                      static_cast<long long>(cand - big_cand), tile_surv, ms_expand, ms_big, ms_rest,
                      (now_s() - step_t0) * 1e6, arena_.reserved() / 1e6, arena_.grow_seconds() * 1e3,
-                     pc[0] * 1e-6, pc[1] * 1e-6, pc[2] * 1e-6, pc[3] * 1e-6, pc[4] * 1e-6, pc[5] * 1e-6, pc[6] * 1e-6);
+                     pc[0] * 1e-6, pc[1] * 1e-6, pc[2] * 1e-6, pc[3] * 1e-6, pc[4] * 1e-6, pc[5] * 1e-6, pc[6] * 1e-6,
+                     pc[7] * 1e-6, pc[8] * 1e-6);
     }
     for (void *q : step_scratch_) arena_.release(q);
     step_scratch_.clear();

@@ -326,6 +326,11 @@ class Engine {
     // Lexicographic tiles stage each arc's parent run into shared memory with one bulk copy
     // (cp.async.bulk on an mbarrier) instead of per-thread loads: PMDD_LEX_BULK=1 / 0.
     bool lex_bulk_ = false;
+    // Oversized three-objective destinations of at most this many arc runs, all from
+    // sorted frontiers, take the lexicographic path (big_lex.cu); the others the
+    // SFS / pivot-mark passes.  PMDD_BIG_LEX_MAX_ARCS, 0 .. kBigLexMaxArcs.
+    static constexpr int32_t kDefaultLexMaxArcs = 16;
+    int32_t lex_max_arcs_ = kDefaultLexMaxArcs;
     int32_t lex_pair_max_fixed_ = -1;
     std::map<std::pair<int, int>, int64_t> tuned_pair_max_;
     int32_t pair_max_for(int d, int problem_type) const;

@@ -35,7 +35,6 @@ struct BigLaunch {
     int32_t *order;              // num_work ints: SFS blocks largest destination first; nullptr: list order
     bool lex_big;                // three objectives: destinations with sorted runs take big_lex.cu
     int lex_rounds;              // merge rounds the destinations with the most runs need
-    int64_t max_n;               // candidates of the largest oversized destination
 };
 // Most oversized destinations whose SFS blocks are put in size order (one block sorts them).
 constexpr int kBigOrderMax = 4096;

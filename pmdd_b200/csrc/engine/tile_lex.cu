@@ -50,6 +50,10 @@ namespace {
 constexpr int kLT = kTileThreads;
 constexpr int kLexWarps = kLT / 32;
 constexpr int kStairCap = 64;      // staircase entries a warp keeps; beyond it: pairwise
+// Destinations walked by staircase warps are split into segments of at most kLexSeg
+// candidates, one warp each; a segment's staircase never outgrows kStairCap.
+constexpr int kLexSeg = 64;
+constexpr int kLexSlots = kTileCap / kLexSeg;  // staircases kept for the segments after them
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kWaitIters = 1 << 22;  // bulk-copy barrier: try_wait rounds before giving up
 
@@ -66,7 +70,9 @@ struct LexSmem {
     int32_t item_a0g[kTileItemCap];      // staged destination -> first arc (global id)
     int64_t item_c0[kTileItemCap];       // staged destination -> job-local candidate start
     uint8_t item_count[kTileItemCap];    // 1: merge by counting
-    int16_t big[kTileItemCap];           // destinations filtered by a staircase warp
+    int32_t big[kTileItemCap + kLexSlots];  // staircase segments: destination | segment << 16
+    int8_t item_slot0[kTileItemCap];     // segmented destination -> slot of its first segment
+    int16_t slot_m[kLexSlots];           // entries of each kept staircase (-1: not kept)
     int16_t arc_pos[kTileArcCap + 1];    // staged arc -> first candidate position
     int16_t arc_item[kTileArcCap];       // staged arc -> staged destination
     int32_t arc_w[kTileArcCap];          // staged arc -> weight row
@@ -75,7 +81,7 @@ struct LexSmem {
     uint64_t bar;                        // bulk staging barrier
     int32_t warp_i[32];
     int32_t tot_i, tot_a, i0, i1, job;
-    int32_t n_big, next_big, next_chunk, tot_stage;
+    int32_t n_big, next_big, next_chunk, tot_stage, n_slot;
 };
 
 // Phase clock (J.phase_clk, a diagnostic): thread 0 adds the cycles its block spent in
@@ -96,9 +102,18 @@ struct PhaseClock {
     }
 };
 
-// Per-warp staircase storage, laid over pts once the merge has read it.
+// Per-warp staircase storage, laid over pts once the merge has read it, followed by the
+// final staircases of the segments that later segments are checked against.
 template <typename T>
 using Stair = StairBuf<T, kStairCap>;
+template <typename T>
+struct SegStair {
+    T v1[kStairCap];  // objective 1, descending
+    T v2[kStairCap];  // objective 2, ascending
+};
+
+// Segments of a destination of c candidates walked by staircase warps (c > pair_max).
+__device__ __forceinline__ int lex_segments(int c) { return (c + kLexSeg - 1) / kLexSeg; }
 
 // Largest x over the threads before this one (-1 for thread 0); every thread calls it.
 template <int THREADS>
@@ -144,9 +159,12 @@ __device__ __forceinline__ bool lex_eq(const PackedPt<3, T> &a, const PackedPt<3
     return a.v[0] == b.v[0] && a.v[1] == b.v[1] && a.v[2] == b.v[2];
 }
 
-// Candidates of one big destination, merged positions [s, e), walked by one warp.
+// Candidates at merged positions [s, e) (one segment of a destination) walked by one
+// warp from an empty staircase; with `save` the final staircase is kept there (its entry
+// count in *save_m, -1 if it outgrew kStairCap).
 template <typename T>
-__device__ void stair_filter(LexSmem<T> &S, Stair<T> &sb, int s, int e, int lane) {
+__device__ void stair_filter(LexSmem<T> &S, Stair<T> &sb, int s, int e, int lane, SegStair<T> *save,
+                             int16_t *save_m) {
     StairState st;
     for (int c0 = s; c0 < e; c0 += 32) {
         const int p = c0 + lane;
@@ -166,9 +184,16 @@ __device__ void stair_filter(LexSmem<T> &S, Stair<T> &sb, int s, int e, int lane
                 if (((j - s) & 15) == 15 && __all_sync(kFull, dom)) break;
             }
         } else {
-            dom = stair_chunk<T, kStairCap>(sb, st, valid, q1, q2, c0 + 32 < e);
+            dom = stair_chunk<T, kStairCap>(sb, st, valid, q1, q2, save != nullptr || c0 + 32 < e);
         }
         if (valid) S.keep[p] = dom ? 0 : 1;
+    }
+    if (save != nullptr) {
+        for (int i = lane; i < st.m && !st.overflow; i += 32) {
+            save->v1[i] = sb.v1[st.cur][i];
+            save->v2[i] = sb.v2[st.cur][i];
+        }
+        if (lane == 0) *save_m = st.overflow ? -1 : static_cast<int16_t>(st.m);
     }
 }
 
@@ -181,6 +206,7 @@ __global__ void __launch_bounds__(kLT) expand_tile_lex_kernel(const ExpandJob *_
     extern __shared__ __align__(16) unsigned char smem_raw[];
     LexSmem<T> &S = *reinterpret_cast<LexSmem<T> *>(smem_raw);
     Stair<T> *stairs = reinterpret_cast<Stair<T> *>(&S.pts[0]);
+    SegStair<T> *slots = reinterpret_cast<SegStair<T> *>(stairs + kLexWarps);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     unsigned bar_phase = 0;
     bool aborted = false;
@@ -279,6 +305,7 @@ __global__ void __launch_bounds__(kLT) expand_tile_lex_kernel(const ExpandJob *_
                 S.n_big = 0;
                 S.next_big = 0;
                 S.next_chunk = 0;
+                S.n_slot = 0;
             }
             __syncthreads();
             const int32_t total = S.tot_i, total_a = S.tot_a;
@@ -451,28 +478,41 @@ __global__ void __launch_bounds__(kLT) expand_tile_lex_kernel(const ExpandJob *_
                 }
                 S.mpts[js + rank] = me;
             }
-            // destinations for the staircase warps, largest first in three tiers
+            // segments for the staircase warps, those of the largest destinations first (three
+            // tiers); a destination of more than kLexSeg candidates gets one slot per segment
+            // but its last for the staircases the later segments are checked against
             for (int tier = 0; tier < 3; ++tier) {
                 const int lo_c = tier == 0 ? 512 : (tier == 1 ? 128 : pair_max);
                 const int hi_c = tier == 0 ? kTileCap : (tier == 1 ? 512 : 128);
                 for (int k = tid; k < n_it; k += kLT) {
                     const int c = S.item_s[k + 1] - S.item_s[k];
-                    if (c > lo_c && c <= hi_c && c > pair_max) S.big[atomicAdd(&S.n_big, 1)] = static_cast<int16_t>(k);
+                    if (c > lo_c && c <= hi_c && c > pair_max) {
+                        const int nseg = lex_segments(c);
+                        const int at = atomicAdd(&S.n_big, nseg);
+                        for (int g = 0; g < nseg; ++g) S.big[at + g] = k | (g << 16);
+                        if (nseg > 1) S.item_slot0[k] = static_cast<int8_t>(atomicAdd(&S.n_slot, nseg - 1));
+                    }
                 }
                 __syncthreads();
             }
             clk.lap(4);
-            // --- filter, big destinations: one staircase warp each
+            // --- filter, big destinations: one staircase warp per segment
+            const long long f0 = (J.phase_clk && lane == 0) ? clock64() : 0;
             while (true) {
                 int b = 0;
                 if (lane == 0) b = atomicAdd(&S.next_big, 1);
                 b = __shfl_sync(kFull, b, 0);
                 if (b >= S.n_big) break;
-                const int k = S.big[b];
-                if (lane == 0 && J.tile_surv != nullptr)
-                    atomicAdd(J.tile_surv + 1, static_cast<unsigned long long>(S.item_s[k + 1] - S.item_s[k]));
-                stair_filter<T>(S, stairs[warp], S.item_s[k], S.item_s[k + 1], lane);
+                const int k = S.big[b] & 0xffff, g = S.big[b] >> 16;
+                const int js = S.item_s[k], c = S.item_s[k + 1] - js;
+                const int nseg = lex_segments(c), len = (c + nseg - 1) / nseg;
+                if (g == 0 && lane == 0 && J.tile_surv != nullptr)
+                    atomicAdd(J.tile_surv + 1, static_cast<unsigned long long>(c));
+                const int slot = g + 1 < nseg ? S.item_slot0[k] + g : -1;
+                stair_filter<T>(S, stairs[warp], js + g * len, js + min(c, (g + 1) * len), lane,
+                                slot >= 0 ? slots + slot : nullptr, slot >= 0 ? S.slot_m + slot : nullptr);
             }
+            const long long f1 = (J.phase_clk && lane == 0) ? clock64() : 0;
             // --- filter, small destinations: every candidate against the points before it
             while (true) {
                 int c0 = 0;
@@ -507,7 +547,45 @@ __global__ void __launch_bounds__(kLT) expand_tile_lex_kernel(const ExpandJob *_
                 }
                 if (mine) S.keep[q] = dom ? 0 : 1;
             }
+            if (J.phase_clk && lane == 0) {  // warp busy cycles: staircase loop, pairwise loop
+                const long long f2 = clock64();
+                atomicAdd(J.phase_clk + 7, static_cast<unsigned long long>(f1 - f0));
+                atomicAdd(J.phase_clk + 8, static_cast<unsigned long long>(f2 - f1));
+            }
             __syncthreads();
+            // --- filter, segmented destinations: a survivor of its own segment is checked
+            // against the staircases of the segments before it (every point of a segment is
+            // covered by an entry of its staircase), or their points if a staircase was not kept
+            if (S.n_slot > 0) {
+                for (int q = tid; q < total; q += kLT) {
+                    if (!S.keep[q]) continue;
+                    const int k = S.item_of[q];
+                    const int js = S.item_s[k], c = S.item_s[k + 1] - js;
+                    if (c <= pair_max || c <= kLexSeg) continue;
+                    const int nseg = lex_segments(c), len = (c + nseg - 1) / nseg;
+                    const int g = (q - js) / len;
+                    const T q1 = S.mpts[q].v[1], q2 = S.mpts[q].v[2];
+                    bool dom = false;
+                    for (int t = 0; t < g && !dom; ++t) {
+                        const int slot = S.item_slot0[k] + t;
+                        const int m = S.slot_m[slot];
+                        if (m >= 0) {
+                            int a = 0, b = m;  // entries with objective 1 >= q1
+                            while (a < b) {
+                                const int mid = (a + b) >> 1;
+                                if (slots[slot].v1[mid] >= q1) a = mid + 1;
+                                else b = mid;
+                            }
+                            dom = a > 0 && slots[slot].v2[a - 1] >= q2;
+                        } else {
+                            for (int j = js + t * len; j < js + (t + 1) * len && !dom; ++j)
+                                dom = (S.mpts[j].v[1] >= q1) & (S.mpts[j].v[2] >= q2);
+                        }
+                    }
+                    if (dom) S.keep[q] = 0;
+                }
+                __syncthreads();
+            }
             clk.lap(5);
             // --- exclusive scan of keep flags (merged order)
             constexpr int QPER = kTileCap / kLT;
@@ -560,7 +638,8 @@ namespace {
 template <typename T>
 cudaError_t launch_lex_t(const ExpandJob *jobs, const int64_t *tile_bases, int num_jobs, int64_t total_tiles, int grid,
                          cudaStream_t stream) {
-    static_assert(sizeof(Stair<T>) * kLexWarps <= sizeof(PackedPt<3, T>) * kTileCap, "staircases fit over pts");
+    static_assert(sizeof(Stair<T>) * kLexWarps + sizeof(SegStair<T>) * kLexSlots <= sizeof(PackedPt<3, T>) * kTileCap,
+                  "staircases fit over pts");
     const size_t smem = sizeof(LexSmem<T>);
     const cudaError_t e = ensure_smem_limit(reinterpret_cast<const void *>(expand_tile_lex_kernel<T>), smem);
     if (e != cudaSuccess) return e;

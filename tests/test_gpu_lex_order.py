@@ -8,7 +8,9 @@
 * Both ends of the pairwise / staircase crossover (PMDD_LEX_PAIR_MAX 0: every
   destination by a staircase warp; 1024: every destination pairwise), the parent runs
   staged by bulk copies or loaded directly (PMDD_LEX_BULK 1 / 0), and the pairwise tile
-  kernel (PMDD_LEX_TILES=0) stay exact on the golden fixtures and seeded instances.  The
+  kernel (PMDD_LEX_TILES=0) stay exact on the golden fixtures and seeded instances, and
+  so do oversized destinations of up to 4096 runs sorted by merge rounds
+  (PMDD_BIG_LEX_MAX_ARCS=4096) or none of them on the lexicographic path (0).  The
   engine reads these settings at start-up, so each runs in a child process.
 """
 import json
@@ -79,13 +81,15 @@ print(json.dumps({{"checked": n}}))
 
 
 @pytest.mark.parametrize("env", [{"PMDD_LEX_PAIR_MAX": "0"}, {"PMDD_LEX_PAIR_MAX": "1024"}, {"PMDD_LEX_TILES": "0"},
-                                 {"PMDD_LEX_BULK": "1"}, {"PMDD_LEX_BULK": "0"}],
-                         ids=["all-staircase", "all-pairwise", "pairwise-kernel", "bulk-staging", "direct-loads"])
+                                 {"PMDD_LEX_BULK": "1"}, {"PMDD_LEX_BULK": "0"}, {"PMDD_BIG_LEX_MAX_ARCS": "4096"},
+                                 {"PMDD_BIG_LEX_MAX_ARCS": "0"}],
+                         ids=["all-staircase", "all-pairwise", "pairwise-kernel", "bulk-staging", "direct-loads",
+                              "merge-rounds", "no-oversized-lex"])
 def test_filter_paths_stay_exact(env):
     from conftest import ROOT
 
     e = dict(os.environ)
-    for k in ("PMDD_LEX_PAIR_MAX", "PMDD_LEX_TILES", "PMDD_LEX_BULK"):
+    for k in ("PMDD_LEX_PAIR_MAX", "PMDD_LEX_TILES", "PMDD_LEX_BULK", "PMDD_BIG_LEX_MAX_ARCS"):
         e.pop(k, None)
     e.update(env)
     p = subprocess.run([sys.executable, "-c", CHILD.format(root=ROOT, tests=os.path.join(ROOT, "tests"))], env=e,

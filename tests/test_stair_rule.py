@@ -8,7 +8,9 @@ computes (asserting the staircase stays strictly ordered and no two entries coll
 Its keep flags must give the oracle's frontier (the reference GPU filter's keep rule,
 src/pmdd/enum/gpu/dominance_utils.cuh:10-23) on seeded sets with duplicates, with
 anti-correlated objectives, and with a staircase capacity small enough to force the
-fallback to checking every earlier point.
+fallback to checking every earlier point.  The tile kernel's split of a large
+destination into segments walked by separate warps, joined by looking each survivor up
+in the earlier segments' final staircases, must give the same keep flags.
 """
 import numpy as np
 import pytest
@@ -16,7 +18,9 @@ import pytest
 import oracle
 
 
-def stair_walk(P, cap):
+def stair_walk(P, cap, save=False):
+    """Keep flags of one warp's walk; with `save` also the final staircase (None if it
+    outgrew cap)."""
     n = len(P)
     keep = np.zeros(n, bool)
     stair = []          # (objective 1, objective 2), objective 1 descending
@@ -58,7 +62,7 @@ def stair_walk(P, cap):
         for l in lanes:
             if valid[l]:
                 keep[c0 + l] = not dom[l]
-        if c0 + 32 >= n:
+        if c0 + 32 >= n and not save:
             break
         fresh = [l for l in lanes if not dom[l] and not rem[l]]
         kill = [any(q1[j] >= e1 and q2[j] >= e2 for j in fresh) for e1, e2 in stair]
@@ -79,6 +83,48 @@ def stair_walk(P, cap):
         for x, y in zip(new, new[1:]):
             assert x[0] > y[0] and x[1] < y[1]
         stair = new
+    if save:
+        return keep, (None if overflow else stair)
+    return keep
+
+
+def segmented_walk(P, seg, cap):
+    """The tile kernel's split of a large destination (tile_lex.cu): segments of equal
+    length at most `seg`, each walked from an empty staircase by its own warp, the final
+    staircases of all but the last kept; then every survivor of segment g is looked up in
+    the staircases of segments 0..g-1 (or compared with their points where one was not
+    kept)."""
+    n = len(P)
+    nseg = (n + seg - 1) // seg
+    ln = (n + nseg - 1) // nseg
+    keep = np.zeros(n, bool)
+    stairs = []
+    for g in range(nseg):
+        a, b = g * ln, min(n, (g + 1) * ln)
+        assert a < b
+        k, st = stair_walk(P[a:b], cap, save=True)
+        keep[a:b] = k
+        stairs.append(st)
+    for q in range(n):
+        if not keep[q]:
+            continue
+        q1, q2 = P[q, 1], P[q, 2]
+        for t in range(q // ln):
+            st = stairs[t]
+            if st is None:
+                dom = any(P[j, 1] >= q1 and P[j, 2] >= q2 for j in range(t * ln, (t + 1) * ln))
+            else:
+                lo, hi = 0, len(st)
+                while lo < hi:
+                    mid = (lo + hi) // 2
+                    if st[mid][0] >= q1:
+                        lo = mid + 1
+                    else:
+                        hi = mid
+                dom = lo > 0 and st[lo - 1][1] >= q2
+            if dom:
+                keep[q] = False
+                break
     return keep
 
 
@@ -101,3 +147,22 @@ def test_staircase_walk_keeps_the_oracle_frontier(cap):
         want = oracle.nd_keep(P.astype(np.int32))
         assert np.array_equal(oracle.sorted_set(P[keep]), oracle.sorted_set(P[want])), t
         assert keep.sum() == want.sum()
+
+
+@pytest.mark.parametrize("seg,cap", [(64, 64), (64, 5), (32, 64)])
+def test_segmented_walk_gives_the_same_keep_flags(seg, cap):
+    rng = np.random.default_rng(seg * 100 + cap)
+    for t in range(40):
+        n = int(rng.integers(1, 700))
+        hi = int(rng.choice([4, 10, 50, 1000, 100000]))
+        pts = rng.integers(0, hi, size=(n, 3)).astype(np.int64)
+        if t % 4 == 0:
+            pts[n // 3:2 * n // 3] = pts[:2 * n // 3 - n // 3]
+        if t % 5 == 1:
+            x = rng.integers(0, 1000, size=n)
+            y = rng.integers(0, 1000, size=n)
+            pts = np.stack([x, y, 2000 - x - y + rng.integers(0, 5, size=n)], 1)
+        order = sorted(range(n), key=lambda i: (-pts[i, 0], -pts[i, 1], -pts[i, 2], i))
+        P = pts[order]
+        got = segmented_walk(P, seg, cap)
+        assert np.array_equal(got, oracle.nd_keep(P.astype(np.int32))), t
