@@ -12,7 +12,8 @@ run whose every launch covers every instance still running.
   e2e     solves/s through pmdd_enumerate_batch with host DD buffers: DD upload and
           frontier download inside the timed region (host clock around the call).
 Extra keys: one-at-a-time solves/s of the same stream through pmdd_enumerate, the
-served loop (Poisson arrivals at 50/200/800 req/s, KP/SP method 1 + TSP method 3),
+served loop (Poisson arrivals at 50/200/800 req/s, KP/SP method 1 + TSP method 3, and
+the same mix submitted at once for the server's capacity),
 the config-1 filter roofline (1024 x KP d=3 n=40), the reference CPU baseline.
 
 Multi-GPU: one process per GPU (torchrun); every rank enumerates its own stream
@@ -224,7 +225,8 @@ def single_instances(P, instances, device, with_ref):
 
 # --------------------------------------------------------------- served loop
 def served_loop(rate, n_req, seed, P, instances, device=0):
-    """Poisson arrivals at `rate` req/s; KP (n~U{20..60}) / SP (n~U{60..100}) method 1 and
+    """Poisson arrivals at `rate` req/s (rate 0: every request at once, so that solves/s is
+    the server's capacity on the mix); KP (n~U{20..60}) / SP (n~U{60..100}) method 1 and
     TSP (n~U{9..13}, method 3); latency = finish - arrival on the host clock.  Afterwards
     every request runs alone on an idle server (submit -> result); the slowdown of a
     request is its served latency over its lone one.  Knapsack
@@ -240,8 +242,7 @@ def served_loop(rate, n_req, seed, P, instances, device=0):
     built = iter(build_dds([(p, t, "") for p, t, _ in specs if p != 3]))
     dds = [t if p == 3 else next(built) for p, t, _ in specs]
     rng = np.random.default_rng(seed + 1)
-    gaps = rng.exponential(1.0 / rate, size=n_req)
-    arrivals = np.cumsum(gaps)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=n_req)) if rate > 0 else np.zeros(n_req)
     srv = P.Server(device=device)
     outdir = tempfile.mkdtemp(prefix="pmdd_served_")
     writer = FrontierWriter()
@@ -300,7 +301,8 @@ def served_loop(rate, n_req, seed, P, instances, device=0):
     ids = np.array([i for i, _ in lat])
     lat = np.array([x for _, x in lat])
     slow = lat / np.maximum(alone[ids], 1e-3)
-    return {"rate_rps": rate, "requests": n_req, "p50_ms": float(np.percentile(lat, 50)),
+    return {"rate_rps": rate if rate > 0 else None, "arrivals": "poisson" if rate > 0 else "all at once",
+            "requests": n_req, "p50_ms": float(np.percentile(lat, 50)),
             "p99_ms": float(np.percentile(lat, 99)), "solves_per_s": n_req / wall,
             "alone_p50_ms": float(np.percentile(alone, 50)), "alone_p99_ms": float(np.percentile(alone, 99)),
             "slowdown_p50": float(np.percentile(slow, 50)), "slowdown_p99": float(np.percentile(slow, 99)),
@@ -343,6 +345,7 @@ SINGLE_CASES = {
     "kp4_n60": (1, 4, lambda I: I.knapsack_text(60, 4, 0)),
     "kp7_n25": (1, 7, lambda I: I.knapsack_text(25, 7, 0)),
     "sp3_n100_m20": (2, 3, lambda I: I.setpacking_text(100, 20, 3, 0)),
+    "tsp5_n13": (3, 5, lambda I: I.tsp_text(13, 5, 0)),
 }
 
 
@@ -364,8 +367,11 @@ def instance_only(args):
     runs = []
     for _ in range(max(1, args.steps)):
         st = {}
+        t0 = time.perf_counter()
         pts = P.enumerate_dd(dd, method=args.method, stats=st)
-        runs.append({"device_s": st["device_elapsed_s"], "solutions": int(len(pts)),
+        wall = time.perf_counter() - t0
+        runs.append({"device_s": st["device_elapsed_s"], "wall_s": wall, "solutions": int(len(pts)),
+                     "chained_layers": int(st["work_chained_layers"]),
                      "candidates": int(st["work_candidates_total"]), "join_products": int(st["work_join_products_total"]),
                      "launches": int(st["gpu_launches"])})
     print(json.dumps({"instance": args.instance, "method": args.method, "runs": runs}))
@@ -410,15 +416,28 @@ def main():
                     help="only the config-1 filter leg on this many KP d=3 n=40 instances (profiling aid; "
                          "prints its own JSON line, not a bench line)")
     ap.add_argument("--instance", default="",
-                    help="only one single-instance configuration (kp3_n40, kp4_n60, kp7_n25, sp3_n100_m20) by "
+                    help="only one single-instance configuration (kp3_n40, kp4_n60, kp7_n25, sp3_n100_m20, tsp5_n13) by "
                          "--method, `--warmup` untimed then `--steps` timed runs (profiling aid; own JSON line)")
     ap.add_argument("--method", type=int, default=1)
+    ap.add_argument("--served", action="store_true",
+                    help="only the served-loop legs (profiling aid; prints its own JSON line, not a bench line)")
     args = ap.parse_args()
     if args.config1 > 0:
         config1_only(args)
         return
     if args.instance:
         instance_only(args)
+        return
+    if args.served:
+        import torch
+
+        import pmdd_b200 as P
+        from pmdd_b200 import instances
+
+        torch.cuda.set_device(0)
+        legs = [served_loop(rate, {50: 100, 200: 200, 800: 400, 0: 400}[rate], rate, P, instances, 0)
+                for rate in (50, 200, 800, 0)]
+        print(json.dumps({"served": legs}))
         return
 
     rank = int(os.environ.get("RANK", "0"))
@@ -608,8 +627,8 @@ def main():
                                  "batched_e2e_over_one_at_a_time": e2e_value / world / oat}
         # served loop
         served = []
-        for rate in (50, 200, 800):
-            n_req = {50: 100, 200: 200, 800: 400}[rate] // (4 if args.quick else 1)
+        for rate in (50, 200, 800, 0):
+            n_req = {50: 100, 200: 200, 800: 400, 0: 400}[rate] // (4 if args.quick else 1)
             served.append(served_loop(rate, n_req, rate, P, instances, device))
         line["served"] = served
         # config-1 filter roofline: 1024 x KP d=3 n=40

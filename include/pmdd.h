@@ -142,6 +142,8 @@ typedef struct pmdd_stats {
     int64_t work_stair_candidates_total; /* three objectives: candidates of destinations filtered by a
                                             staircase warp (tiles above the pairwise limit, and
                                             oversized destinations with sorted runs) */
+    int64_t work_chained_layers;         /* layers expanded by chained steps (several layers between two
+                                            host read-backs, for steps with few candidates) */
 } pmdd_stats;
 
 /* ------------------------------------------------------------ one-shot entry

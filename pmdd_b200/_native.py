@@ -105,6 +105,7 @@ class PmddStats(ctypes.Structure):
         ("work_tile_survivors_total", c_i64),
         ("tile_launches", c_i64),
         ("work_stair_candidates_total", c_i64),
+        ("work_chained_layers", c_i64),
     ]
 
     def as_dict(self) -> dict:

@@ -200,7 +200,7 @@ __device__ __forceinline__ bool sweep_after(const PackedPt<D, T> *ys, int a, int
     return dom;
 }
 
-// Pivots: the candidates of largest objective sum, about pivot_target(n) of a destination's
+// Pivots: the candidates of largest objective sum, about pivot_target(n, rule) of a destination's
 // n.  A candidate that a pivot dominates is dropped at once.  Whatever dominates a remaining
 // candidate is itself remaining (a pivot dominating the dominator would dominate the
 // candidate as well, equal points included), so the exact pairwise sweep then runs over the
@@ -210,9 +210,10 @@ constexpr int kPivotSample = 4096;
 constexpr int kPivotMax = 8192;
 constexpr int kCompactThreads = 1024;
 
-__device__ __forceinline__ int64_t pivot_target(int64_t n) {
-    const int64_t t = n / 64;
-    return t < 512 ? 512 : (t > 4096 ? 4096 : t);
+__device__ __forceinline__ int64_t pivot_target(int64_t n, int rule) {
+    const int64_t t = rule == 1 ? static_cast<int64_t>(4.0 * sqrt(static_cast<double>(n))) : n / 64;
+    const int64_t lo = rule == 1 ? 32 : 512;
+    return t < lo ? lo : (t > 4096 ? 4096 : t);
 }
 
 // Objective sum as the pivot ranking key; it wraps for int64 objectives, which changes only
@@ -226,7 +227,7 @@ __device__ __forceinline__ long long pivot_key(const T *p) {
 }
 
 // One block per mark-path destination: the sums of an even sample of up to 4096 candidates,
-// sorted, give the threshold of the pivot_target(n) largest; the candidates at or above it
+// sorted, give the threshold of the pivot_target(n, rule) largest; the candidates at or above it
 // (the first kPivotMax in candidate order) are copied with their positions to the
 // destination's big_surv / big_surv_idx rows.
 template <int D, typename T>
@@ -272,7 +273,7 @@ __global__ void __launch_bounds__(kPivotThreads) big_pivot_kernel(const ExpandJo
             }
             __syncthreads();
         }
-    int64_t r = (static_cast<int64_t>(m) * pivot_target(n) + n - 1) / n - 1;
+    int64_t r = (static_cast<int64_t>(m) * pivot_target(n, J.pivot_rule) + n - 1) / n - 1;
     r = r < 0 ? 0 : (r >= m ? m - 1 : r);
     const long long tau = key[r];
     int32_t carry = 0;

@@ -304,6 +304,7 @@ int collect_batch(std::vector<std::unique_ptr<pmdd::Instance>> &reqs, pmdd_front
             stats->work_tile_candidates_total += st.work_tile_candidates_total;
             stats->work_tile_survivors_total += st.work_tile_survivors_total;
             stats->work_stair_candidates_total += st.work_stair_candidates_total;
+            stats->work_chained_layers += st.work_chained_layers;
             stats->gpu_mem_peak_used_bytes = std::max(stats->gpu_mem_peak_used_bytes, st.gpu_mem_peak_used_bytes);
             stats->gpu_mem_peak_reserved_bytes = st.gpu_mem_peak_reserved_bytes;
         }

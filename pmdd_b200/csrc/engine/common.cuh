@@ -98,7 +98,8 @@ struct ExpandJob {
     int32_t *tile_first;           // [num_tiles+1]: first destination of each tile (tile_plan_kernel)
     const int64_t *big_list;       // (local item, scratch offset) pairs
     int32_t num_big;
-    int32_t pad0;
+    int32_t pivot_rule;            // pivots per mark-path destination of n candidates:
+                                   // 1: 4*sqrt(n) within [32, 4096]; 0: n/64 within [512, 4096]
     void *big_pts;                 // scratch: candidates of oversized destinations (AoS)
     void *big_pts2;                // scratch: the same candidates in sum-bucket order
     void *big_surv;                // scratch: survivors of one bucket that overflow shared memory
@@ -143,6 +144,22 @@ struct CountJob {
     int64_t *arc_cand_off;         // out: num_arcs + 1 entries
     int64_t *big_list;             // out: (local item, scratch offset) pairs, capacity num_items
     struct CountResult *result;    // out
+    // Chained layers (chain.cu): nothing to count while *stop != 0.  With `next`, the block
+    // then sizes and plans this request's next chained expansion from the counts (what
+    // chain_prep_kernel and tile_plan_kernel do for a chain's first layer), and the last
+    // block of the launch to finish writes every request's first tile.
+    int32_t *stop;
+    int32_t *stopped_at;
+    struct ExpandJob *next;        // nullptr: no next chained expansion
+    int64_t *next_tiles;           // [chain_n] tiles of each request's next expansion (0: stopped)
+    int64_t *next_bases;           // [chain_n] out: exclusive prefix of next_tiles
+    int64_t *next_total;           // out: their sum
+    unsigned int *done;            // zeroed: blocks of the launch that have finished
+    int64_t cap;                   // candidates the next expansion's buffers hold
+    int32_t next_layer;            // the next expansion's chained layer, from 1
+    int32_t last;                  // the request's last chained layer
+    int32_t slot;                  // the request's index in the launch (= block)
+    int32_t chain_n;               // requests (blocks) in the launch
 };
 
 struct CountResult {
@@ -152,6 +169,23 @@ struct CountResult {
     int64_t cur_total;   // points of the current layer's frontiers (survivor statistics)
     int32_t num_big;
     int32_t max_big_arcs;  // most arcs of an oversized destination
+};
+
+// One chained layer of a group of requests (chain.cu): sizes that layer's expansions from
+// the counts before them, on the device, so that the host need not read them back.
+constexpr int kChainThreads = 1024;  // most requests one chain group takes
+struct ChainPrep {
+    struct ExpandJob *jobs;        // [n] this layer's expansions: total_cand, num_tiles written
+    int64_t *tile_bases;           // [n] written: first tile of each expansion
+    int64_t *tiles_total;          // written: the expansions' tiles in total
+    const CountResult *prev;       // the counts these expansions read, slot i at prev[prev_idx[i]]
+    const int32_t *prev_idx;       // nullptr: slot i reads prev[i]
+    int32_t *stop;                 // [n] per request, sticky: 1 once its chain has stopped
+    int32_t *stopped_at;           // [n] the layer at which it stopped (0: never)
+    const int64_t *cap;            // [n] candidates its chained frontier buffers hold
+    const int32_t *last;           // [n] its last chained layer
+    int32_t layer;                 // this layer, from 1
+    int32_t n;
 };
 
 // Big-path work entry: one oversized destination of one job.

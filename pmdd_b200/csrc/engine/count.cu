@@ -1,15 +1,84 @@
 // Next-layer counting: per-arc candidate offsets (exclusive scan of the neighbour's
 // frontier size), destination sizes, the list of oversized destinations with their
 // scratch offsets, and the current layer's survivor total.  One block per job.
+//
+// In a chained layer (chain.cu) the block also sizes its request's next chained
+// expansion from these counts -- candidates and tiles, or a stop at an oversized
+// destination, a full buffer or the request's last chained layer -- and writes that
+// expansion's tile plan (each tile's first destination, as tile_plan_kernel does); the
+// last block of the launch to finish then writes the first tile of every request, so
+// the next layer's tile kernel follows with no other launch in between.
 #include "kernels.cuh"
 #include "scan.cuh"
 
 namespace pmdd {
 namespace dev {
 
-__global__ void __launch_bounds__(kCountThreads) count_scan_kernel(const CountJob *jobs) {
-    const CountJob J = jobs[blockIdx.x];
-    __shared__ int64_t warp_buf[32];
+namespace {
+
+// Next chained expansion of the block's request (every thread of the block calls it).
+__device__ void chain_next(const CountJob &J, bool skip, int64_t *warp_buf, int64_t *s_total) {
+    __shared__ int64_t s_tiles;
+    __shared__ int s_last;
+    ExpandJob &N = *J.next;
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        int64_t tiles = 0;
+        bool stop = skip || J.next_layer > J.last;
+        if (!stop) {
+            const CountResult r = *J.result;  // written by this block's thread 0
+            stop = r.num_big > 0 || r.total > J.cap;
+            if (!stop) {
+                tiles = r.total > 0 ? (r.total + N.tile_window - 1) / N.tile_window : 1;
+                N.total_cand = r.total;
+                N.num_tiles = tiles;
+            }
+        }
+        if (stop) {
+            N.total_cand = 0;
+            N.num_tiles = 0;
+            if (*J.stop == 0) {
+                *J.stop = 1;
+                *J.stopped_at = J.next_layer;
+            }
+        }
+        s_tiles = tiles;
+    }
+    __syncthreads();
+    const int64_t T = s_tiles;
+    if (T > 0) {  // tile plan: destination i belongs to tile min(start_i / window, T - 1)
+        auto tile_of = [&](int32_t k) -> int64_t {
+            const int64_t t = item_start(N.item_arc_off, J.arc_cand_off, N.item_base, N.arc_base, k) / N.tile_window;
+            return t < T - 1 ? t : T - 1;
+        };
+        for (int32_t i = tid; i < N.num_items; i += kCountThreads) {
+            const int64_t ti = tile_of(i);
+            const int64_t tp = i == 0 ? -1 : tile_of(i - 1);
+            for (int64_t t = tp + 1; t <= ti; ++t) N.tile_first[t] = i;
+            if (i == N.num_items - 1)
+                for (int64_t t = ti + 1; t <= T; ++t) N.tile_first[t] = N.num_items;
+        }
+    }
+    // the last block to finish writes every request's first tile
+    if (tid == 0) {
+        J.next_tiles[J.slot] = T;
+        __threadfence();
+        s_last = atomicAdd(J.done, 1u) == static_cast<unsigned>(J.chain_n - 1) ? 1 : 0;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    for (int base = 0; base < J.chain_n; base += kCountThreads) {  // chain_n <= kChainThreads
+        const int k = base + tid;
+        const int64_t x = k < J.chain_n ? __ldcg(J.next_tiles + k) : 0;
+        const int64_t ex = block_exclusive_scan<int64_t, kCountThreads>(x, warp_buf, s_total);
+        if (k < J.chain_n) J.next_bases[k] = ex;
+    }
+    if (tid == 0) *J.next_total = *s_total;
+}
+
+// The counts of one job (every thread of the block calls it).
+__device__ void count_body(const CountJob &J, int64_t *warp_buf) {
     __shared__ int64_t s_total;
     __shared__ int64_t s_carry;
     __shared__ unsigned long long s_max;
@@ -77,6 +146,21 @@ __global__ void __launch_bounds__(kCountThreads) count_scan_kernel(const CountJo
         J.result->cur_total = cur_total;
         J.result->num_big = nbig;
         J.result->max_big_arcs = s_maxarcs;
+    }
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(kCountThreads) count_scan_kernel(const CountJob *jobs) {
+    const CountJob J = jobs[blockIdx.x];
+    // a chained request whose expansion before did not run has nothing to count
+    const bool skip = J.stop != nullptr && *J.stop != 0;
+    __shared__ int64_t warp_buf[32];
+    __shared__ int64_t s_sum;
+    if (!skip) count_body(J, warp_buf);
+    if (J.next != nullptr) {
+        __syncthreads();
+        chain_next(J, skip, warp_buf, &s_sum);
     }
 }
 

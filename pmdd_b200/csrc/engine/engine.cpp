@@ -578,6 +578,16 @@ Engine::Engine(int device, int64_t budget_bytes, int max_slots) : device_(device
     if (lx && lx[0] == '0') lex_tiles_ = false;
     const char *lb = std::getenv("PMDD_LEX_BULK");
     if (lb && *lb) lex_bulk_ = lb[0] == '1';
+    const char *cl = std::getenv("PMDD_CHAIN_LAYERS");
+    if (cl && *cl) chain_layers_ = std::max(0, std::min(std::atoi(cl), kChainMaxLayers));
+    const char *pr = std::getenv("PMDD_PIVOT_RULE");
+    if (pr && *pr) pivot_rule_ = std::strcmp(pr, "n64") == 0 ? 0 : 1;
+    const char *cg = std::getenv("PMDD_CHAIN_GROW");
+    if (cg && *cg) chain_grow_all_ = std::strcmp(cg, "all") == 0;
+    const char *cr = std::getenv("PMDD_CHAIN_MAX_REQUESTS");
+    if (cr && *cr) chain_max_requests_ = std::max<int64_t>(0, std::atoll(cr));
+    const char *cm = std::getenv("PMDD_CHAIN_MAX_CAND");
+    if (cm && *cm) chain_max_cand_ = std::max<int64_t>(0, std::atoll(cm));
     const char *la = std::getenv("PMDD_BIG_LEX_MAX_ARCS");
     if (la && *la) lex_max_arcs_ = std::max(0, std::min(std::atoi(la), dev::kBigLexMaxArcs));
     const char *pm = std::getenv("PMDD_LEX_PAIR_MAX");
@@ -943,6 +953,55 @@ struct CountPlan {
     bool after_expand;  // score update (false for the initial counts at admission)
 };
 
+// A request chained within one step (chain.cu): chained layer j (from 1) expands it to
+// layer e->nl + j into buffer set j % 2, reading set (j - 1) % 2 (layer 1: the step's own
+// expansion and count), and counts the layer after it into the same set.
+struct ChainSlot {
+    Instance *I = nullptr;
+    const ExpPlan *e = nullptr;    // this step's expansion of the request
+    size_t count_idx = 0;          // this step's count of the layer after it
+    int32_t last = 0;              // chained layers at most (the terminal layer included)
+    int64_t cap = 0;               // candidates a frontier buffer holds
+    int64_t ntiles = 0;            // tiles a chained layer may need
+    int32_t vmax = 0, amax = 0;    // most nodes / in-arcs of a chained layer
+    int32_t cmax = 0;              // most nodes of a layer a chained count counts
+    int64_t items[2] = {0, 0};
+    void *pts[2] = {nullptr, nullptr};
+    int64_t *off[2] = {nullptr, nullptr};
+    int32_t *size[2] = {nullptr, nullptr};  // sizes | tile plan | sorted flags (at sorted())
+    int64_t *arc[2] = {nullptr, nullptr};
+    int64_t *big[2] = {nullptr, nullptr};
+    uint8_t *sorted(int b) const { return reinterpret_cast<uint8_t *>(size[b] + vmax + ntiles + 1); }
+};
+
+// The chained requests of one (objectives, point type) pair, sharing launches.
+struct ChainGroup {
+    int d = 0;
+    bool wide = false;
+    std::vector<ChainSlot> slots;
+    int32_t layers = 0;            // most chained layers of a slot
+    size_t layer_bytes = 0;        // staging per layer: jobs | tile bases | item bases | count jobs
+    size_t st_off = 0;             // staging: layers, then cap | last | count index
+    size_t dv_off = 0;             // the group's part of the chain block (layout below)
+    size_t dv_bytes = 0;
+    size_t first_slot = 0;         // index of its first slot over all groups
+    std::vector<int64_t> items, tiles;  // per layer: destinations, tile bound
+    size_t r_bytes() const { return align256(sizeof(dev::CountResult) * static_cast<size_t>(layers) * slots.size()); }
+    size_t n4() const { return align256(sizeof(int32_t) * slots.size()); }
+    size_t ln(size_t each) const { return align256(each * static_cast<size_t>(layers)); }
+    // chain block: counts [layers][n] | stop [n] | stopped_at [n] | tile survivors and
+    // staircase candidates [layers][n][2] | tile queue [layers] | tiles [layers] |
+    // next expansion's tiles [layers][n] | finished count blocks [layers]
+    size_t off_stop() const { return r_bytes(); }
+    size_t off_stopped() const { return off_stop() + n4(); }
+    size_t off_ts() const { return off_stopped() + n4(); }
+    size_t off_queue() const { return off_ts() + ln(2 * sizeof(unsigned long long) * slots.size()); }
+    size_t off_tiles() const { return off_queue() + ln(sizeof(unsigned long long)); }
+    size_t off_nt() const { return off_tiles() + ln(sizeof(int64_t)); }
+    size_t off_done() const { return off_nt() + ln(sizeof(int64_t) * slots.size()); }
+    size_t bytes() const { return off_done() + ln(sizeof(unsigned int)); }
+};
+
 }  // namespace
 
 std::atomic<int64_t> g_total_launches{0};
@@ -1159,6 +1218,7 @@ int Engine::step() {
                     J.big_rows = e.big_rows;
                     const int64_t mm = mark_min_for(I.d, I.opts.problem_type);
                     J.big_mark_min = mm;
+                    J.pivot_rule = pivot_rule_;
                     if (s.res.max_item >= mm) gl.mark_cap += e.big_rows / mm + 1;
                     gl.big_passes = std::max<int64_t>(gl.big_passes, (e.big_total + e.big_window - 1) / e.big_window);
                 }
@@ -1262,7 +1322,8 @@ int Engine::step() {
     const size_t f_sd = f_ts + 2 * sizeof(unsigned long long) * exps.size();  // (survivors, staircase) per expansion
     const size_t f_err = f_sd + sizeof(int64_t) * sdjobs.size();
     const size_t f_clk = f_err + sizeof(uint64_t);  // PMDD_TRACE: tile phase cycles (8 counters)
-    const size_t f_total = f_clk + (trace_ ? 10 * sizeof(unsigned long long) : 0);
+    const size_t f_q = f_clk + (trace_ ? 10 * sizeof(unsigned long long) : 0);  // tile queue per group
+    const size_t f_total = f_q + sizeof(unsigned long long) * glaunch.size();
     char *d_fixed = static_cast<char *>(scratch(f_total));
     dev::CountResult *d_results = counts.empty() ? nullptr : reinterpret_cast<dev::CountResult *>(d_fixed);
     unsigned long long *d_tile_surv = d_fixed ? reinterpret_cast<unsigned long long *>(d_fixed + f_ts) : nullptr;
@@ -1350,6 +1411,104 @@ int Engine::step() {
     const size_t off_u = off_k;  // CoupleJob array
     const size_t off_ctrinit = align256(off_u + sizeof(dev::CoupleJob) * n_couple_max);
     stage_bytes = align256(off_ctrinit + sizeof(int64_t) * dev::kCtrCount * n_couple_max);
+
+    // ------------------------------------------------------------ layer chains
+    // A small step lets requests whose next count it computes (method 1, no state
+    // dominance, not yet at the terminal) expand further layers before the read-back.
+    std::vector<ChainGroup> chains;
+    size_t chain_dev_bytes = 0, chain_slots = 0;
+    char *d_chain = nullptr;
+    auto release_slot = [&](ChainSlot &c) {
+        for (int b = 0; b < 2; ++b)
+            for (void *q : {c.pts[b], static_cast<void *>(c.off[b]), static_cast<void *>(c.size[b]),
+                            static_cast<void *>(c.arc[b]), static_cast<void *>(c.big[b])})
+                arena_.release(q);
+    };
+    auto release_chains = [&]() {
+        for (auto &g : chains)
+            for (auto &c : g.slots) release_slot(c);
+        chains.clear();
+    };
+    if (chain_layers_ > 0 && count_alloc_ok && static_cast<int64_t>(exps.size()) <= chain_max_requests_) {
+        for (size_t k = 0; k < counts.size(); ++k) {
+            const CountPlan &cp = counts[k];
+            if (!cp.after_expand || !cp.td) continue;
+            Instance &I = *cp.I;
+            if (I.opts.method != 1 || I.opts.state_dominance > 0 || I.phase != Instance::RUNNING) continue;
+            const ExpPlan *e = nullptr;
+            for (const ExpPlan &x : exps)
+                if (x.I == &I && x.td) e = &x;
+            if (e == nullptr || e->cand > chain_max_cand_) continue;
+            ChainSlot c;
+            c.I = &I;
+            c.e = e;
+            c.count_idx = k;
+            // longer chains delay whatever else waits for the step: beyond the base length
+            // only for a request the engine runs alone
+            int32_t want = I.chain_len > 0 ? I.chain_len : chain_layers_;
+            if (!chain_grow_all_ && !(active_.size() == 1 && queued_.empty())) want = std::min(want, chain_layers_);
+            c.last = std::min<int32_t>(want, I.L - 1 - e->nl);
+            if (c.last <= 0) continue;
+            c.cap = std::min<int64_t>(std::max<int64_t>(8 * std::max<int64_t>(e->cand, 1), 16384), int64_t(1) << 22);
+            c.ntiles = c.cap / window + 2;
+            for (int j = 1; j <= c.last; ++j) {
+                c.vmax = std::max(c.vmax, I.nodes_in(e->nl + j));
+                if (e->nl + j < I.L - 1) {
+                    c.amax = std::max(c.amax, I.arc_at_layer[e->nl + j + 2] - I.arc_at_layer[e->nl + j + 1]);
+                    c.cmax = std::max(c.cmax, I.nodes_in(e->nl + j + 1));
+                }
+            }
+            bool okc = true;
+            for (int b = 0; b < 2; ++b) {
+                c.pts[b] = arena_.alloc(static_cast<size_t>(c.cap) * I.d * I.elem());
+                c.off[b] = static_cast<int64_t *>(arena_.alloc(sizeof(int64_t) * static_cast<size_t>(c.vmax)));
+                c.size[b] = static_cast<int32_t *>(
+                    arena_.alloc(sizeof(int32_t) * static_cast<size_t>(c.vmax + c.ntiles + 1) + static_cast<size_t>(c.vmax)));
+                c.arc[b] = static_cast<int64_t *>(arena_.alloc(sizeof(int64_t) * static_cast<size_t>(c.amax + 1)));
+                c.big[b] = static_cast<int64_t *>(arena_.alloc(sizeof(int64_t) * 2 * static_cast<size_t>(std::max(1, c.cmax))));
+                okc = okc && c.pts[b] && c.off[b] && c.size[b] && c.arc[b] && c.big[b];
+            }
+            if (!okc) {  // no room: this request and the rest take ordinary steps
+                release_slot(c);
+                break;
+            }
+            ChainGroup *g = nullptr;
+            for (auto &x : chains)
+                if (x.d == I.d && x.wide == I.wide) g = &x;
+            if (g == nullptr) {
+                chains.emplace_back();
+                g = &chains.back();
+                g->d = I.d;
+                g->wide = I.wide;
+            }
+            if (static_cast<int>(g->slots.size()) >= dev::kChainThreads) {
+                release_slot(c);
+                continue;
+            }
+            g->slots.push_back(c);
+        }
+        for (auto &g : chains) {
+            const size_t n = g.slots.size();
+            g.first_slot = chain_slots;
+            chain_slots += n;
+            for (const auto &c : g.slots) g.layers = std::max(g.layers, c.last);
+            g.layer_bytes = align256(sizeof(dev::ExpandJob) * n) + 2 * align256(sizeof(int64_t) * n) +
+                            align256(sizeof(dev::CountJob) * n);
+            g.st_off = stage_bytes;
+            stage_bytes += g.layer_bytes * static_cast<size_t>(g.layers) + align256(sizeof(int64_t) * n) + 2 * g.n4();
+            g.dv_off = chain_dev_bytes;
+            g.dv_bytes = g.bytes();
+            chain_dev_bytes += g.dv_bytes;
+        }
+        if (chain_dev_bytes > 0) {
+            d_chain = static_cast<char *>(scratch(chain_dev_bytes));
+            if (d_chain == nullptr) {
+                release_chains();
+                chain_dev_bytes = chain_slots = 0;
+            }
+        }
+        if (chains.empty()) stage_bytes = align256(off_ctrinit + sizeof(int64_t) * dev::kCtrCount * n_couple_max);
+    }
     // Every device and pinned allocation of the step is made here, before any side moves
     // or launch, so that running out of memory rolls the step back and fails one request
     // instead of the engine.
@@ -1359,7 +1518,10 @@ int Engine::step() {
     const size_t s_counts = 0, s_ts = f_ts, s_sd = f_sd, s_err = f_err;
     const size_t s_ctr = align256(f_total);
     const size_t s_fin = align256(s_ctr + sizeof(int64_t) * dev::kCtrCount * n_couple_max);
-    const size_t s_total = s_fin + sizeof(int32_t) * exps.size();
+    // ... | the chain block | the terminal sizes of chained requests
+    const size_t s_chain = align256(s_fin + sizeof(int32_t) * exps.size());
+    const size_t s_chfin = s_chain + chain_dev_bytes;
+    const size_t s_total = s_chfin + sizeof(int32_t) * chain_slots;
     // oversized path: per group, the size-order list and the mark-path plan
     std::vector<int32_t *> big_order(glaunch.size(), nullptr);
     std::vector<void *> big_plan(glaunch.size(), nullptr);
@@ -1393,6 +1555,7 @@ int Engine::step() {
             for (void *q : {e.out_pts, static_cast<void *>(e.out_off), static_cast<void *>(e.out_size), e.big_mem})
                 arena_.release(q);
         }
+        release_chains();
         for (void *q : step_scratch_) arena_.release(q);
         step_scratch_.clear();
         // the request with the largest expansion of this step (else the last one counted)
@@ -1432,6 +1595,107 @@ int Engine::step() {
     if (!sdjobs.empty()) {
         std::memcpy(hs + off_sd, sdjobs.data(), sizeof(dev::StateDomJob) * sdjobs.size());
         std::memcpy(hs + off_sdb, sd_bases.data(), sizeof(int64_t) * sd_bases.size());
+    }
+    // chained layers: every descriptor but the sizes the prep kernel fills in
+    for (auto &g : chains) {
+        const size_t n = g.slots.size();
+        char *dv = d_chain + g.dv_off;
+        dev::CountResult *dR = reinterpret_cast<dev::CountResult *>(dv);
+        int32_t *dstop = reinterpret_cast<int32_t *>(dv + g.off_stop());
+        int32_t *dstopped = reinterpret_cast<int32_t *>(dv + g.off_stopped());
+        unsigned long long *dts = reinterpret_cast<unsigned long long *>(dv + g.off_ts());
+        int64_t *dtiles = reinterpret_cast<int64_t *>(dv + g.off_tiles());
+        int64_t *dnt = reinterpret_cast<int64_t *>(dv + g.off_nt());
+        unsigned int *ddone = reinterpret_cast<unsigned int *>(dv + g.off_done());
+        g.items.assign(static_cast<size_t>(g.layers) + 1, 0);
+        g.tiles.assign(static_cast<size_t>(g.layers) + 1, 0);
+        for (int j = 1; j <= g.layers; ++j) {
+            char *hl = hs + g.st_off + g.layer_bytes * static_cast<size_t>(j - 1);
+            dev::ExpandJob *hx = reinterpret_cast<dev::ExpandJob *>(hl);
+            int64_t *hib = reinterpret_cast<int64_t *>(hl + align256(sizeof(dev::ExpandJob) * n) +
+                                                       align256(sizeof(int64_t) * n));
+            dev::CountJob *hc = reinterpret_cast<dev::CountJob *>(hl + align256(sizeof(dev::ExpandJob) * n) +
+                                                                 2 * align256(sizeof(int64_t) * n));
+            for (size_t i = 0; i < n; ++i) {
+                ChainSlot &c = g.slots[i];
+                Instance &I = *c.I;
+                const int b = j % 2, pb = (j - 1) % 2;
+                dev::ExpandJob &J = hx[i];
+                dev::CountJob &C = hc[i];
+                std::memset(&J, 0, sizeof(J));
+                std::memset(&C, 0, sizeof(C));
+                hib[i] = g.items[j];
+                J.tile_window = window;
+                J.err = d_err_step;
+                J.tile_surv = dts + 2 * (static_cast<size_t>(j - 1) * n + i);
+                C.stop = dstop + i;
+                C.stopped_at = dstopped + i;
+                C.result = dR + static_cast<size_t>(j - 1) * n + i;
+                if (j < g.layers) {  // the count sizes and plans this request's next chained expansion
+                    char *dn = d_stage + g.st_off + g.layer_bytes * static_cast<size_t>(j);
+                    C.next = reinterpret_cast<dev::ExpandJob *>(dn) + i;
+                    C.next_tiles = dnt + static_cast<size_t>(j - 1) * n;
+                    C.next_bases = reinterpret_cast<int64_t *>(dn + align256(sizeof(dev::ExpandJob) * n));
+                    C.next_total = dtiles + j;
+                    C.done = ddone + (j - 1);
+                    C.cap = c.cap;
+                    C.next_layer = j + 1;
+                    C.last = c.last;
+                    C.slot = static_cast<int32_t>(i);
+                    C.chain_n = static_cast<int32_t>(n);
+                }
+                C.arc_cand_off = c.arc[b];
+                C.big_list = c.big[b];
+                J.tile_first = c.size[b];
+                if (j > c.last) continue;  // past its last layer: the prep stops it
+                const int cur = c.e->nl + j - 1, nl = cur + 1;
+                J.item_arc_off = I.d_in_off;
+                J.arc_nbr = I.d_arc_src;
+                J.arc_wrow = I.d_arc_w;
+                J.arc_base = I.arc_at_layer[nl];
+                J.weights = I.d_weights;
+                J.arc_cand_off = j == 1 ? new_arc_off[c.count_idx] : c.arc[pb];
+                J.item_base = I.layer_off[nl];
+                J.num_items = I.nodes_in(nl);
+                J.prev_base = I.layer_off[cur];
+                J.prev_pts = j == 1 ? c.e->out_pts : c.pts[pb];
+                J.prev_off = j == 1 ? c.e->out_off : c.off[pb];
+                J.prev_size = j == 1 ? c.e->out_size : c.size[pb];
+                J.prev_sorted = j == 1 ? c.e->out_sorted : c.sorted(pb);
+                J.out_pts = c.pts[b];
+                J.out_off = c.off[b];
+                J.out_size = c.size[b];
+                J.out_sorted = c.sorted(b);
+                J.tile_first = c.size[b] + J.num_items;
+                J.big_list = j == 1 ? new_big[c.count_idx] : c.big[pb];
+                J.pair_max = pair_max_for(I.d, I.opts.problem_type);
+                J.lex_big = (I.d == 3 && lex_tiles_) ? 1 : 0;
+                J.lex_bulk = lex_bulk_ ? 1 : 0;
+                J.lex_max_arcs = lex_max_arcs_;
+                g.items[j] += J.num_items;
+                g.tiles[j] += c.ntiles;
+                if (nl < I.L - 1) {  // the count of the layer after it (none at the terminal)
+                    C.item_arc_off = I.d_in_off;
+                    C.arc_nbr = I.d_arc_src;
+                    C.arc_base = I.arc_at_layer[nl + 1];
+                    C.num_arcs = I.arc_at_layer[nl + 2] - I.arc_at_layer[nl + 1];
+                    C.item_base = I.layer_off[nl + 1];
+                    C.num_items = I.nodes_in(nl + 1);
+                    C.cur_base = I.layer_off[nl];
+                    C.cur_nodes = I.nodes_in(nl);
+                    C.cur_size = c.size[b];
+                }
+            }
+        }
+        char *hp = hs + g.st_off + g.layer_bytes * static_cast<size_t>(g.layers);
+        int64_t *hcap = reinterpret_cast<int64_t *>(hp);
+        int32_t *hlast = reinterpret_cast<int32_t *>(hp + align256(sizeof(int64_t) * n));
+        int32_t *hidx = reinterpret_cast<int32_t *>(hp + align256(sizeof(int64_t) * n) + g.n4());
+        for (size_t i = 0; i < n; ++i) {
+            hcap[i] = g.slots[i].cap;
+            hlast[i] = g.slots[i].last;
+            hidx[i] = static_cast<int32_t>(g.slots[i].count_idx);
+        }
     }
 
     // ------------------------------------------------- expansion bookkeeping
@@ -1524,17 +1788,23 @@ int Engine::step() {
     }
     cudaMemsetAsync(d_fixed + f_ts, 0, f_total - f_ts, stream_);
     cudaEventRecord(ev0, stream_);
-    for (const GroupLaunch &gl : glaunch) {
+    for (size_t gi = 0; gi < glaunch.size(); ++gi) {
+        const GroupLaunch &gl = glaunch[gi];
+        unsigned long long *queue = reinterpret_cast<unsigned long long *>(d_fixed + f_q) + gi;
         const dev::ExpandJob *dj = reinterpret_cast<const dev::ExpandJob *>(d_stage + off_x) + gl.first;
         const int64_t *dtb = reinterpret_cast<const int64_t *>(d_stage + off_tb) + gl.first;
         const int64_t *dib = reinterpret_cast<const int64_t *>(d_stage + off_ib) + gl.first;
         if (!cuda_ok(dev::launch_tile_plan(dj, dib, static_cast<int>(gl.count), gl.items, stream_), "tile_plan_kernel"))
             return -1;
-        const int grid = sms_ * 8;
+        // blocks beyond the tiles would only be scheduled to exit (several waves of them at
+        // the tiles' shared-memory size cost more than a small step's work)
+        const int grid = static_cast<int>(std::min<int64_t>(sms_ * 8, std::max<int64_t>(1, gl.tiles)));
         const bool lex = gl.d == 3 && lex_tiles_;
         const cudaError_t te =
-            lex ? dev::launch_expand_tiles_lex(gl.wide, dj, dtb, static_cast<int>(gl.count), gl.tiles, grid, stream_)
-                : dev::launch_expand_tiles(gl.d, gl.wide, dj, dtb, static_cast<int>(gl.count), gl.tiles, grid, stream_);
+            lex ? dev::launch_expand_tiles_lex(gl.wide, dj, dtb, static_cast<int>(gl.count), gl.tiles, grid, queue,
+                                               nullptr, stream_)
+                : dev::launch_expand_tiles(gl.d, gl.wide, dj, dtb, static_cast<int>(gl.count), gl.tiles, grid, queue,
+                                           nullptr, stream_);
         if (!cuda_ok(te, lex ? "expand_tile_lex_kernel" : "expand_tile_kernel")) return -1;
         launches_ += 2;
         ktimes_.tile_launches += 1;
@@ -1617,6 +1887,66 @@ int Engine::step() {
         }
     }
     cudaEventRecord(ev3, stream_);
+    // chained layers, per layer and group: the tiles and the counts of the layer after
+    // (which size and plan the next layer); the first layer is sized and planned by its own
+    // two kernels from the step's counts
+    int32_t chain_layers_run = 0;
+    if (!chains.empty()) {
+        cudaEventRecord(ev_[4], stream_);
+        cudaMemsetAsync(d_chain, 0, chain_dev_bytes, stream_);
+        for (const auto &g : chains) chain_layers_run = std::max(chain_layers_run, g.layers);
+        for (int j = 1; j <= chain_layers_run; ++j) {
+            for (const auto &g : chains) {
+                if (j > g.layers) continue;
+                const size_t n = g.slots.size();
+                char *dl = d_stage + g.st_off + g.layer_bytes * static_cast<size_t>(j - 1);
+                char *dv = d_chain + g.dv_off;
+                char *dp = d_stage + g.st_off + g.layer_bytes * static_cast<size_t>(g.layers);
+                dev::ExpandJob *dj = reinterpret_cast<dev::ExpandJob *>(dl);
+                int64_t *dtb = reinterpret_cast<int64_t *>(dl + align256(sizeof(dev::ExpandJob) * n));
+                const int64_t *dib = dtb + align256(sizeof(int64_t) * n) / sizeof(int64_t);
+                const dev::CountJob *dc = reinterpret_cast<const dev::CountJob *>(
+                    dl + align256(sizeof(dev::ExpandJob) * n) + 2 * align256(sizeof(int64_t) * n));
+                const dev::CountResult *dR = reinterpret_cast<const dev::CountResult *>(dv);
+                // chain block after the survivor counters: tile queue per layer, tiles per layer
+                unsigned long long *queue = reinterpret_cast<unsigned long long *>(dv + g.off_queue()) + (j - 1);
+                int64_t *tiles_dev = reinterpret_cast<int64_t *>(dv + g.off_tiles()) + (j - 1);
+                dev::ChainPrep P;
+                P.jobs = dj;
+                P.tile_bases = dtb;
+                P.tiles_total = tiles_dev;
+                P.prev = j == 1 ? d_results : dR + static_cast<size_t>(j - 2) * n;
+                P.prev_idx = j == 1 ? reinterpret_cast<const int32_t *>(dp + align256(sizeof(int64_t) * n) + g.n4())
+                                    : nullptr;
+                P.stop = reinterpret_cast<int32_t *>(dv + g.off_stop());
+                P.stopped_at = reinterpret_cast<int32_t *>(dv + g.off_stopped());
+                P.cap = reinterpret_cast<const int64_t *>(dp);
+                P.last = reinterpret_cast<const int32_t *>(dp + align256(sizeof(int64_t) * n));
+                P.layer = j;
+                P.n = static_cast<int32_t>(n);
+                if (j == 1) {  // later layers are sized and planned by the count before them
+                    if (!cuda_ok(dev::launch_chain_prep(P, stream_), "chain_prep_kernel")) return -1;
+                    if (!cuda_ok(dev::launch_tile_plan(dj, dib, static_cast<int>(n), g.items[j], stream_),
+                                 "tile_plan_kernel"))
+                        return -1;
+                    launches_ += 2;
+                }
+                const bool lex = g.d == 3 && lex_tiles_;
+                // the tiles' bound assumes full buffers: one wave of blocks loops over them
+                const int grid = static_cast<int>(std::min<int64_t>(sms_ * 2, std::max<int64_t>(1, g.tiles[j])));
+                const cudaError_t te =
+                    lex ? dev::launch_expand_tiles_lex(g.wide, dj, dtb, static_cast<int>(n), g.tiles[j], grid, queue,
+                                                       tiles_dev, stream_)
+                        : dev::launch_expand_tiles(g.d, g.wide, dj, dtb, static_cast<int>(n), g.tiles[j], grid, queue,
+                                                   tiles_dev, stream_);
+                if (!cuda_ok(te, lex ? "expand_tile_lex_kernel" : "expand_tile_kernel")) return -1;
+                if (!cuda_ok(dev::launch_count_scan(dc, static_cast<int>(n), stream_), "count_scan_kernel")) return -1;
+                launches_ += 2;
+                ktimes_.tile_launches += 1;
+            }
+        }
+        cudaEventRecord(ev_[5], stream_);
+    }
     char *hsum = static_cast<char *>(h_summary_.p);
     cudaMemcpyAsync(hsum + s_counts, d_fixed, f_total, cudaMemcpyDeviceToHost, stream_);
     for (size_t k = 0; k < ujobs.size(); ++k)
@@ -1625,6 +1955,16 @@ int Engine::step() {
     for (size_t k = 0; k < finishing.size(); ++k)
         cudaMemcpyAsync(hsum + s_fin + sizeof(int32_t) * k, finishing[k]->td.size, sizeof(int32_t),
                         cudaMemcpyDeviceToHost, stream_);
+    if (!chains.empty()) {
+        cudaMemcpyAsync(hsum + s_chain, d_chain, chain_dev_bytes, cudaMemcpyDeviceToHost, stream_);
+        for (const auto &g : chains)
+            for (size_t i = 0; i < g.slots.size(); ++i) {
+                const ChainSlot &c = g.slots[i];
+                if (c.e->nl + c.last == c.I->L - 1)  // the chain may reach the terminal node
+                    cudaMemcpyAsync(hsum + s_chfin + sizeof(int32_t) * (g.first_slot + i), c.size[c.last % 2],
+                                    sizeof(int32_t), cudaMemcpyDeviceToHost, stream_);
+            }
+    }
     for (void *q : to_release) arena_.release(q);
     const cudaError_t se = cudaStreamSynchronize(stream_);
     if (!cuda_ok(se, "engine step")) {
@@ -1638,6 +1978,9 @@ int Engine::step() {
     ktimes_.expand += ms_expand * 1e-3;
     ktimes_.big += ms_big * 1e-3;
     ktimes_.rest += ms_rest * 1e-3;
+    float ms_chain = 0;
+    if (!chains.empty()) cudaEventElapsedTime(&ms_chain, ev_[4], ev_[5]);
+    ktimes_.expand += ms_chain * 1e-3;
     if (trace_) {
         int64_t cand = 0, big_cand = 0, max_item = 0, nbig = 0;
         for (const ExpPlan &e : exps) {
@@ -1747,6 +2090,87 @@ int Engine::step() {
             cudaStreamSynchronize(stream_);
         }
     }
+    // chained requests move to the last layer they finished
+    int64_t chained_done = 0;
+    for (auto &g : chains) {
+        const size_t n = g.slots.size();
+        const char *hv = hsum + s_chain + g.dv_off;
+        const dev::CountResult *R = reinterpret_cast<const dev::CountResult *>(hv);
+        const int32_t *stopped = reinterpret_cast<const int32_t *>(hv + g.off_stopped());
+        const unsigned long long *ts = reinterpret_cast<const unsigned long long *>(hv + g.off_ts());
+        for (size_t i = 0; i < n; ++i) {
+            ChainSlot &c = g.slots[i];
+            Instance &I = *c.I;
+            const int32_t done = stopped[i] == 0 ? c.last : stopped[i] - 1;
+            // next chain: twice as long after one that ran to its end, one layer past
+            // where it stopped otherwise
+            I.chain_len = done == c.last ? std::min(kChainMaxLayers, 2 * std::max(c.last, chain_layers_))
+                                         : std::max(1, done + 1);
+            if (I.phase != Instance::RUNNING || done <= 0) {
+                release_slot(c);
+                continue;
+            }
+            Side &s = I.td;
+            int64_t C = 0;
+            for (int j = 1; j <= done; ++j) {
+                C = j == 1 ? hres[c.count_idx].total : R[static_cast<size_t>(j - 2) * n + i].total;
+                const size_t t = 2 * (static_cast<size_t>(j - 1) * n + i);
+                I.stats.work_candidates_total += C;
+                I.stats.work_candidates_peak = std::max(I.stats.work_candidates_peak, C);
+                I.peak_cand = std::max(I.peak_cand, C);
+                I.stats.work_tile_candidates_total += C;
+                I.stats.work_tile_survivors_total += static_cast<int64_t>(ts[t]);
+                I.stats.work_stair_candidates_total += static_cast<int64_t>(ts[t + 1]);
+                I.stats.layers_td++;
+                I.stats.work_chained_layers++;
+                if (c.e->nl + j < I.L - 1) {
+                    const int64_t surv = R[static_cast<size_t>(j - 1) * n + i].cur_total;
+                    I.stats.work_frontier_survivors_total += surv;
+                    I.stats.work_frontier_peak_points = std::max(I.stats.work_frontier_peak_points, surv);
+                }
+            }
+            I.stats.kernel_expand_td_s += ms_chain * 1e-3;
+            I.stats.kernel_total_s += ms_chain * 1e-3;
+            chained_done += done;
+            const int b = done % 2;
+            for (void *q : {s.pts, static_cast<void *>(s.off), static_cast<void *>(s.size), static_cast<void *>(s.arc_off),
+                            static_cast<void *>(s.big_list), c.pts[b ^ 1], static_cast<void *>(c.off[b ^ 1]),
+                            static_cast<void *>(c.size[b ^ 1]), static_cast<void *>(c.arc[b ^ 1]),
+                            static_cast<void *>(c.big[b ^ 1])})
+                arena_.release(q);
+            s.pts = c.pts[b];
+            s.off = c.off[b];
+            s.size = c.size[b];
+            s.sorted = c.sorted(b);
+            s.layer = c.e->nl + done;
+            s.slot_points = std::max<int64_t>(C, 1);
+            if (s.layer == I.L - 1) {  // the terminal: its frontier is the result
+                arena_.release(c.arc[b]);
+                arena_.release(c.big[b]);
+                s.arc_off = nullptr;
+                s.big_list = nullptr;
+                s.counted = false;
+                const int32_t rn = *reinterpret_cast<const int32_t *>(hsum + s_chfin + sizeof(int32_t) * (g.first_slot + i));
+                I.result_n = rn;
+                I.result.resize(static_cast<size_t>(rn) * I.d * I.elem());
+                if (rn > 0 && !cuda_ok(cudaMemcpy(I.result.data(), s.pts, I.result.size(), cudaMemcpyDeviceToHost), "D2H"))
+                    return -1;
+                I.stats.work_frontier_survivors_total += rn;
+                I.stats.work_frontier_peak_points = std::max<int64_t>(I.stats.work_frontier_peak_points, rn);
+                I.phase = Instance::DONE;
+            } else {
+                s.arc_off = c.arc[b];
+                s.big_list = c.big[b];
+                s.res = R[static_cast<size_t>(done - 1) * n + i];
+                s.counted = true;
+                s.score = s.res.total;
+            }
+        }
+    }
+    chained_layers_total_ += chained_done;
+    if (trace_ && !chains.empty())
+        std::fprintf(stderr, "[pmdd chain] requests=%zu layers=%d chained=%lld chain_ms=%.3f\n", chain_slots,
+                     chain_layers_run, static_cast<long long>(chained_done), ms_chain);
     if (blocked && exps.empty() && ujobs.empty() && counts.empty()) {
         // nothing could move: the largest blocked request cannot fit next to the others
         fail(*blocked, PMDD_ERR_OOM, "device memory budget exhausted (layer does not fit)");

@@ -149,6 +149,7 @@ struct Instance {
     int64_t peak_cand = 0;              // largest expansion (candidates) so far, either side
     int64_t max_layer_arcs = 0, max_layer_nodes = 0;
     int32_t skipped = 0;                // admission passes this request was passed over
+    int32_t chain_len = 0;              // layers its next chained step tries (0: the engine's base)
     bool external_dd = false;           // DD already resident (owned by a pmdd_resident set)
     const TspStructure *tsp = nullptr;  // TSP MDD: structure shared, I.dd holds the weight table only
     bool with_out_csr = false;          // device copy carries the bottom-up CSR
@@ -298,7 +299,7 @@ class Engine {
     int sms_ = 148;
     int max_slots_ = 0;
     cudaStream_t stream_ = nullptr;
-    cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};  // per-step phase timing, reused
+    cudaEvent_t ev_[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};  // per-step phase timing, reused
     std::map<int, std::unique_ptr<TspStructure>> tsp_cache_;
     Arena arena_;
     std::deque<std::unique_ptr<Instance>> queued_;
@@ -330,6 +331,24 @@ class Engine {
     // sorted frontiers, take the lexicographic path (big_lex.cu); the others the
     // SFS / pivot-mark passes.  PMDD_BIG_LEX_MAX_ARCS, 0 .. kBigLexMaxArcs.
     static constexpr int32_t kDefaultLexMaxArcs = 16;
+    // Layer chaining (chain.cu): a request expanding by method 1 without state dominance
+    // whose expansion in a step has at most chain_max_cand_ candidates goes on for more
+    // layers in the same step, before the host reads back: chain_layers_ the first time,
+    // then twice as many after a chain that ran to its end (up to kChainMaxLayers), or
+    // one layer past where the last one stopped; beyond chain_layers_ only while the
+    // request runs alone (PMDD_CHAIN_GROW=all: always).  Steps expanding more than
+    // chain_max_requests_ requests chain none: their host work per request is already
+    // shared, and the chained buffers would cost allocations per request.
+    // PMDD_CHAIN_LAYERS (0: off), PMDD_CHAIN_MAX_CAND and PMDD_CHAIN_MAX_REQUESTS.
+    int32_t chain_layers_ = 8;
+    static constexpr int32_t kChainMaxLayers = 64;
+    bool chain_grow_all_ = false;
+    int64_t chain_max_requests_ = 128;
+    // Pivots of a mark-path destination of n candidates (big.cu): about 4*sqrt(n) (1), or
+    // n/64 with a floor of 512 (0, PMDD_PIVOT_RULE=n64).
+    int32_t pivot_rule_ = 1;
+    int64_t chain_max_cand_ = int64_t(1) << 17;
+    int64_t chained_layers_total_ = 0;  // layers expanded by chained steps (statistics)
     int32_t lex_max_arcs_ = kDefaultLexMaxArcs;
     int32_t lex_pair_max_fixed_ = -1;
     std::map<std::pair<int, int>, int64_t> tuned_pair_max_;

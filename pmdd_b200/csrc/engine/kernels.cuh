@@ -8,11 +8,18 @@ namespace pmdd {
 namespace dev {
 
 cudaError_t launch_count_scan(const CountJob *jobs, int num_jobs, cudaStream_t stream);
+// One chained layer's sizes from the counts before it (chain.cu); one block, P.n <= kChainThreads.
+cudaError_t launch_chain_prep(const ChainPrep &P, cudaStream_t stream);
+// `queue`: a zeroed device counter from which the launch's blocks draw tiles;
+// `tiles_dev` (or nullptr): the jobs' tiles in total, written on the device before the
+// launch, when total_tiles is only a bound (chained layers).
 cudaError_t launch_expand_tiles(int d, bool wide, const ExpandJob *jobs, const int64_t *tile_bases, int num_jobs,
-                                int64_t total_tiles, int grid, cudaStream_t stream);
+                                int64_t total_tiles, int grid, unsigned long long *queue, const int64_t *tiles_dev,
+                                cudaStream_t stream);
 // Three objectives, frontiers in descending lexicographic order (tile_lex.cu).
 cudaError_t launch_expand_tiles_lex(bool wide, const ExpandJob *jobs, const int64_t *tile_bases, int num_jobs,
-                                    int64_t total_tiles, int grid, cudaStream_t stream);
+                                    int64_t total_tiles, int grid, unsigned long long *queue,
+                                    const int64_t *tiles_dev, cudaStream_t stream);
 size_t lex_tile_smem_bytes(bool wide);
 // Fills every job's tile_first (destination i belongs to tile min(start_i / kTileWindow,
 // num_tiles - 1)); one thread per destination over all jobs.

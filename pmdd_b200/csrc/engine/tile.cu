@@ -54,6 +54,7 @@ struct TileSmem {
     int32_t i0, i1;
     int32_t job;
     int32_t chunk;                      // next 32-candidate chunk to filter
+    int64_t tile;                       // tile taken from the launch's queue
 };
 
 // ------------------------------------------------------------------ tile plan
@@ -65,6 +66,7 @@ __global__ void tile_plan_kernel(const ExpandJob *__restrict__ jobs, const int64
         const ExpandJob &J = jobs[j];
         const int32_t i = static_cast<int32_t>(g - item_bases[j]);
         const int64_t T = J.num_tiles;
+        if (T == 0) continue;  // a chained expansion that stopped (chain.cu)
         auto tile_of = [&](int32_t k) -> int64_t {
             const int64_t s = item_start(J.item_arc_off, J.arc_cand_off, J.item_base, J.arc_base, k);
             const int64_t t = s / J.tile_window;
@@ -132,18 +134,29 @@ __device__ __forceinline__ bool sweep_other_arcs(const TileSmem<D, T> &S, int a,
 template <int D, typename T>
 __global__ void __launch_bounds__(kTT) expand_tile_kernel(const ExpandJob *__restrict__ jobs,
                                                           const int64_t *__restrict__ tile_bases, int num_jobs,
-                                                          int64_t total_tiles) {
+                                                          int64_t total_tiles, unsigned long long *queue,
+                                                          const int64_t *tiles_dev) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     TileSmem<D, T> &S = *reinterpret_cast<TileSmem<D, T> *>(smem_raw);
     const int tid = threadIdx.x, lane = tid & 31;
-    for (int64_t tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
+    // tiles are handed out by an atomic counter over all the launch's jobs, so a block
+    // that drew cheap tiles takes more
+    auto next_tile = [&]() -> int64_t {
+        if (tid == 0) S.tile = static_cast<int64_t>(atomicAdd(queue, 1ull));
+        __syncthreads();
+        return S.tile;
+    };
+    // jobs sized on the device (chain.cu) publish their tiles' total there
+    if (tiles_dev != nullptr) total_tiles = min(total_tiles, *tiles_dev);
+    for (int64_t tile = next_tile(); tile < total_tiles; tile = next_tile()) {
         if (tid == 0) {
             const int j = find_base(tile_bases, num_jobs, tile);
             const ExpandJob &J = jobs[j];
             const int64_t t = tile - tile_bases[j];
             S.job = j;
-            S.i0 = J.tile_first[t];
-            S.i1 = J.tile_first[t + 1];
+            // a job sized on the device may have fewer tiles than the launch allows for
+            S.i0 = t < J.num_tiles ? J.tile_first[t] : 0;
+            S.i1 = t < J.num_tiles ? J.tile_first[t + 1] : 0;
         }
         __syncthreads();
         const ExpandJob &J = jobs[S.job];
@@ -358,7 +371,8 @@ __global__ void __launch_bounds__(kTT) expand_tile_kernel(const ExpandJob *__res
 
 template <int D, typename T>
 static cudaError_t launch_expand_tiles_t(const ExpandJob *jobs, const int64_t *tile_bases, int num_jobs,
-                                         int64_t total_tiles, int grid, cudaStream_t stream) {
+                                         int64_t total_tiles, int grid, unsigned long long *queue,
+                                         const int64_t *tiles_dev, cudaStream_t stream) {
     const size_t smem = sizeof(TileSmem<D, T>);
     {
         const cudaError_t e = ensure_smem_limit(reinterpret_cast<const void *>(expand_tile_kernel<D, T>), smem);
@@ -366,16 +380,20 @@ static cudaError_t launch_expand_tiles_t(const ExpandJob *jobs, const int64_t *t
     }
     if (total_tiles <= 0) return cudaSuccess;
     const int64_t g = std::min<int64_t>(total_tiles, grid);
-    expand_tile_kernel<D, T><<<static_cast<unsigned>(g), kTT, smem, stream>>>(jobs, tile_bases, num_jobs, total_tiles);
+    expand_tile_kernel<D, T><<<static_cast<unsigned>(g), kTT, smem, stream>>>(jobs, tile_bases, num_jobs, total_tiles,
+                                                                                queue, tiles_dev);
     return cudaGetLastError();
 }
 
 cudaError_t launch_expand_tiles(int d, bool wide, const ExpandJob *jobs, const int64_t *tile_bases, int num_jobs,
-                                int64_t total_tiles, int grid, cudaStream_t stream) {
+                                int64_t total_tiles, int grid, unsigned long long *queue, const int64_t *tiles_dev,
+                                cudaStream_t stream) {
     if (wide) {
-        PMDD_DISPATCH_D(d, (launch_expand_tiles_t<DD, int64_t>(jobs, tile_bases, num_jobs, total_tiles, grid, stream)));
+        PMDD_DISPATCH_D(d, (launch_expand_tiles_t<DD, int64_t>(jobs, tile_bases, num_jobs, total_tiles, grid, queue,
+                                                               tiles_dev, stream)));
     }
-    PMDD_DISPATCH_D(d, (launch_expand_tiles_t<DD, int32_t>(jobs, tile_bases, num_jobs, total_tiles, grid, stream)));
+    PMDD_DISPATCH_D(d, (launch_expand_tiles_t<DD, int32_t>(jobs, tile_bases, num_jobs, total_tiles, grid, queue,
+                                                           tiles_dev, stream)));
 }
 
 }  // namespace dev

@@ -82,6 +82,7 @@ struct LexSmem {
     int32_t warp_i[32];
     int32_t tot_i, tot_a, i0, i1, job;
     int32_t n_big, next_big, next_chunk, tot_stage, n_slot;
+    int64_t tile;                        // tile taken from the launch's queue
 };
 
 // Phase clock (J.phase_clk, a diagnostic): thread 0 adds the cycles its block spent in
@@ -202,7 +203,8 @@ __device__ void stair_filter(LexSmem<T> &S, Stair<T> &sb, int s, int e, int lane
 template <typename T>
 __global__ void __launch_bounds__(kLT) expand_tile_lex_kernel(const ExpandJob *__restrict__ jobs,
                                                               const int64_t *__restrict__ tile_bases, int num_jobs,
-                                                              int64_t total_tiles) {
+                                                              int64_t total_tiles, unsigned long long *queue,
+                                                              const int64_t *tiles_dev) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     LexSmem<T> &S = *reinterpret_cast<LexSmem<T> *>(smem_raw);
     Stair<T> *stairs = reinterpret_cast<Stair<T> *>(&S.pts[0]);
@@ -212,14 +214,24 @@ __global__ void __launch_bounds__(kLT) expand_tile_lex_kernel(const ExpandJob *_
     bool aborted = false;
     if (tid == 0) mbar_init(&S.bar, 1);
     __syncthreads();
-    for (int64_t tile = blockIdx.x; tile < total_tiles && !aborted; tile += gridDim.x) {
+    // tiles are handed out by an atomic counter over all the launch's jobs, so a block
+    // that drew cheap tiles takes more
+    auto next_tile = [&]() -> int64_t {
+        if (tid == 0) S.tile = static_cast<int64_t>(atomicAdd(queue, 1ull));
+        __syncthreads();
+        return S.tile;
+    };
+    // jobs sized on the device (chain.cu) publish their tiles' total there
+    if (tiles_dev != nullptr) total_tiles = min(total_tiles, *tiles_dev);
+    for (int64_t tile = next_tile(); tile < total_tiles && !aborted; tile = next_tile()) {
         if (tid == 0) {
             const int j = find_base(tile_bases, num_jobs, tile);
             const ExpandJob &J = jobs[j];
             const int64_t t = tile - tile_bases[j];
             S.job = j;
-            S.i0 = J.tile_first[t];
-            S.i1 = J.tile_first[t + 1];
+            // a job sized on the device may have fewer tiles than the launch allows for
+            S.i0 = t < J.num_tiles ? J.tile_first[t] : 0;
+            S.i1 = t < J.num_tiles ? J.tile_first[t + 1] : 0;
         }
         __syncthreads();
         const ExpandJob &J = jobs[S.job];
@@ -637,7 +649,7 @@ namespace {
 
 template <typename T>
 cudaError_t launch_lex_t(const ExpandJob *jobs, const int64_t *tile_bases, int num_jobs, int64_t total_tiles, int grid,
-                         cudaStream_t stream) {
+                         unsigned long long *queue, const int64_t *tiles_dev, cudaStream_t stream) {
     static_assert(sizeof(Stair<T>) * kLexWarps + sizeof(SegStair<T>) * kLexSlots <= sizeof(PackedPt<3, T>) * kTileCap,
                   "staircases fit over pts");
     const size_t smem = sizeof(LexSmem<T>);
@@ -645,7 +657,8 @@ cudaError_t launch_lex_t(const ExpandJob *jobs, const int64_t *tile_bases, int n
     if (e != cudaSuccess) return e;
     if (total_tiles <= 0) return cudaSuccess;
     const int64_t g = std::min<int64_t>(total_tiles, grid);
-    expand_tile_lex_kernel<T><<<static_cast<unsigned>(g), kLT, smem, stream>>>(jobs, tile_bases, num_jobs, total_tiles);
+    expand_tile_lex_kernel<T><<<static_cast<unsigned>(g), kLT, smem, stream>>>(jobs, tile_bases, num_jobs, total_tiles,
+                                                                              queue, tiles_dev);
     return cudaGetLastError();
 }
 
@@ -654,9 +667,10 @@ cudaError_t launch_lex_t(const ExpandJob *jobs, const int64_t *tile_bases, int n
 size_t lex_tile_smem_bytes(bool wide) { return wide ? sizeof(LexSmem<int64_t>) : sizeof(LexSmem<int32_t>); }
 
 cudaError_t launch_expand_tiles_lex(bool wide, const ExpandJob *jobs, const int64_t *tile_bases, int num_jobs,
-                                    int64_t total_tiles, int grid, cudaStream_t stream) {
-    if (wide) return launch_lex_t<int64_t>(jobs, tile_bases, num_jobs, total_tiles, grid, stream);
-    return launch_lex_t<int32_t>(jobs, tile_bases, num_jobs, total_tiles, grid, stream);
+                                    int64_t total_tiles, int grid, unsigned long long *queue,
+                                    const int64_t *tiles_dev, cudaStream_t stream) {
+    if (wide) return launch_lex_t<int64_t>(jobs, tile_bases, num_jobs, total_tiles, grid, queue, tiles_dev, stream);
+    return launch_lex_t<int32_t>(jobs, tile_bases, num_jobs, total_tiles, grid, queue, tiles_dev, stream);
 }
 
 }  // namespace dev
