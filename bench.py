@@ -421,6 +421,8 @@ def main():
     ap.add_argument("--method", type=int, default=1)
     ap.add_argument("--served", action="store_true",
                     help="only the served-loop legs (profiling aid; prints its own JSON line, not a bench line)")
+    ap.add_argument("--served-rates", default="50,200,800,0",
+                    help="with --served: arrival rates in req/s (0: every request at once)")
     args = ap.parse_args()
     if args.config1 > 0:
         config1_only(args)
@@ -435,8 +437,8 @@ def main():
         from pmdd_b200 import instances
 
         torch.cuda.set_device(0)
-        legs = [served_loop(rate, {50: 100, 200: 200, 800: 400, 0: 400}[rate], rate, P, instances, 0)
-                for rate in (50, 200, 800, 0)]
+        rates = [int(x) for x in args.served_rates.split(",") if x]
+        legs = [served_loop(rate, {50: 100, 200: 200}.get(rate, 400), rate, P, instances, 0) for rate in rates]
         print(json.dumps({"served": legs}))
         return
 

@@ -329,6 +329,11 @@ int64_t pmdd_tuned_mark_min(const char *path, int32_t nobjs, int32_t problem_typ
  * rules as pmdd_tuned_mark_min.  No counterpart in the reference, whose filter is
  * pairwise at every size (src/pmdd/enum/gpu/topdown.cu:163-240). */
 int64_t pmdd_tuned_lex_pair_max(const char *path, int32_t nobjs, int32_t problem_type);
+/* The largest tile window (a tile's destinations start within this many candidates) the
+ * tuning file holds for (nobjs, problem_type), or -1 if none (engines then use 1024; a
+ * step uses its candidates over six tiles per SM, between 128 and this).  Same file rules
+ * as pmdd_tuned_mark_min.  No counterpart in the reference. */
+int64_t pmdd_tuned_tile_window_max(const char *path, int32_t nobjs, int32_t problem_type);
 
 #ifdef __cplusplus
 }

@@ -230,6 +230,7 @@ GPU_SYMBOLS = {
     "pmdd_launch_count": (c_i64, []),
     "pmdd_tuned_mark_min": (c_i64, [ctypes.c_char_p, c_i32, c_i32]),
     "pmdd_tuned_lex_pair_max": (c_i64, [ctypes.c_char_p, c_i32, c_i32]),
+    "pmdd_tuned_tile_window_max": (c_i64, [ctypes.c_char_p, c_i32, c_i32]),
 }
 
 _host = None

@@ -22,6 +22,12 @@ before them and larger ones by a staircase warp.  It is timed over PAIR_MAX_SIZE
 chosen oversized crossover in place (PMDD_LEX_PAIR_MAX in a fresh process); sizes within
 2 % of the fastest tie and the default (48) wins a tie, else the smallest.
 
+Every family also gets "tile_window_max", the largest tile window (the candidates a tile's
+destinations start within; a step's window is its candidates over six tiles per SM,
+between 128 and this): timed over WINDOW_SIZES with the choices above in place
+(PMDD_TILE_WINDOW_MAX in a fresh process); ties as for the pairwise limit, the default
+(1024) winning, else the largest.
+
     python -m pmdd_b200.autotune --nobjs 3 5 --ptype 1 3 [--out PATH]
 
 The file is PMDD_TUNING_FILE if set, else $XDG_CACHE_HOME/pmdd_b200/tuning.json or
@@ -42,6 +48,8 @@ CANDIDATE_SIZES = (1025, 4096, 16384, 65536, 1 << 40)
 DEFAULT_MARK_MIN = 1025
 PAIR_MAX_SIZES = (0, 16, 32, 48, 96, 256, 1024)
 DEFAULT_PAIR_MAX = 48
+WINDOW_SIZES = (256, 512, 1024)
+DEFAULT_WINDOW = 1024
 
 
 def tuning_path() -> str:
@@ -79,11 +87,12 @@ print(json.dumps({{"seconds": best}}))
 
 
 def time_in_child(path: str, nobjs: int, problem_type: int, method: int, mark_min: Optional[int],
-                  repeats: int = 3, timeout: float = 600.0, pair_max: Optional[int] = None) -> Optional[float]:
+                  repeats: int = 3, timeout: float = 600.0, pair_max: Optional[int] = None,
+                  window: Optional[int] = None) -> Optional[float]:
     """Best device time of `repeats` enumerations in a fresh process with the given
-    oversized crossover (None: the engine's built-in behaviour, no tuning file) and
-    three-objective pairwise limit (None: the built-in 48); None if the run fails or times
-    out."""
+    oversized crossover (None: the engine's built-in behaviour, no tuning file),
+    three-objective pairwise limit (None: the built-in 48) and largest tile window (None:
+    the built-in 1024); None if the run fails or times out."""
     root = os.path.abspath(os.path.join(os.path.dirname(__file__), ".."))
     code = _CHILD.format(root=root, path=path, ptype=problem_type, nobjs=nobjs, method=method, repeats=repeats)
     env = dict(os.environ, PMDD_TUNING_FILE=path + ".no-tuning.json")
@@ -95,6 +104,10 @@ def time_in_child(path: str, nobjs: int, problem_type: int, method: int, mark_mi
         env.pop("PMDD_LEX_PAIR_MAX", None)
     else:
         env["PMDD_LEX_PAIR_MAX"] = str(int(pair_max))
+    if window is None:
+        env.pop("PMDD_TILE_WINDOW_MAX", None)
+    else:
+        env["PMDD_TILE_WINDOW_MAX"] = str(int(window))
     try:
         p = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=timeout)
     except subprocess.TimeoutExpired:
@@ -134,6 +147,17 @@ def choose_pair_max(times: Dict[int, Optional[float]]) -> int:
     return DEFAULT_PAIR_MAX if DEFAULT_PAIR_MAX in tied else min(tied)
 
 
+def choose_window(times: Dict[int, Optional[float]]) -> int:
+    """Fastest largest tile window; sizes within 2 % of the fastest tie, the default wins
+    a tie, else the largest; no usable timing -> the default."""
+    ok = {k: v for k, v in times.items() if v is not None}
+    if not ok:
+        return DEFAULT_WINDOW
+    best = min(ok.values())
+    tied = [k for k, v in ok.items() if v <= best * 1.02]
+    return DEFAULT_WINDOW if DEFAULT_WINDOW in tied else max(tied)
+
+
 def tune(families: Iterable[tuple], sizes: Sequence[int] = CANDIDATE_SIZES, method: int = 1,
          timer: Optional[Callable[..., Optional[float]]] = None, workdir: Optional[str] = None) -> Dict[str, dict]:
     """Tunes every (nobjs, problem_type) of `families`; returns the entries to store."""
@@ -153,10 +177,14 @@ def tune(families: Iterable[tuple], sizes: Sequence[int] = CANDIDATE_SIZES, meth
         seconds["builtin"] = builtin
         pick = choose(times, builtin)
         entry = {"builtin": True} if pick is None else {"big_mark_min": pick}
+        pair = None
         if nobjs == 3:
             pt = {int(k): timer(path, nobjs, ptype, method, pick, pair_max=int(k)) for k in PAIR_MAX_SIZES}
-            entry["lex_pair_max"] = choose_pair_max(pt)
+            pair = entry["lex_pair_max"] = choose_pair_max(pt)
             entry["pair_max_seconds"] = {str(k): v for k, v in pt.items()}
+        wt = {int(k): timer(path, nobjs, ptype, method, pick, pair_max=pair, window=int(k)) for k in WINDOW_SIZES}
+        entry["tile_window_max"] = choose_window(wt)
+        entry["window_seconds"] = {str(k): v for k, v in wt.items()}
         entry.update({"seconds": seconds, "instance": desc})
         out[f"d{nobjs}_p{ptype}"] = entry
     return out
@@ -191,7 +219,7 @@ def main(argv=None):
     entries = tune([(d, p) for d in args.nobjs for p in args.ptype])
     path = write(entries, args.out)
     for k, v in entries.items():
-        print(k, v.get("big_mark_min", "built-in"), v.get("lex_pair_max", "-"), v["seconds"])
+        print(k, v.get("big_mark_min", "built-in"), v.get("lex_pair_max", "-"), v.get("tile_window_max"), v["seconds"])
     print("written", path)
 
 

@@ -1034,4 +1034,10 @@ int64_t pmdd_tuned_lex_pair_max(const char *path, int32_t nobjs, int32_t problem
     return it != table.end() ? it->second : -1;
 }
 
+int64_t pmdd_tuned_tile_window_max(const char *path, int32_t nobjs, int32_t problem_type) {
+    const auto table = pmdd::read_tuning(path ? std::string(path) : pmdd::default_tuning_path(), "tile_window_max");
+    auto it = table.find({nobjs, problem_type});
+    return it != table.end() ? it->second : -1;
+}
+
 }  // extern "C"

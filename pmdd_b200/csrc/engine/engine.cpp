@@ -60,7 +60,7 @@ bool Arena::grow(size_t at_least) {
     grow_s_ += now_s() - t0;
     const uintptr_t a = reinterpret_cast<uintptr_t>(p);
     chunks_[a] = bytes;
-    free_[a] = bytes;
+    add_free(a, bytes);
     reserved_ += bytes;
     return true;
 }
@@ -77,12 +77,13 @@ void *Arena::alloc(size_t bytes) {
     }
     bytes = align256(bytes == 0 ? 1 : bytes);
     for (int attempt = 0; attempt < 2; ++attempt) {
-        for (auto it = free_.begin(); it != free_.end(); ++it) {
-            if (it->second < bytes) continue;
-            const uintptr_t a = it->first;
-            const size_t rem = it->second - bytes;
-            free_.erase(it);
-            if (rem) free_[a + bytes] = rem;
+        // best fit: the smallest free block that holds `bytes` (lowest address among equals)
+        auto bs = by_size_.lower_bound({bytes, 0});
+        if (bs != by_size_.end()) {
+            const uintptr_t a = bs->second;
+            const size_t rem = bs->first - bytes;
+            drop_free(free_.find(a));
+            if (rem) add_free(a + bytes, rem);
             live_[a] = bytes;
             used_ += bytes;
             peak_ = std::max(peak_, used_);
@@ -91,6 +92,16 @@ void *Arena::alloc(size_t bytes) {
         if (attempt == 0 && !grow(bytes)) return nullptr;
     }
     return nullptr;
+}
+
+void Arena::add_free(uintptr_t a, size_t bytes) {
+    free_[a] = bytes;
+    by_size_.insert({bytes, a});
+}
+
+void Arena::drop_free(std::map<uintptr_t, size_t>::iterator it) {
+    by_size_.erase({it->second, it->first});
+    free_.erase(it);
 }
 
 void Arena::release(void *p) {
@@ -108,17 +119,19 @@ void Arena::release(void *p) {
     auto next = free_.lower_bound(start);
     if (next != free_.end() && next->first == start + bytes && next->first < c1) {
         bytes += next->second;
-        next = free_.erase(next);
+        auto after = std::next(next);
+        drop_free(next);
+        next = after;
     }
     if (next != free_.begin()) {
         auto prev = std::prev(next);
         if (prev->first + prev->second == start && prev->first >= c0) {
             start = prev->first;
             bytes += prev->second;
-            free_.erase(prev);
+            drop_free(prev);
         }
     }
-    free_[start] = bytes;
+    add_free(start, bytes);
 }
 
 bool Engine::Pinned::reserve(size_t bytes) {
@@ -590,6 +603,8 @@ Engine::Engine(int device, int64_t budget_bytes, int max_slots) : device_(device
     if (cm && *cm) chain_max_cand_ = std::max<int64_t>(0, std::atoll(cm));
     const char *la = std::getenv("PMDD_BIG_LEX_MAX_ARCS");
     if (la && *la) lex_max_arcs_ = std::max(0, std::min(std::atoi(la), dev::kBigLexMaxArcs));
+    const char *tw = std::getenv("PMDD_TILE_WINDOW_MAX");
+    if (tw && *tw) window_max_fixed_ = std::atoll(tw);
     const char *pm = std::getenv("PMDD_LEX_PAIR_MAX");
     if (pm && *pm && std::atoi(pm) >= 0) lex_pair_max_fixed_ = std::atoi(pm);
     ok_ = true;
@@ -664,6 +679,17 @@ void Engine::load_tuning() {
     for (auto it = tuned_mark_min_.begin(); it != tuned_mark_min_.end();)  // 0 is not a crossover
         it = it->second > 0 ? std::next(it) : tuned_mark_min_.erase(it);
     tuned_pair_max_ = read_tuning(path, "lex_pair_max");
+    tuned_window_max_ = read_tuning(path, "tile_window_max");
+}
+
+int64_t Engine::window_max_for(int d, int problem_type) const {
+    int64_t w = dev::kTileWindow;
+    if (window_max_fixed_ > 0) w = window_max_fixed_;
+    else {
+        auto it = tuned_window_max_.find({d, problem_type});
+        if (it != tuned_window_max_.end()) w = it->second;
+    }
+    return std::max<int64_t>(dev::kTileWindowMin, std::min<int64_t>(dev::kTileWindow, w));
 }
 
 int64_t Engine::mark_min_for(int d, int problem_type) const {
@@ -944,6 +970,7 @@ struct ExpPlan {
     // destinations whose scratch offset is in [p * big_window, (p + 1) * big_window),
     // so big_rows = min(big_total, big_window + largest destination) rows suffice
     int64_t big_window = 1;
+    int64_t window = dev::kTileWindow;  // its tile window
     int64_t big_rows = 0;
 };
 
@@ -1083,8 +1110,8 @@ int Engine::step() {
         if (s.counted) step_cand += s.res.total;
     }
     const int64_t want_tiles = static_cast<int64_t>(sms_) * 6;
-    const int64_t window = std::max<int64_t>(dev::kTileWindowMin, std::min<int64_t>(dev::kTileWindow,
-                                                                                     step_cand / want_tiles));
+    const int64_t step_window = std::max<int64_t>(dev::kTileWindowMin, std::min<int64_t>(dev::kTileWindow,
+                                                                                          step_cand / want_tiles));
     for (auto &p : active_) {
         Instance &I = *p;
         if (I.phase != Instance::RUNNING) continue;
@@ -1096,6 +1123,8 @@ int Engine::step() {
         const int64_t C = s.res.total;
         const int32_t V = I.nodes_in(nl);
         ExpPlan e{&I, is_td, nl, nullptr, nullptr, nullptr, nullptr, nullptr, 0, C, s.res.max_item, s.res.num_big};
+        e.window = std::min<int64_t>(step_window, window_max_for(I.d, I.opts.problem_type));
+        const int64_t window = e.window;
         const size_t pts_bytes = static_cast<size_t>(std::max<int64_t>(C, 1)) * I.d * I.elem();
         e.out_pts = arena_.alloc(pts_bytes);
         e.out_off = static_cast<int64_t *>(arena_.alloc(sizeof(int64_t) * V));
@@ -1189,8 +1218,8 @@ int Engine::step() {
                 J.out_off = e.out_off;
                 J.out_size = e.out_size;
                 J.total_cand = s.res.total;
-                J.tile_window = window;
-                J.num_tiles = std::max<int64_t>(1, (s.res.total + window - 1) / window);
+                J.tile_window = e.window;
+                J.num_tiles = std::max<int64_t>(1, (s.res.total + e.window - 1) / e.window);
                 J.tile_first = e.out_size + J.num_items;
                 J.prev_sorted = s.sorted;
                 J.out_sorted = e.out_sorted;
@@ -1450,7 +1479,7 @@ int Engine::step() {
             c.last = std::min<int32_t>(want, I.L - 1 - e->nl);
             if (c.last <= 0) continue;
             c.cap = std::min<int64_t>(std::max<int64_t>(8 * std::max<int64_t>(e->cand, 1), 16384), int64_t(1) << 22);
-            c.ntiles = c.cap / window + 2;
+            c.ntiles = c.cap / e->window + 2;
             for (int j = 1; j <= c.last; ++j) {
                 c.vmax = std::max(c.vmax, I.nodes_in(e->nl + j));
                 if (e->nl + j < I.L - 1) {
@@ -1625,7 +1654,7 @@ int Engine::step() {
                 std::memset(&J, 0, sizeof(J));
                 std::memset(&C, 0, sizeof(C));
                 hib[i] = g.items[j];
-                J.tile_window = window;
+                J.tile_window = c.e->window;
                 J.err = d_err_step;
                 J.tile_surv = dts + 2 * (static_cast<size_t>(j - 1) * n + i);
                 C.stop = dstop + i;
@@ -1991,17 +2020,19 @@ int Engine::step() {
             max_item = std::max(max_item, e.max_item);
             nbig += e.num_big;
         }
+        long long step_tiles = 0;
+        for (const GroupLaunch &gl : glaunch) step_tiles += gl.tiles;
         unsigned long long tile_surv = 0;
         for (size_t k = 0; k < exps.size(); ++k)
             tile_surv += reinterpret_cast<const unsigned long long *>(static_cast<char *>(h_summary_.p) + s_ts)[2 * k];
         const unsigned long long *pc = reinterpret_cast<const unsigned long long *>(static_cast<char *>(h_summary_.p) + f_clk);
         std::fprintf(stderr,
                      "[pmdd step] jobs=%zu counts=%zu couple=%zu cand=%lld big_items=%lld big_cand=%lld max_item=%lld "
-                     "tile_cand=%lld tile_surv=%llu tiles_ms=%.3f big_ms=%.3f rest_ms=%.3f host_to_sync_us=%.1f "
+                     "tile_cand=%lld tile_surv=%llu tiles=%lld tiles_ms=%.3f big_ms=%.3f rest_ms=%.3f host_to_sync_us=%.1f "
                      "arena_reserved_mb=%.0f arena_grow_ms=%.1f phase_mcyc=%.2f,%.2f,%.2f,%.2f,%.2f,%.2f,%.2f warp_mcyc=%.2f,%.2f\n",
                      exps.size(), counts.size(), ujobs.size(), static_cast<long long>(cand),
                      static_cast<long long>(nbig), static_cast<long long>(big_cand), static_cast<long long>(max_item),
-                     static_cast<long long>(cand - big_cand), tile_surv, ms_expand, ms_big, ms_rest,
+                     static_cast<long long>(cand - big_cand), tile_surv, step_tiles, ms_expand, ms_big, ms_rest,
                      (now_s() - step_t0) * 1e6, arena_.reserved() / 1e6, arena_.grow_seconds() * 1e3,
                      pc[0] * 1e-6, pc[1] * 1e-6, pc[2] * 1e-6, pc[3] * 1e-6, pc[4] * 1e-6, pc[5] * 1e-6, pc[6] * 1e-6,
                      pc[7] * 1e-6, pc[8] * 1e-6);

@@ -12,6 +12,7 @@
 #include <functional>
 #include <map>
 #include <memory>
+#include <set>
 #include <string>
 #include <unordered_map>
 #include <vector>
@@ -61,8 +62,11 @@ class Arena {
     size_t cap_ = 0, reserved_ = 0, used_ = 0, peak_ = 0;
     double grow_s_ = 0;
     std::map<uintptr_t, size_t> chunks_;            // cudaMalloc base -> bytes
-    std::map<uintptr_t, size_t> free_;              // address -> bytes
+    std::map<uintptr_t, size_t> free_;              // address -> bytes (free blocks, for coalescing)
+    std::set<std::pair<size_t, uintptr_t>> by_size_;  // the same blocks by (bytes, address): best fit
     std::unordered_map<uintptr_t, size_t> live_;    // address -> bytes
+    void add_free(uintptr_t a, size_t bytes);
+    void drop_free(std::map<uintptr_t, size_t>::iterator it);
 };
 
 // Frontiers of one direction at its current layer, in slot layout: node i's points
@@ -353,6 +357,13 @@ class Engine {
     int32_t lex_pair_max_fixed_ = -1;
     std::map<std::pair<int, int>, int64_t> tuned_pair_max_;
     int32_t pair_max_for(int d, int problem_type) const;
+    // Largest tile window (candidates a tile's destinations start within) for a family:
+    // PMDD_TILE_WINDOW_MAX if set, else "tile_window_max" in the tuning file, else
+    // kTileWindow; clamped to kTileWindowMin..kTileWindow.  A step's window is its
+    // candidates over six tiles per SM, within kTileWindowMin and this.
+    int64_t window_max_for(int d, int problem_type) const;
+    int64_t window_max_fixed_ = 0;
+    std::map<std::pair<int, int>, int64_t> tuned_window_max_;
     int64_t big_mark_min_fixed_ = 0;
     std::map<std::pair<int, int>, int64_t> tuned_mark_min_;
     // Footprint model: largest layer's candidates per DD arc, learned per (problem type,

@@ -1,5 +1,7 @@
-"""The crossover autotuner (pmdd_b200/autotune.py) and the engine's reading of its
-tuning file (pmdd_tuned_mark_min, the same parser the engine uses at start-up)."""
+"""The autotuner (pmdd_b200/autotune.py) and the engine's reading of its tuning file
+(pmdd_tuned_mark_min / _lex_pair_max / _tile_window_max, the same parser the engine uses
+at start-up): the choices with a fake timer, and on the GPU that the engine applies a
+tuned oversized crossover, pairwise limit and tile window."""
 import json
 import os
 
@@ -21,9 +23,12 @@ def test_choose_picks_fastest_and_breaks_ties_upward():
 def test_tune_with_a_fake_timer(tmp_path):
     calls = []
 
-    def timer(path, nobjs, ptype, method, mark_min, pair_max=None):
-        calls.append((nobjs, ptype, mark_min, pair_max))
+    def timer(path, nobjs, ptype, method, mark_min, pair_max=None, window=None):
+        calls.append((nobjs, ptype, mark_min, pair_max, window))
         assert os.path.exists(path)
+        if window is not None:  # with the other choices in place: 512 for d=3, a tie for d=5
+            assert pair_max == (96 if nobjs == 3 else None)
+            return 1.0 + (abs(window - 512) / 1e3 if nobjs == 3 else 0.0)
         if pair_max is not None:  # three objectives: the staircase pays from 96 candidates up
             assert nobjs == 3 and mark_min == 16384
             return 1.0 + abs(pair_max - 96) / 1e3
@@ -37,7 +42,9 @@ def test_tune_with_a_fake_timer(tmp_path):
     assert entries["d3_p1"]["lex_pair_max"] == 96
     assert entries["d5_p3"]["builtin"] is True and "big_mark_min" not in entries["d5_p3"]
     assert "lex_pair_max" not in entries["d5_p3"]
-    assert len(calls) == 8 + len(autotune.PAIR_MAX_SIZES)
+    assert entries["d3_p1"]["tile_window_max"] == 512
+    assert entries["d5_p3"]["tile_window_max"] == autotune.DEFAULT_WINDOW
+    assert len(calls) == 8 + len(autotune.PAIR_MAX_SIZES) + 2 * len(autotune.WINDOW_SIZES)
     # the engine reads a built-in entry as untuned, the other one as tuned
     path = autotune.write(entries, str(tmp_path / "t.json"))
     lib = _native.gpu_lib()
@@ -45,6 +52,9 @@ def test_tune_with_a_fake_timer(tmp_path):
     assert lib.pmdd_tuned_mark_min(path.encode(), 5, 3) == 0
     assert lib.pmdd_tuned_lex_pair_max(path.encode(), 3, 1) == 96
     assert lib.pmdd_tuned_lex_pair_max(path.encode(), 5, 3) == -1
+    assert lib.pmdd_tuned_tile_window_max(path.encode(), 3, 1) == 512
+    assert lib.pmdd_tuned_tile_window_max(path.encode(), 5, 3) == 1024
+    assert lib.pmdd_tuned_tile_window_max(path.encode(), 4, 2) == -1
 
 
 def test_choose_pair_max():
@@ -188,3 +198,53 @@ def test_engine_applies_the_tuned_pair_max(tmp_path):
     assert all_stair["ok"] and all_pair["ok"]
     assert all_stair["stair"] > 0.9 * all_stair["cand"]
     assert all_pair["stair"] < 0.05 * all_pair["cand"]
+
+
+def test_choose_window():
+    assert autotune.choose_window({256: 1.0, 512: 2.0, 1024: 3.0}) == 256
+    assert autotune.choose_window({256: 1.0, 512: 1.01, 1024: 1.015}) == autotune.DEFAULT_WINDOW
+    assert autotune.choose_window({256: 1.0, 512: 1.01, 1024: 2.0}) == 512
+    assert autotune.choose_window({256: None, 512: None}) == autotune.DEFAULT_WINDOW
+
+
+WINDOW_CHILD = r"""
+import sys, json
+sys.path.insert(0, {root!r})
+import numpy as np
+import oracle
+import pmdd_b200 as P
+from pmdd_b200 import instances
+from conftest import frontier_digest
+dds = [P.DecisionDiagram.from_text(instances.knapsack_text(40, 3, s), 1, 3) for s in range(16)]
+got = P.enumerate_batch(dds, method=1)
+print(json.dumps({{"digests": [frontier_digest(g) for g in got]}}))
+"""
+
+
+@pytest.mark.gpu
+def test_engine_applies_the_tuned_tile_window(tmp_path):
+    """A tuning file that caps the three-objective knapsack family's tile window at 256
+    makes the steps of a 16-instance batch (up to ~10^6 candidates, so a 1024 window
+    otherwise) use several times more tiles (the PMDD_TRACE step lines' tiles= count) than
+    one that leaves it at 1024; the frontiers are the same."""
+    import re
+    import subprocess
+    import sys
+
+    from conftest import ROOT
+
+    def run(window):
+        path = str(tmp_path / f"w{window}.json")
+        autotune.write({"d3_p1": {"tile_window_max": window}}, path)
+        env = dict(os.environ, PMDD_TUNING_FILE=path, PMDD_TRACE="1", PMDD_CHAIN_LAYERS="0")
+        env.pop("PMDD_TILE_WINDOW_MAX", None)
+        p = subprocess.run([sys.executable, "-c", WINDOW_CHILD.format(root=ROOT)], env=env, capture_output=True,
+                           text=True, timeout=600, cwd=os.path.join(ROOT, "tests"))
+        assert p.returncode == 0, p.stdout + p.stderr
+        tiles = sum(int(t) for t in re.findall(r" tiles=(\d+)", p.stderr))
+        return json.loads(p.stdout.strip().splitlines()[-1])["digests"], tiles
+
+    d256, t256 = run(256)
+    d1024, t1024 = run(1024)
+    assert d256 == d1024
+    assert t256 > 2 * t1024
