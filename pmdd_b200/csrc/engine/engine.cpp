@@ -1127,10 +1127,15 @@ int Engine::step() {
         const int64_t window = e.window;
         const size_t pts_bytes = static_cast<size_t>(std::max<int64_t>(C, 1)) * I.d * I.elem();
         e.out_pts = arena_.alloc(pts_bytes);
-        e.out_off = static_cast<int64_t *>(arena_.alloc(sizeof(int64_t) * V));
-        // sizes of the new frontier, followed by the tile plan of this expansion
+        // one block: slot offsets | sizes of the new frontier | the tile plan of this
+        // expansion | sorted flags (released through out_off; the arena ignores the
+        // release of out_size, which it did not hand out)
         const int64_t ntiles = std::max<int64_t>(1, (C + window - 1) / window);
-        e.out_size = static_cast<int32_t *>(arena_.alloc(sizeof(int32_t) * (V + ntiles + 1) + static_cast<size_t>(V)));
+        const size_t off_bytes = align256(sizeof(int64_t) * V);
+        char *ix = static_cast<char *>(
+            arena_.alloc(off_bytes + sizeof(int32_t) * (V + ntiles + 1) + static_cast<size_t>(V)));
+        e.out_off = reinterpret_cast<int64_t *>(ix);
+        e.out_size = ix ? reinterpret_cast<int32_t *>(ix + off_bytes) : nullptr;
         if (e.out_size) e.out_sorted = reinterpret_cast<uint8_t *>(e.out_size + V + ntiles + 1);
         bool okay = e.out_pts && e.out_off && e.out_size;
         if (okay && s.res.num_big > 0) {
@@ -1266,6 +1271,7 @@ int Engine::step() {
         }
         exps.swap(ordered);
     }
+    const double t_p1 = trace_ ? now_s() : 0.0;  // expansions planned and described
 
     // state dominance on the top-down layers that knapsack and set-packing requests asking
     // for it expand this step, in both methods (jobs follow the expansion order, so
@@ -1385,9 +1391,20 @@ int Engine::step() {
 
     // --------------------------------------------------- finish planning of counts
     // Counts read the frontier a side will have after this step's expansions.
+    // this step's expansion of each (request, direction), looked up per count
+    std::unordered_map<const Instance *, std::pair<int32_t, int32_t>> exp_of;  // td, bu index (-1: none)
+    exp_of.reserve(exps.size() * 2);
+    for (size_t i = 0; i < exps.size(); ++i) {
+        auto ins = exp_of.emplace(exps[i].I, std::make_pair(int32_t(-1), int32_t(-1)));
+        (exps[i].td ? ins.first->second.first : ins.first->second.second) = static_cast<int32_t>(i);
+    }
+    auto exp_index = [&](const Instance &I, bool td) -> int32_t {
+        auto it = exp_of.find(&I);
+        return it == exp_of.end() ? -1 : (td ? it->second.first : it->second.second);
+    };
     auto side_after = [&](Instance &I, bool td) -> std::pair<int, int32_t *> {
-        for (const ExpPlan &e : exps)
-            if (e.I == &I && e.td == td) return {e.nl, e.out_size};
+        const int32_t i = exp_index(I, td);
+        if (i >= 0) return {exps[i].nl, exps[i].out_size};
         Side &s = td ? I.td : I.bu;
         return {s.layer, s.size};
     };
@@ -1415,8 +1432,11 @@ int Engine::step() {
         J.cur_base = I.layer_off[l];
         J.cur_nodes = I.nodes_in(l);
         J.cur_size = cur.second;
-        new_arc_off[k] = static_cast<int64_t *>(arena_.alloc(sizeof(int64_t) * (static_cast<size_t>(J.num_arcs) + 1)));
-        new_big[k] = static_cast<int64_t *>(arena_.alloc(sizeof(int64_t) * 2 * std::max(1, J.num_items)));
+        // one block: per-arc candidate offsets | oversized list (released through the offsets)
+        const size_t arc_bytes = align256(sizeof(int64_t) * (static_cast<size_t>(J.num_arcs) + 1));
+        char *cb = static_cast<char *>(arena_.alloc(arc_bytes + sizeof(int64_t) * 2 * std::max(1, J.num_items)));
+        new_arc_off[k] = reinterpret_cast<int64_t *>(cb);
+        new_big[k] = cb ? reinterpret_cast<int64_t *>(cb + arc_bytes) : nullptr;
         if (!new_arc_off[k] || !new_big[k]) {
             count_alloc_ok = false;
             break;
@@ -1464,9 +1484,8 @@ int Engine::step() {
             if (!cp.after_expand || !cp.td) continue;
             Instance &I = *cp.I;
             if (I.opts.method != 1 || I.opts.state_dominance > 0 || I.phase != Instance::RUNNING) continue;
-            const ExpPlan *e = nullptr;
-            for (const ExpPlan &x : exps)
-                if (x.I == &I && x.td) e = &x;
+            const int32_t ei = exp_index(I, true);
+            const ExpPlan *e = ei >= 0 ? &exps[ei] : nullptr;
             if (e == nullptr || e->cand > chain_max_cand_) continue;
             ChainSlot c;
             c.I = &I;
@@ -1807,6 +1826,7 @@ int Engine::step() {
 
     // ----------------------------------------------------------- device work
     cudaEvent_t ev0 = ev_[0], ev1 = ev_[1], ev2 = ev_[2], ev3 = ev_[3];
+    const double t_issue = trace_ ? now_s() : 0.0;  // host planning done
     if (stage_bytes && !cuda_ok(cudaMemcpyAsync(d_stage, hs, stage_bytes, cudaMemcpyHostToDevice, stream_), "H2D"))
         return -1;
     // coupling counters of requests that just reached their cutset start from the staged init values
@@ -1994,8 +2014,11 @@ int Engine::step() {
                                     sizeof(int32_t), cudaMemcpyDeviceToHost, stream_);
             }
     }
+    const double t_rel = trace_ ? now_s() : 0.0;
     for (void *q : to_release) arena_.release(q);
+    const double t_enq = trace_ ? now_s() : 0.0;  // every copy and launch enqueued
     const cudaError_t se = cudaStreamSynchronize(stream_);
+    const double t_sync = trace_ ? now_s() : 0.0;
     if (!cuda_ok(se, "engine step")) {
         for (auto &p : active_) fail(*p, PMDD_ERR_CUDA, error_);
         return -1;
@@ -2029,11 +2052,14 @@ int Engine::step() {
         std::fprintf(stderr,
                      "[pmdd step] jobs=%zu counts=%zu couple=%zu cand=%lld big_items=%lld big_cand=%lld max_item=%lld "
                      "tile_cand=%lld tile_surv=%llu tiles=%lld tiles_ms=%.3f big_ms=%.3f rest_ms=%.3f host_to_sync_us=%.1f "
+                     "plan_us=%.1f plan_exp_us=%.1f enqueue_us=%.1f release_us=%.1f wait_us=%.1f prev_post_us=%.1f "
                      "arena_reserved_mb=%.0f arena_grow_ms=%.1f phase_mcyc=%.2f,%.2f,%.2f,%.2f,%.2f,%.2f,%.2f warp_mcyc=%.2f,%.2f\n",
                      exps.size(), counts.size(), ujobs.size(), static_cast<long long>(cand),
                      static_cast<long long>(nbig), static_cast<long long>(big_cand), static_cast<long long>(max_item),
                      static_cast<long long>(cand - big_cand), tile_surv, step_tiles, ms_expand, ms_big, ms_rest,
-                     (now_s() - step_t0) * 1e6, arena_.reserved() / 1e6, arena_.grow_seconds() * 1e3,
+                     (now_s() - step_t0) * 1e6, (t_issue - step_t0) * 1e6, (t_p1 - step_t0) * 1e6,
+                     (t_rel - t_issue) * 1e6, (t_enq - t_rel) * 1e6, (t_sync - t_enq) * 1e6, last_post_us_,
+                     arena_.reserved() / 1e6, arena_.grow_seconds() * 1e3,
                      pc[0] * 1e-6, pc[1] * 1e-6, pc[2] * 1e-6, pc[3] * 1e-6, pc[4] * 1e-6, pc[5] * 1e-6, pc[6] * 1e-6,
                      pc[7] * 1e-6, pc[8] * 1e-6);
     }
@@ -2077,14 +2103,19 @@ int Engine::step() {
             I.stats.work_frontier_peak_points = std::max(I.stats.work_frontier_peak_points, s.res.cur_total);
         }
     }
+    // frontiers of the requests this step finishes: fetched together below (one pinned
+    // buffer, one synchronisation) instead of one blocking copy each
+    std::vector<std::pair<Instance *, const void *>> fetches;
+    auto fetch = [&](Instance &I, const void *src) {
+        if (!I.result.empty()) fetches.push_back({&I, src});
+    };
     for (size_t k = 0; k < finishing.size(); ++k) {
         Instance &I = *finishing[k];
         if (I.phase == Instance::DONE) continue;
         const int32_t n = *reinterpret_cast<const int32_t *>(hsum + s_fin + sizeof(int32_t) * k);
         I.result_n = n;
         I.result.resize(static_cast<size_t>(n) * I.d * I.elem());
-        if (n > 0 && !cuda_ok(cudaMemcpy(I.result.data(), I.td.pts, I.result.size(), cudaMemcpyDeviceToHost), "D2H"))
-            return -1;
+        fetch(I, I.td.pts);
         I.stats.work_frontier_survivors_total += n;
         I.stats.work_frontier_peak_points = std::max<int64_t>(I.stats.work_frontier_peak_points, n);
         I.phase = Instance::DONE;
@@ -2099,8 +2130,7 @@ int Engine::step() {
             const int64_t n = c[dev::kCtrF];
             I.result_n = n;
             I.result.resize(static_cast<size_t>(n) * I.d * I.elem());
-            if (n > 0 && !cuda_ok(cudaMemcpy(I.result.data(), I.cu_U, I.result.size(), cudaMemcpyDeviceToHost), "D2H"))
-                return -1;
+            fetch(I, I.cu_U);
             I.stats.work_frontier_survivors_total += n;
             I.stats.work_frontier_peak_points = std::max<int64_t>(I.stats.work_frontier_peak_points, n);
             I.phase = Instance::DONE;
@@ -2184,8 +2214,7 @@ int Engine::step() {
                 const int32_t rn = *reinterpret_cast<const int32_t *>(hsum + s_chfin + sizeof(int32_t) * (g.first_slot + i));
                 I.result_n = rn;
                 I.result.resize(static_cast<size_t>(rn) * I.d * I.elem());
-                if (rn > 0 && !cuda_ok(cudaMemcpy(I.result.data(), s.pts, I.result.size(), cudaMemcpyDeviceToHost), "D2H"))
-                    return -1;
+                fetch(I, s.pts);
                 I.stats.work_frontier_survivors_total += rn;
                 I.stats.work_frontier_peak_points = std::max<int64_t>(I.stats.work_frontier_peak_points, rn);
                 I.phase = Instance::DONE;
@@ -2199,6 +2228,26 @@ int Engine::step() {
         }
     }
     chained_layers_total_ += chained_done;
+    if (!fetches.empty()) {
+        size_t total = 0;
+        for (auto &f : fetches) total += align256(f.first->result.size());
+        if (!h_results_.reserve(total)) {
+            error_ = "cudaMallocHost failed";
+            return -1;
+        }
+        size_t at = 0;
+        for (auto &f : fetches) {
+            cudaMemcpyAsync(static_cast<char *>(h_results_.p) + at, f.second, f.first->result.size(),
+                            cudaMemcpyDeviceToHost, stream_);
+            at += align256(f.first->result.size());
+        }
+        if (!cuda_ok(cudaStreamSynchronize(stream_), "D2H")) return -1;
+        at = 0;
+        for (auto &f : fetches) {
+            std::memcpy(f.first->result.data(), static_cast<char *>(h_results_.p) + at, f.first->result.size());
+            at += align256(f.first->result.size());
+        }
+    }
     if (trace_ && !chains.empty())
         std::fprintf(stderr, "[pmdd chain] requests=%zu layers=%d chained=%lld chain_ms=%.3f\n", chain_slots,
                      chain_layers_run, static_cast<long long>(chained_done), ms_chain);
@@ -2222,6 +2271,7 @@ int Engine::step() {
             ++it;
         }
     }
+    if (trace_) last_post_us_ = (now_s() - t_sync) * 1e6;
     return done;
 }
 

@@ -311,10 +311,12 @@ class Engine {
     std::deque<std::unique_ptr<Instance>> finished_;
     std::vector<void *> step_scratch_;
     Pinned h_desc_, h_summary_, h_init_, h_stage_;
+    Pinned h_results_;  // the frontiers of the requests a step finishes, fetched together
 
     int64_t launches_ = 0;
     KernelTimes ktimes_;
     bool trace_ = false;  // PMDD_TRACE=1: one stderr line per step
+    double last_post_us_ = 0;  // PMDD_TRACE: host time after the last step's synchronisation
     // Oversized destinations of at least mark_min_for(d, problem type) candidates are
     // filtered by the GPU-wide pivot/mark pass instead of one SFS block: PMDD_BIG_MARK_MIN
     // if set, else the tuned value for (d, problem type) from the tuning file, else
