@@ -224,7 +224,7 @@ def single_instances(P, instances, device, with_ref):
 
 
 # --------------------------------------------------------------- served loop
-def served_loop(rate, n_req, seed, P, instances, device=0):
+def served_loop(rate, n_req, seed, P, instances, device=0, detail=None):
     """Poisson arrivals at `rate` req/s (rate 0: every request at once, so that solves/s is
     the server's capacity on the mix); KP (n~U{20..60}) / SP (n~U{60..100}) method 1 and
     TSP (n~U{9..13}, method 3); latency = finish - arrival on the host clock.  Afterwards
@@ -301,6 +301,10 @@ def served_loop(rate, n_req, seed, P, instances, device=0):
     ids = np.array([i for i, _ in lat])
     lat = np.array([x for _, x in lat])
     slow = lat / np.maximum(alone[ids], 1e-3)
+    if detail is not None:  # per request: tag, method, served and lone latency (profiling aid)
+        served_ms = dict(zip(ids.tolist(), lat.tolist()))
+        detail.extend({"tag": mix[i][3], "method": mix[i][2], "served_ms": served_ms[i], "alone_ms": float(alone[i]),
+                       "arrival_s": float(arrivals[i])} for i in range(n_req))
     return {"rate_rps": rate if rate > 0 else None, "arrivals": "poisson" if rate > 0 else "all at once",
             "requests": n_req, "p50_ms": float(np.percentile(lat, 50)),
             "p99_ms": float(np.percentile(lat, 99)), "solves_per_s": n_req / wall,
@@ -423,6 +427,8 @@ def main():
                     help="only the served-loop legs (profiling aid; prints its own JSON line, not a bench line)")
     ap.add_argument("--served-rates", default="50,200,800,0",
                     help="with --served: arrival rates in req/s (0: every request at once)")
+    ap.add_argument("--served-detail", default="",
+                    help="with --served: write every request's tag and served / lone latency to this JSON file")
     args = ap.parse_args()
     if args.config1 > 0:
         config1_only(args)
@@ -438,7 +444,14 @@ def main():
 
         torch.cuda.set_device(0)
         rates = [int(x) for x in args.served_rates.split(",") if x]
-        legs = [served_loop(rate, {50: 100, 200: 200}.get(rate, 400), rate, P, instances, 0) for rate in rates]
+        detail = {}
+        legs = []
+        for rate in rates:
+            detail[str(rate)] = []
+            legs.append(served_loop(rate, {50: 100, 200: 200}.get(rate, 400), rate, P, instances, 0, detail[str(rate)]))
+        if args.served_detail:
+            with open(args.served_detail, "w") as f:
+                json.dump(detail, f)
         print(json.dumps({"served": legs}))
         return
 

@@ -259,7 +259,17 @@ int pmdd_resident_dd_copy(pmdd_resident *res, int32_t i, int32_t *layer_offsets,
  * whose DD alone exceeds the budget finishes at once with PMDD_ERR_OOM; one that runs
  * out of memory while running finishes with PMDD_ERR_OOM while the others continue
  * (the reference's GPU path returns NULL with a reason and the CLI exits,
- * src/pmdd/main.cpp:338-345, or lets a Thrust allocation exception escape). */
+ * src/pmdd/main.cpp:338-345, or lets a Thrust allocation exception escape).
+ *
+ * Lanes: a server runs two engines.  Requests whose DD has at most 2^17 arcs
+ * (PMDD_SERVER_HEAVY_ARCS) go to the light lane, on the device's highest-priority
+ * stream, which pmdd_server_run steps in the caller's thread; larger ones go to the
+ * heavy lane, which a worker thread of the server steps on its own while it has work,
+ * so small requests neither wait for a large one's steps nor queue behind its blocks.
+ * The light lane gets a quarter of the budget (at least half of it, up to 512 MB), the
+ * heavy lane the rest; max_slots applies to each lane.  A budget below 512 MB, or
+ * PMDD_SERVER_LANES=1: one engine with the whole budget, stepped by the caller.  A server's functions are called from one
+ * thread at a time. */
 typedef struct pmdd_server pmdd_server;
 
 typedef struct pmdd_result {
@@ -281,13 +291,16 @@ int pmdd_server_submit(pmdd_server *srv, const pmdd_dd *dd, const pmdd_options *
 /* Submits a TSP request by its cost matrices: the server uses its shared n-city MDD
  * structure (built on the device on first use) and uploads only the weight table. */
 int pmdd_server_submit_tsp(pmdd_server *srv, const pmdd_tsp *inst, const pmdd_options *opts, uint64_t req_id);
-/* Runs engine steps until at least one request completes or nothing is pending;
- * returns the number of results now waiting. */
+/* Runs light-lane steps until at least one request completes (in either lane), max_steps
+ * light-lane steps have run (0: no limit) or nothing is pending; while the light lane
+ * is idle it waits up to 2 ms at a time for the heavy lane.  Returns the number of
+ * results now waiting, or -1 after a CUDA failure of either lane. */
 int pmdd_server_run(pmdd_server *srv, int32_t max_steps);
 /* Non-blocking: 1 and fills *out if a finished result is available, else 0. */
 int pmdd_server_poll(pmdd_server *srv, pmdd_result *out);
 int pmdd_server_cancel(pmdd_server *srv, uint64_t req_id);
-/* Requests submitted but not yet finished (queued + running). */
+/* Requests submitted and not yet reported by pmdd_server_run (queued, running, or
+ * finished in the heavy lane while the caller was away). */
 int pmdd_server_pending(const pmdd_server *srv);
 
 /* Serving counters and memory figures since the server was created.  `rejected`:

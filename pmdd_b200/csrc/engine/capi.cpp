@@ -2,7 +2,10 @@
 #include <algorithm>
 #include <array>
 #include <atomic>
+#include <chrono>
 #include <climits>
+#include <condition_variable>
+#include <deque>
 #include <cstdlib>
 #include <cstring>
 #include <functional>
@@ -892,18 +895,165 @@ int pmdd_resident_dd_copy(pmdd_resident *R, int32_t i, int32_t *layer_offsets, i
 }
 
 // ------------------------------------------------------------------ serving
-struct pmdd_server {
+// A server runs two lanes, each an engine of its own (memory budget, CUDA stream).
+// Requests predicted to be small (heavy_request below: by DD arcs) go to the light lane, whose
+// stream has the device's highest priority and which the caller's thread steps inside
+// pmdd_server_run; the others go to the heavy lane, which a worker thread steps on its
+// own whenever it has work.  A small request then waits neither for a step of a large
+// one on the host nor behind its queued blocks on the GPU.  The heavy lane's engine is
+// touched only by its worker: the caller posts submissions, cancellations and
+// failure-injection settings as commands, and reads results and counters that the
+// worker publishes after every step.  PMDD_SERVER_LANES=1 keeps a single lane.
+namespace {
+
+struct HeavyLane {
     std::unique_ptr<pmdd::Engine> engine;
-    uint64_t submitted = 0;
+    std::thread worker;
+    std::mutex mu;                                   // guards everything below
+    std::condition_variable wake;                    // the worker: commands, or stop
+    std::condition_variable done;                    // the caller: a result, or idle
+    std::vector<std::function<void(pmdd::Engine &)>> cmds;
+    int64_t inbox_requests = 0;                      // submissions posted and not yet published
+                                                     // as queued or running
+    std::deque<std::unique_ptr<pmdd::Instance>> outbox;
+    // published by the worker after each pass
+    size_t queued = 0, running = 0;
+    pmdd::Engine::Counters counters{};
+    int64_t budget = 0, used = 0, peak = 0, growth = 0, injected = 0;
+    bool stop = false, failed = false, working = false;
+    std::string error;
+    int64_t posted_requests = 0;                     // submissions among cmds (the worker's share)
+
+    void post(std::function<void(pmdd::Engine &)> fn, bool request) {
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            cmds.push_back(std::move(fn));
+            if (request) {
+                ++inbox_requests;
+                ++posted_requests;
+            }
+        }
+        wake.notify_one();
+    }
+    bool busy_locked() const { return !cmds.empty() || working || queued + running > 0; }
+
+    void publish_locked() {
+        pmdd::Engine &E = *engine;
+        while (!E.finished().empty()) {
+            outbox.push_back(std::move(E.finished().front()));
+            E.finished().pop_front();
+        }
+        queued = E.queued();
+        running = E.running();
+        counters = E.counters();
+        budget = static_cast<int64_t>(E.arena().capacity());
+        used = static_cast<int64_t>(E.arena().used());
+        peak = static_cast<int64_t>(E.arena().peak());
+        growth = E.reserved_growth();
+        injected = E.arena().injected_failures();
+    }
+
+    void run_worker() {
+        for (;;) {
+            std::vector<std::function<void(pmdd::Engine &)>> batch;
+            int64_t batch_requests = 0;
+            {
+                std::unique_lock<std::mutex> lk(mu);
+                wake.wait(lk, [&] { return stop || !cmds.empty() || (!failed && !engine->idle()); });
+                if (stop) return;
+                batch.swap(cmds);
+                batch_requests = posted_requests;
+                posted_requests = 0;
+                working = true;
+            }
+            for (auto &fn : batch) fn(*engine);
+            int rc = 0;
+            if (!failed && !engine->idle()) rc = engine->step();
+            {
+                std::lock_guard<std::mutex> lk(mu);
+                if (rc < 0) {
+                    failed = true;
+                    error = engine->error();
+                }
+                publish_locked();
+                inbox_requests -= batch_requests;  // now counted by the engine (or finished)
+                working = false;
+            }
+            done.notify_all();
+        }
+    }
+
+    ~HeavyLane() {
+        if (worker.joinable()) {
+            {
+                std::lock_guard<std::mutex> lk(mu);
+                stop = true;
+            }
+            wake.notify_all();
+            worker.join();
+        }
+    }
 };
+
+}  // namespace
+
+struct pmdd_server {
+    std::unique_ptr<pmdd::Engine> engine;  // the light lane, or the only one
+    std::unique_ptr<HeavyLane> heavy;      // nullptr: one lane
+    std::deque<std::unique_ptr<pmdd::Instance>> ready;  // heavy-lane results handed over by run
+    std::unordered_map<uint64_t, int> heavy_ids;
+    uint64_t submitted = 0;
+    int64_t heavy_arcs = int64_t(1) << 17;
+};
+
+namespace {
+
+// A request goes to the heavy lane when its DD has more than srv->heavy_arcs arcs
+// (PMDD_SERVER_HEAVY_ARCS, default 2^17).  On the served mix (knapsack n 20..60, set
+// packing n 60..100, TSP 9..13 cities, three objectives) a request's lone latency grows
+// with its arcs: the 2^17 limit leaves requests of at most ~3 ms alone in the light lane
+// and sends the larger knapsacks (median ~6 ms alone, up to ~30 ms) to the heavy one.
+bool heavy_request(const pmdd_server *srv, int64_t arcs) {
+    return srv->heavy != nullptr && arcs > srv->heavy_arcs;
+}
+
+}  // namespace
 
 pmdd_server *pmdd_server_create(int32_t device, int64_t budget_bytes, int32_t max_slots, char *err, size_t errlen) {
     std::unique_ptr<pmdd_server> s(new pmdd_server);
     if (budget_bytes <= 0) budget_bytes = default_arena_bytes(device);
-    s->engine.reset(new pmdd::Engine(device, budget_bytes, max_slots));
+    const char *lanes = std::getenv("PMDD_SERVER_LANES");
+    // two lanes need a budget worth splitting (an engine takes at least 64 MB)
+    const bool two = !(lanes && lanes[0] == '1') && budget_bytes >= (int64_t(512) << 20);
+    const char *ha = std::getenv("PMDD_SERVER_HEAVY_ARCS");
+    if (ha && *ha) s->heavy_arcs = std::max<long long>(0, std::atoll(ha));
+    int prio_low = 0, prio_high = 0;
+    if (two && (cudaSetDevice(device) != cudaSuccess ||
+                cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high) != cudaSuccess)) {
+        write_err(err, errlen, std::string("CUDA error: ") + cudaGetErrorString(cudaGetLastError()));
+        return nullptr;
+    }
+    // the light lane: a quarter of the budget, but at least half of it up to 512 MB
+    const int64_t light = two ? std::max<int64_t>(budget_bytes / 4, std::min<int64_t>(budget_bytes / 2, int64_t(512) << 20))
+                              : budget_bytes;
+    s->engine.reset(new pmdd::Engine(device, light, max_slots, two ? prio_high : 0));
     if (!s->engine->ok()) {
         write_err(err, errlen, s->engine->error());
         return nullptr;
+    }
+    if (two) {
+        s->heavy.reset(new HeavyLane);
+        s->heavy->engine.reset(new pmdd::Engine(device, budget_bytes - light, max_slots, prio_low));
+        if (!s->heavy->engine->ok()) {
+            write_err(err, errlen, s->heavy->engine->error());
+            return nullptr;
+        }
+        {
+            std::lock_guard<std::mutex> lk(s->heavy->mu);
+            s->heavy->publish_locked();
+        }
+        HeavyLane *h = s->heavy.get();
+        h->worker = std::thread([h] { h->run_worker(); });
     }
     return s.release();
 }
@@ -923,10 +1073,37 @@ int pmdd_server_submit(pmdd_server *srv, const pmdd_dd *dd, const pmdd_options *
         srv->engine->finish_rejected(std::move(I));
         return rc;
     }
-    srv->engine->submit(std::move(I));
+    if (heavy_request(srv, I->A)) {
+        srv->heavy_ids[req_id] = 1;
+        auto holder = std::make_shared<std::unique_ptr<pmdd::Instance>>(std::move(I));
+        srv->heavy->post([holder](pmdd::Engine &E) { E.submit(std::move(*holder)); }, true);
+    } else {
+        srv->engine->submit(std::move(I));
+    }
     srv->submitted++;
     return PMDD_OK;
 }
+
+namespace {
+
+// A TSP request on one lane's engine (its shared n-city structure); the caller checked
+// the arguments.
+void submit_tsp_on(pmdd::Engine &E, int n, int nobjs, const int32_t *cost, const pmdd_options &o, uint64_t req_id) {
+    std::string msg;
+    const pmdd::TspStructure *S = E.tsp_structure(n, &msg);
+    std::unique_ptr<pmdd::Instance> I(new pmdd::Instance);
+    if (!S) {
+        I->id = req_id;
+        I->status = PMDD_ERR_OOM;
+        I->error = msg;
+        E.finish_rejected(std::move(I));
+        return;
+    }
+    pmdd::prepare_tsp_instance(*S, nobjs, cost, o, req_id, I.get());
+    E.submit(std::move(I));
+}
+
+}  // namespace
 
 int pmdd_server_submit_tsp(pmdd_server *srv, const pmdd_tsp *t, const pmdd_options *opts, uint64_t req_id) {
     if (!srv || !t || !t->cost || t->n < pmdd::dev::kTspMinCities || t->n > pmdd::dev::kTspMaxCities ||
@@ -937,36 +1114,89 @@ int pmdd_server_submit_tsp(pmdd_server *srv, const pmdd_tsp *t, const pmdd_optio
     else pmdd_options_default(&o);
     o.problem_type = 3;
     if ((o.method != 1 && o.method != 3) || o.maximization == 0) return PMDD_ERR_INVALID;
-    std::string msg;
-    const pmdd::TspStructure *S = srv->engine->tsp_structure(t->n, &msg);
-    std::unique_ptr<pmdd::Instance> I(new pmdd::Instance);
-    if (!S) {
-        I->id = req_id;
-        I->status = PMDD_ERR_OOM;
-        I->error = msg;
-        srv->engine->finish_rejected(std::move(I));
-        return PMDD_ERR_OOM;
+    // arcs of the n-city MDD, about: layer l (1..n-1) holds C(n-1, l) visited sets times
+    // l last cities, each state of layer l >= 2 with l - 1 parents
+    int64_t arcs = 0;
+    for (int l = 1; l < t->n; ++l) {
+        int64_t c = 1;
+        for (int k = 1; k <= l; ++k) c = c * (t->n - k) / k;  // C(n - 1, l), exact step by step
+        arcs += c * l * std::max(1, l - 1);
     }
-    pmdd::prepare_tsp_instance(*S, t->nobjs, t->cost, o, req_id, I.get());
-    srv->engine->submit(std::move(I));
+    if (heavy_request(srv, arcs)) {
+        srv->heavy_ids[req_id] = 1;
+        const int n = t->n, nobjs = t->nobjs;
+        auto cost = std::make_shared<std::vector<int32_t>>(t->cost, t->cost + static_cast<size_t>(nobjs) * n * n);
+        srv->heavy->post([n, nobjs, cost, o, req_id](pmdd::Engine &E) { submit_tsp_on(E, n, nobjs, cost->data(), o, req_id); },
+                         true);
+    } else {
+        submit_tsp_on(*srv->engine, t->n, t->nobjs, t->cost, o, req_id);
+    }
     srv->submitted++;
     return PMDD_OK;
 }
 
+namespace {
+
+// Moves the heavy lane's finished results to the caller's side (pmdd_server_run only,
+// so that a result is pending until a run call has reported it, as in one lane).
+size_t ready_results(pmdd_server *srv) {
+    if (srv->heavy) {
+        std::lock_guard<std::mutex> lk(srv->heavy->mu);
+        while (!srv->heavy->outbox.empty()) {
+            srv->ready.push_back(std::move(srv->heavy->outbox.front()));
+            srv->heavy->outbox.pop_front();
+        }
+    }
+    return srv->engine->finished().size() + srv->ready.size();
+}
+
+}  // namespace
+
 int pmdd_server_run(pmdd_server *srv, int32_t max_steps) {
     if (!srv) return -1;
     int steps = 0;
-    while ((max_steps <= 0 || steps < max_steps) && srv->engine->finished().empty() && !srv->engine->idle()) {
-        if (srv->engine->step() < 0) return -1;
-        ++steps;
+    pmdd::Engine &E = *srv->engine;
+    for (;;) {
+        const size_t ready = ready_results(srv);
+        if (ready > 0) return static_cast<int>(ready);
+        if (srv->heavy) {
+            std::lock_guard<std::mutex> lk(srv->heavy->mu);
+            if (srv->heavy->failed) return -1;
+        }
+        if (max_steps > 0 && steps >= max_steps) return 0;
+        if (!E.idle()) {
+            if (E.step() < 0) return -1;
+            ++steps;
+            continue;
+        }
+        if (!srv->heavy) return 0;
+        // the light lane is idle: wait a little for the heavy lane, so that the caller
+        // comes back soon to submit what arrived meanwhile
+        HeavyLane &H = *srv->heavy;
+        std::unique_lock<std::mutex> lk(H.mu);
+        if (H.outbox.empty() && !H.failed && H.busy_locked())
+            H.done.wait_for(lk, std::chrono::milliseconds(2),
+                            [&] { return !H.outbox.empty() || H.failed || !H.busy_locked(); });
+        const bool got = !H.outbox.empty(), failed = H.failed, busy = H.busy_locked();
+        lk.unlock();
+        if (got) return static_cast<int>(ready_results(srv));
+        if (failed) return -1;
+        if (!busy || max_steps > 0) return 0;
     }
-    return static_cast<int>(srv->engine->finished().size());
 }
 
 int pmdd_server_poll(pmdd_server *srv, pmdd_result *out) {
-    if (!srv || !out || srv->engine->finished().empty()) return 0;
-    std::unique_ptr<pmdd::Instance> I = std::move(srv->engine->finished().front());
-    srv->engine->finished().pop_front();
+    if (!srv || !out) return 0;
+    std::unique_ptr<pmdd::Instance> I;
+    if (!srv->engine->finished().empty()) {
+        I = std::move(srv->engine->finished().front());
+        srv->engine->finished().pop_front();
+    } else if (!srv->ready.empty()) {
+        I = std::move(srv->ready.front());
+        srv->ready.pop_front();
+    }
+    if (!I) return 0;
+    srv->heavy_ids.erase(I->id);
     std::memset(out, 0, sizeof(*out));
     out->req_id = I->id;
     out->submit_s = I->submit_s;
@@ -979,12 +1209,24 @@ int pmdd_server_poll(pmdd_server *srv, pmdd_result *out) {
 
 int pmdd_server_cancel(pmdd_server *srv, uint64_t req_id) {
     if (!srv) return PMDD_ERR_INVALID;
+    if (srv->heavy && srv->heavy_ids.count(req_id)) {
+        srv->heavy->post([req_id](pmdd::Engine &E) { E.cancel(req_id); }, false);
+        return PMDD_OK;
+    }
     return srv->engine->cancel(req_id) ? PMDD_OK : PMDD_ERR_INVALID;
 }
 
 int pmdd_server_pending(const pmdd_server *srv) {
     if (!srv) return 0;
-    return static_cast<int>(srv->engine->queued() + srv->engine->running());
+    size_t p = srv->engine->queued() + srv->engine->running();
+    if (srv->heavy) {
+        std::lock_guard<std::mutex> lk(srv->heavy->mu);
+        // results the worker has finished count until a run call hands them over: they
+        // arrive while the caller is away
+        p += static_cast<size_t>(srv->heavy->inbox_requests) + srv->heavy->queued + srv->heavy->running +
+             srv->heavy->outbox.size();
+    }
+    return static_cast<int>(p);
 }
 
 int pmdd_server_get_info(const pmdd_server *srv, pmdd_server_info *out) {
@@ -1007,12 +1249,34 @@ int pmdd_server_get_info(const pmdd_server *srv, pmdd_server_info *out) {
     out->peak_used_bytes = static_cast<int64_t>(E.arena().peak());
     out->reserved_growth_bytes = E.reserved_growth();
     out->injected_alloc_failures = E.arena().injected_failures();
+    if (srv->heavy) {  // both lanes: sums (peaks: the sum of the lanes' peaks)
+        std::lock_guard<std::mutex> lk(srv->heavy->mu);
+        const HeavyLane &H = *srv->heavy;
+        out->admitted += H.counters.admitted;
+        out->completed += H.counters.completed;
+        out->failed += H.counters.failed;
+        out->rejected += H.counters.rejected;
+        out->cancelled += H.counters.cancelled;
+        out->queued += static_cast<int32_t>(H.queued + static_cast<size_t>(H.inbox_requests));
+        out->running += static_cast<int32_t>(H.running);
+        out->queued_peak += static_cast<int32_t>(H.counters.queued_peak);
+        out->running_peak += static_cast<int32_t>(H.counters.running_peak);
+        out->budget_bytes += H.budget;
+        out->used_bytes += H.used;
+        out->peak_used_bytes += H.peak;
+        out->reserved_growth_bytes += H.growth;
+        out->injected_alloc_failures += H.injected;
+    }
     return PMDD_OK;
 }
 
 int pmdd_server_inject_alloc_failures(pmdd_server *srv, int64_t after, int64_t count) {
     if (!srv || after < 0 || count < 0) return PMDD_ERR_INVALID;
     srv->engine->inject_alloc_failures(after, count);
+    if (srv->heavy) {
+        // commands run in order: the setting applies before any later submission
+        srv->heavy->post([after, count](pmdd::Engine &E) { E.inject_alloc_failures(after, count); }, false);
+    }
     return PMDD_OK;
 }
 

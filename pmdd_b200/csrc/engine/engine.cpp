@@ -526,7 +526,8 @@ void layout_built_knapsack(Instance *I, int d, bool wide, const std::vector<int3
 }
 
 // ------------------------------------------------------------------ Engine
-Engine::Engine(int device, int64_t budget_bytes, int max_slots) : device_(device), max_slots_(max_slots) {
+Engine::Engine(int device, int64_t budget_bytes, int max_slots, int stream_priority)
+    : device_(device), max_slots_(max_slots) {
     const double init_t0 = now_s();
     struct InitTrace {
         const double &t0;
@@ -556,7 +557,8 @@ Engine::Engine(int device, int64_t budget_bytes, int max_slots) : device_(device
         return;
     }
     sms_ = prop.multiProcessorCount;
-    if (!cuda_ok(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate")) return;
+    if (!cuda_ok(cudaStreamCreateWithPriority(&stream_, cudaStreamNonBlocking, stream_priority), "cudaStreamCreate"))
+        return;
     for (cudaEvent_t &ev : ev_)
         if (!cuda_ok(cudaEventCreate(&ev), "cudaEventCreate")) return;
     size_t free_b = 0, total_b = 0;

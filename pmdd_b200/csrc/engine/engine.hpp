@@ -208,7 +208,9 @@ struct KernelTimes {
 
 class Engine {
   public:
-    Engine(int device, int64_t budget_bytes, int max_slots);
+    // stream_priority: the engine stream's CUDA priority (0: default; lower numbers are
+    // higher priorities, as cudaDeviceGetStreamPriorityRange gives them).
+    Engine(int device, int64_t budget_bytes, int max_slots, int stream_priority = 0);
     ~Engine();
     bool ok() const { return ok_; }
     const std::string &error() const { return error_; }

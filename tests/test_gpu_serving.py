@@ -7,10 +7,18 @@
 * A small budget makes requests queue; a request that cannot fit finishes with
   PMDD_ERR_OOM while the others finish correctly (the reference's GPU path returns
   NULL and its CLI exits, src/pmdd/main.cpp:338-345).
-* Cancelling a queued and a running request finishes both with PMDD_ERR_CANCELLED.
+* Cancelling a queued and a running request of the light lane, and a running one of the
+  heavy lane, finishes them with PMDD_ERR_CANCELLED.
 * Device allocations failed by the server's test hook fail requests with PMDD_ERR_OOM,
   never the server: every other result stays exact and later requests are served.
+* The two lanes: small requests (DDs of at most 2^17 arcs) submitted beside a large one
+  (a 4-objective knapsack n=60) finish before it, each equal to its lone frontier; a
+  request run until nothing is pending is then polled, in either lane; with
+  PMDD_SERVER_LANES=1 (one engine, in a child process) the same requests give the same
+  frontiers.
 """
+import json
+
 import numpy as np
 import pytest
 
@@ -71,7 +79,7 @@ def test_served_mix_equals_alone_and_reference():
             [(2, instances.setpacking_text(60 + 5 * i, 20, 3, 910 + i), 3, f"sp3_m3_{i}") for i in range(4)] + \
             [(3, instances.tsp_text(9 + i % 2, 3, 920 + i), 1, f"tsp3_n{9 + i % 2}_s{920 + i}") for i in range(4)]
     reqs += [_request(p, t, m, tag) for p, t, m, tag in extra]
-    srv = P.Server(budget_bytes=1 << 30, max_slots=12)
+    srv = P.Server(budget_bytes=1 << 30, max_slots=4)  # per lane: a queue forms
     try:
         got = _drive(srv, reqs, np.random.default_rng(7))
         info = srv.info()
@@ -116,16 +124,18 @@ def test_budget_queues_requests_and_fails_only_the_one_that_cannot_fit():
 
 
 def test_cancel_queued_and_running_requests():
+    # a, b, c: light lane (77011, 63097, 47735 arcs); d: heavy lane (673929 arcs, ~30 ms)
     a = P.DecisionDiagram.from_text(instances.setpacking_text(100, 20, 3, 3), 2, 3)
-    b = P.DecisionDiagram.from_text(instances.knapsack_text(40, 3, 4), 1, 3)
-    c = P.DecisionDiagram.from_text(instances.knapsack_text(30, 3, 5), 1, 3)
+    b = P.DecisionDiagram.from_text(instances.knapsack_text(30, 3, 5), 1, 3)
+    c = P.DecisionDiagram.from_text(instances.knapsack_text(28, 3, 6), 1, 3)
+    d = P.DecisionDiagram.from_text(instances.knapsack_text(60, 4, 0), 1, 4)
     srv = P.Server(max_slots=2)
     try:
-        for rid, dd in enumerate((a, b, c)):
+        for rid, dd in enumerate((a, b, c, d)):
             assert srv.submit(dd, rid, method=1) == 0
         srv.run(1)
-        assert srv.info()["running"] == 2 and srv.info()["queued"] == 1
-        assert srv.cancel(2) and srv.cancel(0)
+        assert srv.info()["running"] >= 2 and srv.info()["queued"] >= 1
+        assert srv.cancel(2) and srv.cancel(0) and srv.cancel(3)
         got = {}
         while srv.pending() > 0:
             srv.run(0)
@@ -136,10 +146,10 @@ def test_cancel_queued_and_running_requests():
         info = srv.info()
     finally:
         srv.close()
-    assert got[0].status == CANCELLED and got[2].status == CANCELLED
+    assert got[0].status == CANCELLED and got[2].status == CANCELLED and got[3].status == CANCELLED
     assert got[1].status == OK
     assert frontier_digest(got[1].frontier) == frontier_digest(oracle.enumerate(b, 1))
-    assert info["cancelled"] == 2
+    assert info["cancelled"] == 3
 
 
 @pytest.mark.parametrize("count", [1, 20, 200])
@@ -182,3 +192,79 @@ def test_injected_allocation_failures_fail_requests_not_the_server(count):
     assert OK in outcomes
     if count >= 20:
         assert OOM in outcomes
+
+
+LANE_CHILD = r"""
+import json, sys
+sys.path.insert(0, {root!r})
+sys.path.insert(0, {tests!r})
+import pmdd_b200 as P
+from conftest import frontier_digest
+from test_gpu_serving import _lane_requests, _drive_all
+srv = P.Server()
+out = _drive_all(srv, _lane_requests())
+srv.close()
+print(json.dumps({{str(k): frontier_digest(r.frontier) for k, r in out.items()}}))
+"""
+
+
+def _lane_requests():
+    """A large request first (4-objective knapsack n=60, heavy lane), then small ones
+    (TSP 9 cities by method 3, knapsack n=30 and set packing n=70: light lane)."""
+    big = P.DecisionDiagram.from_text(instances.knapsack_text(60, 4, 0), 1, 4)
+    small = [_request(3, instances.tsp_text(9, 3, 930 + i), 3, f"tsp3_n9_s{930 + i}") for i in range(4)] + \
+            [_request(1, instances.knapsack_text(30, 3, 940 + i), 1, "") for i in range(3)] + \
+            [_request(2, instances.setpacking_text(70, 20, 3, 950 + i), 1, "") for i in range(3)]
+    return [("dd", big, 1, big)] + small
+
+
+def _drive_all(srv, reqs):
+    for i, r in enumerate(reqs):
+        _submit(srv, r, i)
+    out = {}
+    while len(out) < len(reqs):
+        assert srv.run(0) >= 0
+        while (x := srv.poll()) is not None:
+            out[x.req_id] = x
+    return out
+
+
+def test_small_requests_pass_a_large_one():
+    import subprocess
+    import sys
+
+    from conftest import ROOT
+
+    reqs = _lane_requests()
+    srv = P.Server()
+    try:
+        got = _drive_all(srv, reqs)
+    finally:
+        srv.close()
+    for i, (kind, payload, method, dd) in enumerate(reqs):
+        assert got[i].status == OK, (i, got[i].error)
+        assert frontier_digest(got[i].frontier) == frontier_digest(P.enumerate_dd(dd, method=method)), i
+    # every small request finished before the large one that was submitted first
+    assert max(got[i].finish_s for i in range(1, len(reqs))) < got[0].finish_s
+    # run until nothing is pending, then poll: a heavy-lane result is pending until a run
+    # call has reported it (bounded loop: a regression must fail, not hang)
+    srv = P.Server()
+    try:
+        for i in (0, 1):
+            _submit(srv, reqs[i], 100 + i)
+            for _ in range(200000):
+                if srv.pending() == 0:
+                    break
+                srv.run(0)
+            assert srv.pending() == 0
+            x = srv.poll()
+            assert x is not None and x.req_id == 100 + i and x.status == OK
+            assert frontier_digest(x.frontier) == frontier_digest(got[i].frontier)
+    finally:
+        srv.close()
+    env = dict(__import__("os").environ, PMDD_SERVER_LANES="1")
+    p = subprocess.run([sys.executable, "-c", LANE_CHILD.format(root=ROOT, tests=__import__("os").path.join(ROOT, "tests"))],
+                       env=env, capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stdout + p.stderr
+    one = json.loads(p.stdout.strip().splitlines()[-1])
+    assert one == {str(i): frontier_digest(got[i].frontier) for i in range(len(reqs))}
