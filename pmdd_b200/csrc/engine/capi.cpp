@@ -6,6 +6,7 @@
 #include <climits>
 #include <condition_variable>
 #include <deque>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <functional>
@@ -387,18 +388,29 @@ int pmdd_enumerate_batch(const pmdd_dd *dds, int32_t count, const pmdd_options *
         for (int32_t i = 0; i < count; ++i) std::memset(&outs[i], 0, sizeof(outs[i]));
     std::vector<std::unique_ptr<pmdd::Instance>> reqs;
     std::string msg;
+    const auto t0 = std::chrono::steady_clock::now();
     int rc = prepare_all(dds, count, o, false, reqs, status, &msg);
     if (rc != PMDD_OK) {
         write_err(err, errlen, count > 1 ? msg : "instance 0: " + msg);
         return rc;
     }
+    const auto t1 = std::chrono::steady_clock::now();
     RunInfo info;
     rc = run_on_device(o.device, reqs, &info, &msg, dds);
     if (rc != PMDD_OK) {
         write_err(err, errlen, msg);
         return rc;
     }
-    return collect_batch(reqs, outs, status, stats, info, err, errlen);
+    const auto t2 = std::chrono::steady_clock::now();
+    rc = collect_batch(reqs, outs, status, stats, info, err, errlen);
+    const char *tr = std::getenv("PMDD_TRACE");
+    if (tr && tr[0] == '1') {
+        const auto t3 = std::chrono::steady_clock::now();
+        auto ms = [](std::chrono::steady_clock::duration d) { return std::chrono::duration<double, std::milli>(d).count(); };
+        std::fprintf(stderr, "[pmdd batch] count=%d prepare_ms=%.1f run_ms=%.1f collect_ms=%.1f\n", count, ms(t1 - t0),
+                     ms(t2 - t1), ms(t3 - t2));
+    }
+    return rc;
 }
 
 // ------------------------------------------------------- standalone filter

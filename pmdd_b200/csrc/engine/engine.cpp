@@ -582,13 +582,17 @@ Engine::Engine(int device, int64_t budget_bytes, int max_slots, int stream_prior
     if (bm && *bm && std::atoll(bm) > 0) big_mark_min_fixed_ = std::atoll(bm);
     load_tuning();
     // constant initial frontier: one zero point (up to 8 int64 values), offset 0, size 1
-    if (!h_init_.reserve(256)) {
+    if (!h_init_.reserve(512)) {
         error_ = "cudaMallocHost failed";
         return;
     }
-    std::memset(h_init_.p, 0, 256);
+    std::memset(h_init_.p, 0, 512);
     *reinterpret_cast<int32_t *>(static_cast<char *>(h_init_.p) + 128) = 1;  // size of the root frontier
     *(static_cast<unsigned char *>(h_init_.p) + 132) = 1;                   // one point is sorted
+    // the seed side of an admitted request, one block: the zero point (64 B) | slot offset
+    // 0 | size 1 | sorted 1
+    *reinterpret_cast<int32_t *>(static_cast<char *>(h_init_.p) + kSeedTemplate + 72) = 1;
+    *(static_cast<unsigned char *>(h_init_.p) + kSeedTemplate + 76) = 1;
     const char *lx = std::getenv("PMDD_LEX_TILES");
     if (lx && lx[0] == '0') lex_tiles_ = false;
     const char *lb = std::getenv("PMDD_LEX_BULK");
@@ -923,15 +927,16 @@ bool Engine::admit(Instance &I) {
     auto seed = [&](Side &s, int layer) -> bool {
         s.layer = layer;
         s.slot_points = 1;
-        s.pts = arena_.alloc(8 * 8);
-        s.off = static_cast<int64_t *>(arena_.alloc(sizeof(int64_t)));
-        s.size = static_cast<int32_t *>(arena_.alloc(2 * sizeof(int32_t)));  // size | sorted flag
-        if (!s.pts || !s.off || !s.size) return false;
-        s.sorted = reinterpret_cast<uint8_t *>(s.size + 1);
-        const char *h = static_cast<const char *>(h_init_.p);
-        cudaMemcpyAsync(s.pts, h, 64, cudaMemcpyHostToDevice, stream_);
-        cudaMemcpyAsync(s.off, h + 64, sizeof(int64_t), cudaMemcpyHostToDevice, stream_);
-        cudaMemcpyAsync(s.size, h + 128, 2 * sizeof(int32_t), cudaMemcpyHostToDevice, stream_);
+        // one block (released through pts; the arena ignores the releases of off and size):
+        // the zero point | slot offset | size | sorted flag, written by one copy
+        char *b = static_cast<char *>(arena_.alloc(kSeedBytes));
+        if (!b) return false;
+        s.pts = b;
+        s.off = reinterpret_cast<int64_t *>(b + 64);
+        s.size = reinterpret_cast<int32_t *>(b + 72);
+        s.sorted = reinterpret_cast<uint8_t *>(b + 76);
+        cudaMemcpyAsync(b, static_cast<const char *>(h_init_.p) + kSeedTemplate, kSeedBytes, cudaMemcpyHostToDevice,
+                        stream_);
         s.counted = false;
         s.score = 0;
         return true;

@@ -314,6 +314,7 @@ class Engine {
     std::vector<void *> step_scratch_;
     Pinned h_desc_, h_summary_, h_init_, h_stage_;
     Pinned h_results_;  // the frontiers of the requests a step finishes, fetched together
+    static constexpr size_t kSeedTemplate = 256, kSeedBytes = 80;  // seed side template in h_init_
 
     int64_t launches_ = 0;
     KernelTimes ktimes_;
