@@ -30,7 +30,8 @@ __global__ void __launch_bounds__(kChainThreads) chain_prep_kernel(ChainPrep P) 
     if (i < P.n) {
         const CountResult r = P.prev[P.prev_idx != nullptr ? P.prev_idx[i] : i];
         ExpandJob &J = P.jobs[i];
-        const bool stop = P.stop[i] != 0 || P.layer > P.last[i] || r.num_big > 0 || r.total > P.cap[i];
+        const bool stop = P.stop[i] != 0 || P.layer > P.last[i] || r.num_big > 0 || r.total > P.cap[i] ||
+                          !chain_side_goes_on(r.total, P.other_score[i], P.bu[i] != 0);
         if (stop) {
             if (P.stop[i] == 0) {
                 P.stop[i] = 1;

@@ -160,7 +160,14 @@ struct CountJob {
     int32_t last;                  // the request's last chained layer
     int32_t slot;                  // the request's index in the launch (= block)
     int32_t chain_n;               // requests (blocks) in the launch
+    int32_t bu;                    // the chained side is the bottom-up one (method 3)
+    int64_t other_score;           // the other side's score (ChainPrep::other_score)
 };
+
+// Whether a chained side goes on after a count of `total` candidates (see ChainPrep).
+__host__ __device__ inline bool chain_side_goes_on(int64_t total, int64_t other_score, bool bu) {
+    return bu ? other_score > static_cast<int64_t>(1.5 * static_cast<double>(total)) : total <= other_score;
+}
 
 struct CountResult {
     int64_t total;       // candidates of the next layer
@@ -184,6 +191,12 @@ struct ChainPrep {
     int32_t *stopped_at;           // [n] the layer at which it stopped (0: never)
     const int64_t *cap;            // [n] candidates its chained frontier buffers hold
     const int32_t *last;           // [n] its last chained layer
+    // [n] method 3: a chain goes on while the host would pick the same side again, its
+    // new score against the other side's (other_score; INT64_MAX for method 1): top-down
+    // (bu 0) while candidates <= other_score, bottom-up (bu 1) while other_score >
+    // 1.5 * candidates (the engine's side rule, Engine::step)
+    const int64_t *other_score;
+    const int32_t *bu;
     int32_t layer;                 // this layer, from 1
     int32_t n;
 };

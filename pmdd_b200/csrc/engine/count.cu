@@ -27,7 +27,7 @@ __device__ void chain_next(const CountJob &J, bool skip, int64_t *warp_buf, int6
         bool stop = skip || J.next_layer > J.last;
         if (!stop) {
             const CountResult r = *J.result;  // written by this block's thread 0
-            stop = r.num_big > 0 || r.total > J.cap;
+            stop = r.num_big > 0 || r.total > J.cap || !chain_side_goes_on(r.total, J.other_score, J.bu != 0);
             if (!stop) {
                 tiles = r.total > 0 ? (r.total + N.tile_window - 1) / N.tile_window : 1;
                 N.total_cand = r.total;

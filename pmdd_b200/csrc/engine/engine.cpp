@@ -995,6 +995,8 @@ struct ChainSlot {
     const ExpPlan *e = nullptr;    // this step's expansion of the request
     size_t count_idx = 0;          // this step's count of the layer after it
     int32_t last = 0;              // chained layers at most (the terminal layer included)
+    int32_t dir = 1;               // +1: the top-down side; -1: the bottom-up one (method 3)
+    int64_t other_score = INT64_MAX;  // method 3: the other side's score (the side rule)
     int64_t cap = 0;               // candidates a frontier buffer holds
     int64_t ntiles = 0;            // tiles a chained layer may need
     int32_t vmax = 0, amax = 0;    // most nodes / in-arcs of a chained layer
@@ -1488,29 +1490,48 @@ int Engine::step() {
     if (chain_layers_ > 0 && count_alloc_ok && static_cast<int64_t>(exps.size()) <= chain_max_requests_) {
         for (size_t k = 0; k < counts.size(); ++k) {
             const CountPlan &cp = counts[k];
-            if (!cp.after_expand || !cp.td) continue;
+            if (!cp.after_expand) continue;
             Instance &I = *cp.I;
-            if (I.opts.method != 1 || I.opts.state_dominance > 0 || I.phase != Instance::RUNNING) continue;
-            const int32_t ei = exp_index(I, true);
+            if (I.opts.state_dominance > 0 || I.phase != Instance::RUNNING) continue;
+            if (I.opts.method != 1 && I.opts.method != 3) continue;
+            if (I.opts.method == 1 && !cp.td) continue;
+            const int32_t ei = exp_index(I, cp.td);
             const ExpPlan *e = ei >= 0 ? &exps[ei] : nullptr;
             if (e == nullptr || e->cand > chain_max_cand_) continue;
+            if (I.chain_skip > 0) {  // its last chain went nowhere (method 3): wait a little
+                --I.chain_skip;
+                continue;
+            }
             ChainSlot c;
             c.I = &I;
             c.e = e;
             c.count_idx = k;
+            c.dir = cp.td ? 1 : -1;
             // longer chains delay whatever else waits for the step: beyond the base length
             // only for a request the engine runs alone
-            int32_t want = I.chain_len > 0 ? I.chain_len : chain_layers_;
+            int32_t want = I.chain_len > 0 ? I.chain_len : (I.opts.method == 3 ? 2 : chain_layers_);
             if (!chain_grow_all_ && !(active_.size() == 1 && queued_.empty())) want = std::min(want, chain_layers_);
-            c.last = std::min<int32_t>(want, I.L - 1 - e->nl);
+            if (I.opts.method == 1) {
+                c.last = std::min<int32_t>(want, I.L - 1 - e->nl);
+            } else {
+                // method 3: the same side while the side rule picks it (checked on the
+                // device), and stopping one layer short of the other side (the meeting
+                // expansion and the cutset join are ordinary steps)
+                const Side &o = cp.td ? I.bu : I.td;
+                c.other_score = o.score;
+                c.last = std::min<int32_t>(want, (cp.td ? o.layer - e->nl : e->nl - o.layer) - 1);
+            }
             if (c.last <= 0) continue;
             c.cap = std::min<int64_t>(std::max<int64_t>(8 * std::max<int64_t>(e->cand, 1), 16384), int64_t(1) << 22);
             c.ntiles = c.cap / e->window + 2;
             for (int j = 1; j <= c.last; ++j) {
-                c.vmax = std::max(c.vmax, I.nodes_in(e->nl + j));
-                if (e->nl + j < I.L - 1) {
-                    c.amax = std::max(c.amax, I.arc_at_layer[e->nl + j + 2] - I.arc_at_layer[e->nl + j + 1]);
-                    c.cmax = std::max(c.cmax, I.nodes_in(e->nl + j + 1));
+                const int x = e->nl + c.dir * j;  // the layer chained layer j writes
+                c.vmax = std::max(c.vmax, I.nodes_in(x));
+                const int y = x + c.dir;          // the layer its count counts
+                if (y >= 0 && y <= I.L - 1) {
+                    c.amax = std::max(c.amax, c.dir > 0 ? I.arc_at_layer[y + 1] - I.arc_at_layer[y]
+                                                        : I.arc_at_layer[y + 2] - I.arc_at_layer[y + 1]);
+                    c.cmax = std::max(c.cmax, I.nodes_in(y));
                 }
             }
             bool okc = true;
@@ -1550,7 +1571,7 @@ int Engine::step() {
             g.layer_bytes = align256(sizeof(dev::ExpandJob) * n) + 2 * align256(sizeof(int64_t) * n) +
                             align256(sizeof(dev::CountJob) * n);
             g.st_off = stage_bytes;
-            stage_bytes += g.layer_bytes * static_cast<size_t>(g.layers) + align256(sizeof(int64_t) * n) + 2 * g.n4();
+            stage_bytes += g.layer_bytes * static_cast<size_t>(g.layers) + 2 * align256(sizeof(int64_t) * n) + 3 * g.n4();
             g.dv_off = chain_dev_bytes;
             g.dv_bytes = g.bytes();
             chain_dev_bytes += g.dv_bytes;
@@ -1698,16 +1719,25 @@ int Engine::step() {
                     C.last = c.last;
                     C.slot = static_cast<int32_t>(i);
                     C.chain_n = static_cast<int32_t>(n);
+                    C.bu = c.dir < 0 ? 1 : 0;
+                    C.other_score = c.other_score;
                 }
                 C.arc_cand_off = c.arc[b];
                 C.big_list = c.big[b];
                 J.tile_first = c.size[b];
                 if (j > c.last) continue;  // past its last layer: the prep stops it
-                const int cur = c.e->nl + j - 1, nl = cur + 1;
-                J.item_arc_off = I.d_in_off;
-                J.arc_nbr = I.d_arc_src;
-                J.arc_wrow = I.d_arc_w;
-                J.arc_base = I.arc_at_layer[nl];
+                const int cur = c.e->nl + c.dir * (j - 1), nl = cur + c.dir;
+                if (c.dir > 0) {
+                    J.item_arc_off = I.d_in_off;
+                    J.arc_nbr = I.d_arc_src;
+                    J.arc_wrow = I.d_arc_w;
+                    J.arc_base = I.arc_at_layer[nl];
+                } else {
+                    J.item_arc_off = I.d_out_off;
+                    J.arc_nbr = I.d_out_head;
+                    J.arc_wrow = I.d_out_w;
+                    J.arc_base = I.arc_at_layer[nl + 1];
+                }
                 J.weights = I.d_weights;
                 J.arc_cand_off = j == 1 ? new_arc_off[c.count_idx] : c.arc[pb];
                 J.item_base = I.layer_off[nl];
@@ -1729,13 +1759,21 @@ int Engine::step() {
                 J.lex_max_arcs = lex_max_arcs_;
                 g.items[j] += J.num_items;
                 g.tiles[j] += c.ntiles;
-                if (nl < I.L - 1) {  // the count of the layer after it (none at the terminal)
-                    C.item_arc_off = I.d_in_off;
-                    C.arc_nbr = I.d_arc_src;
-                    C.arc_base = I.arc_at_layer[nl + 1];
-                    C.num_arcs = I.arc_at_layer[nl + 2] - I.arc_at_layer[nl + 1];
-                    C.item_base = I.layer_off[nl + 1];
-                    C.num_items = I.nodes_in(nl + 1);
+                const int y = nl + c.dir;  // the layer after it in this direction
+                if (y >= 0 && y <= I.L - 1) {  // its count (none past the terminal)
+                    if (c.dir > 0) {
+                        C.item_arc_off = I.d_in_off;
+                        C.arc_nbr = I.d_arc_src;
+                        C.arc_base = I.arc_at_layer[y];
+                        C.num_arcs = I.arc_at_layer[y + 1] - I.arc_at_layer[y];
+                    } else {
+                        C.item_arc_off = I.d_out_off;
+                        C.arc_nbr = I.d_out_head;
+                        C.arc_base = I.arc_at_layer[y + 1];
+                        C.num_arcs = I.arc_at_layer[y + 2] - I.arc_at_layer[y + 1];
+                    }
+                    C.item_base = I.layer_off[y];
+                    C.num_items = I.nodes_in(y);
                     C.cur_base = I.layer_off[nl];
                     C.cur_nodes = I.nodes_in(nl);
                     C.cur_size = c.size[b];
@@ -1746,10 +1784,14 @@ int Engine::step() {
         int64_t *hcap = reinterpret_cast<int64_t *>(hp);
         int32_t *hlast = reinterpret_cast<int32_t *>(hp + align256(sizeof(int64_t) * n));
         int32_t *hidx = reinterpret_cast<int32_t *>(hp + align256(sizeof(int64_t) * n) + g.n4());
+        int64_t *hother = reinterpret_cast<int64_t *>(hp + align256(sizeof(int64_t) * n) + 2 * g.n4());
+        int32_t *hbu = reinterpret_cast<int32_t *>(hp + 2 * align256(sizeof(int64_t) * n) + 2 * g.n4());
         for (size_t i = 0; i < n; ++i) {
             hcap[i] = g.slots[i].cap;
             hlast[i] = g.slots[i].last;
             hidx[i] = static_cast<int32_t>(g.slots[i].count_idx);
+            hother[i] = g.slots[i].other_score;
+            hbu[i] = g.slots[i].dir < 0 ? 1 : 0;
         }
     }
 
@@ -1978,6 +2020,8 @@ int Engine::step() {
                 P.stopped_at = reinterpret_cast<int32_t *>(dv + g.off_stopped());
                 P.cap = reinterpret_cast<const int64_t *>(dp);
                 P.last = reinterpret_cast<const int32_t *>(dp + align256(sizeof(int64_t) * n));
+                P.other_score = reinterpret_cast<const int64_t *>(dp + align256(sizeof(int64_t) * n) + 2 * g.n4());
+                P.bu = reinterpret_cast<const int32_t *>(dp + 2 * align256(sizeof(int64_t) * n) + 2 * g.n4());
                 P.layer = j;
                 P.n = static_cast<int32_t>(n);
                 if (j == 1) {  // later layers are sized and planned by the count before them
@@ -2171,14 +2215,21 @@ int Engine::step() {
             Instance &I = *c.I;
             const int32_t done = stopped[i] == 0 ? c.last : stopped[i] - 1;
             // next chain: twice as long after one that ran to its end, one layer past
-            // where it stopped otherwise
-            I.chain_len = done == c.last ? std::min(kChainMaxLayers, 2 * std::max(c.last, chain_layers_))
-                                         : std::max(1, done + 1);
+            // where it stopped otherwise.  Method 3 grows from its last length and, after a
+            // chain that went nowhere (the other side was due at once), skips two steps:
+            // its sides alternate, and a chain that stops at once only costs launches.
+            if (I.opts.method == 3) {
+                I.chain_len = done == c.last ? std::min(kChainMaxLayers, 2 * c.last) : std::max(1, done + 1);
+                if (done == 0) I.chain_skip = 2;
+            } else {
+                I.chain_len = done == c.last ? std::min(kChainMaxLayers, 2 * std::max(c.last, chain_layers_))
+                                             : std::max(1, done + 1);
+            }
             if (I.phase != Instance::RUNNING || done <= 0) {
                 release_slot(c);
                 continue;
             }
-            Side &s = I.td;
+            Side &s = c.dir > 0 ? I.td : I.bu;
             int64_t C = 0;
             for (int j = 1; j <= done; ++j) {
                 C = j == 1 ? hres[c.count_idx].total : R[static_cast<size_t>(j - 2) * n + i].total;
@@ -2189,9 +2240,11 @@ int Engine::step() {
                 I.stats.work_tile_candidates_total += C;
                 I.stats.work_tile_survivors_total += static_cast<int64_t>(ts[t]);
                 I.stats.work_stair_candidates_total += static_cast<int64_t>(ts[t + 1]);
-                I.stats.layers_td++;
+                if (c.dir > 0) I.stats.layers_td++;
+                else I.stats.layers_bu++;
                 I.stats.work_chained_layers++;
-                if (c.e->nl + j < I.L - 1) {
+                const int y = c.e->nl + c.dir * (j + 1);  // the layer its count counted
+                if (y >= 0 && y <= I.L - 1) {
                     const int64_t surv = R[static_cast<size_t>(j - 1) * n + i].cur_total;
                     I.stats.work_frontier_survivors_total += surv;
                     I.stats.work_frontier_peak_points = std::max(I.stats.work_frontier_peak_points, surv);
@@ -2210,9 +2263,9 @@ int Engine::step() {
             s.off = c.off[b];
             s.size = c.size[b];
             s.sorted = c.sorted(b);
-            s.layer = c.e->nl + done;
+            s.layer = c.e->nl + c.dir * done;
             s.slot_points = std::max<int64_t>(C, 1);
-            if (s.layer == I.L - 1) {  // the terminal: its frontier is the result
+            if (I.opts.method == 1 && s.layer == I.L - 1) {  // the terminal: its frontier is the result
                 arena_.release(c.arc[b]);
                 arena_.release(c.big[b]);
                 s.arc_off = nullptr;
@@ -2230,7 +2283,7 @@ int Engine::step() {
                 s.big_list = c.big[b];
                 s.res = R[static_cast<size_t>(done - 1) * n + i];
                 s.counted = true;
-                s.score = s.res.total;
+                s.score = c.dir > 0 ? s.res.total : static_cast<int64_t>(1.5 * static_cast<double>(s.res.total));
             }
         }
     }

@@ -154,6 +154,7 @@ struct Instance {
     int64_t max_layer_arcs = 0, max_layer_nodes = 0;
     int32_t skipped = 0;                // admission passes this request was passed over
     int32_t chain_len = 0;              // layers its next chained step tries (0: the engine's base)
+    int32_t chain_skip = 0;             // eligible steps to pass over before the next chain
     bool external_dd = false;           // DD already resident (owned by a pmdd_resident set)
     const TspStructure *tsp = nullptr;  // TSP MDD: structure shared, I.dd holds the weight table only
     bool with_out_csr = false;          // device copy carries the bottom-up CSR

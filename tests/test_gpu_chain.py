@@ -10,7 +10,10 @@ the layer before (count.cu), the first by chain_prep_kernel and tile_plan_kernel
 every setting the frontiers of the golden fixtures equal the reference's, and those of
 seeded knapsack (3, 4 and 7 objectives), set-packing and TSP instances, alone and in
 mixed batches of two objective counts, equal the oracle's; the chained settings report
-chained layers, chaining off reports none.
+chained layers, chaining off reports none.  Method 3 chains a side only while the side
+rule would pick it again and stops a layer short of the other side, so its frontiers
+equal the oracle's and its cutset layer and per-side layer counts equal those of the run
+without chaining.
 """
 import json
 import os
@@ -49,7 +52,7 @@ import oracle
 import pmdd_b200 as P
 from conftest import golden_cases, golden_frontier, frontier_digest
 from test_gpu_chain import SINGLE, BATCH, _text
-out = {{"golden": 0, "single": [], "batch": [], "chained": 0}}
+out = {{"golden": 0, "single": [], "batch": [], "chained": 0, "m3": [], "m3_shape": []}}
 for rec in golden_cases():
     dd = P.DecisionDiagram.from_file(rec["dat"], rec["problem_type"], rec["nobjs"])
     for m in rec["methods"]:
@@ -63,6 +66,11 @@ for pt, kind, n, d, seed in SINGLE:
     st = {{}}
     got = P.enumerate_dd(dd, method=1, stats=st)
     out["single"].append(frontier_digest(got))
+    out["chained"] += st["work_chained_layers"]
+    st = {{}}
+    got = P.enumerate_dd(dd, method=3, stats=st)
+    out["m3"].append(frontier_digest(got))
+    out["m3_shape"].append([st["layer_coupling"], st["layers_td"], st["layers_bu"]])
     out["chained"] += st["work_chained_layers"]
 dds = [P.DecisionDiagram.from_text(_text(kind, n, d, seed), pt, d) for pt, kind, n, d, seed in BATCH]
 st = {{}}
@@ -90,7 +98,14 @@ def want():
               for pt, k, n, d, s in SINGLE]
     batch = [frontier_digest(oracle.enumerate(P.DecisionDiagram.from_text(_text(k, n, d, s), pt, d), 1))
              for pt, k, n, d, s in BATCH]
-    return single, batch
+    m3 = [frontier_digest(oracle.enumerate(P.DecisionDiagram.from_text(_text(k, n, d, s), pt, d), 3))
+          for pt, k, n, d, s in SINGLE]
+    return single, batch, m3
+
+
+@pytest.fixture(scope="module")
+def unchained():
+    return _run({"PMDD_CHAIN_LAYERS": "0"})
 
 
 @pytest.mark.parametrize("env,chained", [({"PMDD_CHAIN_LAYERS": "0"}, False), ({}, True),
@@ -98,9 +113,11 @@ def want():
                                          ({"PMDD_CHAIN_LAYERS": "64", "PMDD_CHAIN_MAX_CAND": str(1 << 40),
                                            "PMDD_CHAIN_GROW": "all"}, True)],
                          ids=["off", "default", "one-layer", "long-chains"])
-def test_chained_steps_give_the_same_frontiers(env, chained, want):
+def test_chained_steps_give_the_same_frontiers(env, chained, want, unchained):
     got = _run(env)
     assert got["golden"] > 10
     assert got["single"] == want[0]
     assert got["batch"] == want[1]
+    assert got["m3"] == want[2]
+    assert got["m3_shape"] == unchained["m3_shape"]
     assert (got["chained"] > 0) == chained
