@@ -595,6 +595,8 @@ Engine::Engine(int device, int64_t budget_bytes, int max_slots, int stream_prior
     *(static_cast<unsigned char *>(h_init_.p) + kSeedTemplate + 76) = 1;
     const char *lx = std::getenv("PMDD_LEX_TILES");
     if (lx && lx[0] == '0') lex_tiles_ = false;
+    const char *sx = std::getenv("PMDD_SUM_TILES");
+    if (sx && *sx) sum_tiles_ = sx[0] == '1';
     const char *lb = std::getenv("PMDD_LEX_BULK");
     if (lb && *lb) lex_bulk_ = lb[0] == '1';
     const char *cl = std::getenv("PMDD_CHAIN_LAYERS");
@@ -1897,9 +1899,9 @@ int Engine::step() {
         // blocks beyond the tiles would only be scheduled to exit (several waves of them at
         // the tiles' shared-memory size cost more than a small step's work)
         const int grid = static_cast<int>(std::min<int64_t>(sms_ * 8, std::max<int64_t>(1, gl.tiles)));
-        const bool lex = gl.d == 3 && lex_tiles_;
+        const bool lex = lex_tiles_for(gl.d, gl.wide);
         const cudaError_t te =
-            lex ? dev::launch_expand_tiles_lex(gl.wide, dj, dtb, static_cast<int>(gl.count), gl.tiles, grid, queue,
+            lex ? dev::launch_expand_tiles_lex(gl.d, gl.wide, dj, dtb, static_cast<int>(gl.count), gl.tiles, grid, queue,
                                                nullptr, stream_)
                 : dev::launch_expand_tiles(gl.d, gl.wide, dj, dtb, static_cast<int>(gl.count), gl.tiles, grid, queue,
                                            nullptr, stream_);
@@ -2031,11 +2033,11 @@ int Engine::step() {
                         return -1;
                     launches_ += 2;
                 }
-                const bool lex = g.d == 3 && lex_tiles_;
+                const bool lex = lex_tiles_for(g.d, g.wide);
                 // the tiles' bound assumes full buffers: one wave of blocks loops over them
                 const int grid = static_cast<int>(std::min<int64_t>(sms_ * 2, std::max<int64_t>(1, g.tiles[j])));
                 const cudaError_t te =
-                    lex ? dev::launch_expand_tiles_lex(g.wide, dj, dtb, static_cast<int>(n), g.tiles[j], grid, queue,
+                    lex ? dev::launch_expand_tiles_lex(g.d, g.wide, dj, dtb, static_cast<int>(n), g.tiles[j], grid, queue,
                                                        tiles_dev, stream_)
                         : dev::launch_expand_tiles(g.d, g.wide, dj, dtb, static_cast<int>(n), g.tiles[j], grid, queue,
                                                    tiles_dev, stream_);

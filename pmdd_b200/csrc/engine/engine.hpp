@@ -334,6 +334,13 @@ class Engine {
     // value ("lex_pair_max" in the tuning file), else kDefaultPairMax.
     static constexpr int32_t kDefaultPairMax = 48;
     bool lex_tiles_ = true;
+    // Four objectives with int32 points: tiles in sum order (tile_lex.cu) with
+    // PMDD_SUM_TILES=1; by default the pairwise tile kernel, which measured faster (KP d=4
+    // n=60: 29.6 against 31.2 ms, method 1).
+    bool sum_tiles_ = false;
+    bool lex_tiles_for(int d, bool wide) const {
+        return dev::lex_tiles_cover(d, wide) && (d == 3 ? lex_tiles_ : sum_tiles_);
+    }
     // Lexicographic tiles stage each arc's parent run into shared memory with one bulk copy
     // (cp.async.bulk on an mbarrier) instead of per-thread loads: PMDD_LEX_BULK=1 / 0.
     bool lex_bulk_ = false;

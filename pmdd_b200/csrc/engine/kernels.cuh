@@ -16,11 +16,12 @@ cudaError_t launch_chain_prep(const ChainPrep &P, cudaStream_t stream);
 cudaError_t launch_expand_tiles(int d, bool wide, const ExpandJob *jobs, const int64_t *tile_bases, int num_jobs,
                                 int64_t total_tiles, int grid, unsigned long long *queue, const int64_t *tiles_dev,
                                 cudaStream_t stream);
-// Three objectives, frontiers in descending lexicographic order (tile_lex.cu).
-cudaError_t launch_expand_tiles_lex(bool wide, const ExpandJob *jobs, const int64_t *tile_bases, int num_jobs,
+// Three objectives (frontiers in descending lexicographic order) and four with int32
+// points (descending objective sum) (tile_lex.cu); lex_tiles_cover says which.
+bool lex_tiles_cover(int d, bool wide);
+cudaError_t launch_expand_tiles_lex(int d, bool wide, const ExpandJob *jobs, const int64_t *tile_bases, int num_jobs,
                                     int64_t total_tiles, int grid, unsigned long long *queue,
                                     const int64_t *tiles_dev, cudaStream_t stream);
-size_t lex_tile_smem_bytes(bool wide);
 // Fills every job's tile_first (destination i belongs to tile min(start_i / kTileWindow,
 // num_tiles - 1)); one thread per destination over all jobs.
 cudaError_t launch_tile_plan(const ExpandJob *jobs, const int64_t *item_bases, int num_jobs, int64_t total_items,

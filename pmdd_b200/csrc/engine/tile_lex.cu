@@ -57,10 +57,10 @@ constexpr int kLexSlots = kTileCap / kLexSeg;  // staircases kept for the segmen
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kWaitIters = 1 << 22;  // bulk-copy barrier: try_wait rounds before giving up
 
-template <typename T>
+template <int D, typename T>
 struct LexSmem {
-    PackedPt<3, T> pts[kTileCap];        // candidates in run order; staircases after the merge
-    PackedPt<3, T> mpts[kTileCap];       // candidates in merged (descending lexicographic) order
+    PackedPt<D, T> pts[kTileCap];        // candidates in run order; staircases after the merge
+    PackedPt<D, T> mpts[kTileCap];       // candidates in merged (descending) order
     int16_t tag[kTileCap];               // staged arc of each run-order candidate
     uint16_t item_of[kTileCap];          // staged destination of each candidate (either order)
     uint8_t keep[kTileCap];              // by merged position
@@ -160,11 +160,41 @@ __device__ __forceinline__ bool lex_eq(const PackedPt<3, T> &a, const PackedPt<3
     return a.v[0] == b.v[0] && a.v[1] == b.v[1] && a.v[2] == b.v[2];
 }
 
+// The frontier order: three objectives, descending lexicographic; four (int32 points),
+// descending objective sum, ties descending lexicographic.  Both keep a shifted run in
+// order, and in both a point that dominates another comes before it.
+template <int D, typename T>
+__device__ __forceinline__ bool ord_gt(const PackedPt<D, T> &a, const PackedPt<D, T> &b) {
+    if constexpr (D == 3) {
+        return lex_gt(a, b);
+    } else {
+        int64_t sa = 0, sb = 0;
+#pragma unroll
+        for (int o = 0; o < D; ++o) {
+            sa += a.v[o];
+            sb += b.v[o];
+        }
+        if (sa != sb) return sa > sb;
+#pragma unroll
+        for (int o = 0; o < D; ++o)
+            if (a.v[o] != b.v[o]) return a.v[o] > b.v[o];
+        return false;
+    }
+}
+
+template <int D, typename T>
+__device__ __forceinline__ bool ord_eq(const PackedPt<D, T> &a, const PackedPt<D, T> &b) {
+    bool e = true;
+#pragma unroll
+    for (int o = 0; o < D; ++o) e &= a.v[o] == b.v[o];
+    return e;
+}
+
 // Candidates at merged positions [s, e) (one segment of a destination) walked by one
 // warp from an empty staircase; with `save` the final staircase is kept there (its entry
 // count in *save_m, -1 if it outgrew kStairCap).
 template <typename T>
-__device__ void stair_filter(LexSmem<T> &S, Stair<T> &sb, int s, int e, int lane, SegStair<T> *save,
+__device__ void stair_filter(LexSmem<3, T> &S, Stair<T> &sb, int s, int e, int lane, SegStair<T> *save,
                              int16_t *save_m) {
     StairState st;
     for (int c0 = s; c0 < e; c0 += 32) {
@@ -200,13 +230,13 @@ __device__ void stair_filter(LexSmem<T> &S, Stair<T> &sb, int s, int e, int lane
 
 }  // namespace
 
-template <typename T>
+template <int D, typename T>
 __global__ void __launch_bounds__(kLT) expand_tile_lex_kernel(const ExpandJob *__restrict__ jobs,
                                                               const int64_t *__restrict__ tile_bases, int num_jobs,
                                                               int64_t total_tiles, unsigned long long *queue,
                                                               const int64_t *tiles_dev) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    LexSmem<T> &S = *reinterpret_cast<LexSmem<T> *>(smem_raw);
+    LexSmem<D, T> &S = *reinterpret_cast<LexSmem<D, T> *>(smem_raw);
     Stair<T> *stairs = reinterpret_cast<Stair<T> *>(&S.pts[0]);
     SegStair<T> *slots = reinterpret_cast<SegStair<T> *>(stairs + kLexWarps);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -347,6 +377,11 @@ __global__ void __launch_bounds__(kLT) expand_tile_lex_kernel(const ExpandJob *_
             if (tid == 0) S.arc_pos[total_a] = static_cast<int16_t>(total);
             for (int q = tid; q < total; q += kLT) S.tag[q] = -1;
             __syncthreads();
+            if constexpr (D != 3) {  // a run from an unsorted parent leaves its destination unsorted
+                if (J.out_sorted)
+                    for (int k = tid; k < n_it; k += kLT)
+                        if (S.item_count[k]) J.out_sorted[ic + k] = 0;
+            }
             // --- bulk staging (J.lex_bulk): each parent run, widened to 16-byte boundaries,
             // goes to shared memory (the mpts area, unused until the merge) by one
             // cp.async.bulk completing on the block's barrier, while the arc assignment
@@ -367,9 +402,9 @@ __global__ void __launch_bounds__(kLT) expand_tile_lex_kernel(const ExpandJob *_
                     if (x < total_a) {
                         const int len = S.arc_pos[x + 1] - S.arc_pos[x];
                         if (len > 0) {
-                            const uintptr_t a = reinterpret_cast<uintptr_t>(prev + S.arc_src[x] * 3);
+                            const uintptr_t a = reinterpret_cast<uintptr_t>(prev + S.arc_src[x] * D);
                             const uintptr_t lo = a & ~static_cast<uintptr_t>(15);
-                            const uintptr_t hi = (a + static_cast<uintptr_t>(len) * 3 * sizeof(T) + 15) &
+                            const uintptr_t hi = (a + static_cast<uintptr_t>(len) * D * sizeof(T) + 15) &
                                                  ~static_cast<uintptr_t>(15);
                             padded[r] = static_cast<int32_t>(hi - lo);
                             lo_addr[r] = lo;
@@ -385,7 +420,7 @@ __global__ void __launch_bounds__(kLT) expand_tile_lex_kernel(const ExpandJob *_
                     for (int r = 0; r < AP; ++r) {
                         const int x = tid * AP + r;
                         if (x < total_a && padded[r] > 0) {
-                            const uintptr_t a = reinterpret_cast<uintptr_t>(prev + S.arc_src[x] * 3);
+                            const uintptr_t a = reinterpret_cast<uintptr_t>(prev + S.arc_src[x] * D);
                             S.arc_stage[x] = run + static_cast<int32_t>(a - lo_addr[r]);
                         }
                         run += padded[r];
@@ -446,12 +481,12 @@ __global__ void __launch_bounds__(kLT) expand_tile_lex_kernel(const ExpandJob *_
                 const int x = S.tag[q];
                 const int k = S.arc_item[x];
                 const int64_t idx = q - S.arc_pos[x];
-                const T *src = bulk ? reinterpret_cast<const T *>(stage + S.arc_stage[x]) + idx * 3
-                                    : prev + (S.arc_src[x] + idx) * 3;
-                const int32_t *w = J.weights + static_cast<int64_t>(S.arc_w[x]) * 3;
-                PackedPt<3, T> pt;
+                const T *src = bulk ? reinterpret_cast<const T *>(stage + S.arc_stage[x]) + idx * D
+                                    : prev + (S.arc_src[x] + idx) * D;
+                const int32_t *w = J.weights + static_cast<int64_t>(S.arc_w[x]) * D;
+                PackedPt<D, T> pt;
 #pragma unroll
-                for (int o = 0; o < PackedPt<3, T>::kPad; ++o) pt.v[o] = o < 3 ? src[o] + static_cast<T>(w[o]) : T(0);
+                for (int o = 0; o < PackedPt<D, T>::kPad; ++o) pt.v[o] = o < D ? src[o] + static_cast<T>(w[o]) : T(0);
                 S.pts[q] = pt;
                 S.item_of[q] = static_cast<uint16_t>(k);
             }
@@ -462,7 +497,7 @@ __global__ void __launch_bounds__(kLT) expand_tile_lex_kernel(const ExpandJob *_
                 const int k = S.item_of[q];
                 const int x = S.tag[q];
                 const int js = S.item_s[k], je = S.item_s[k + 1];
-                const PackedPt<3, T> me = S.pts[q];
+                const PackedPt<D, T> me = S.pts[q];
                 int rank = 0;
                 if (S.item_count[k] == 0) {
                     rank = q - S.arc_pos[x];
@@ -475,126 +510,169 @@ __global__ void __launch_bounds__(kLT) expand_tile_lex_kernel(const ExpandJob *_
                         int a = lo, b = hi;
                         while (a < b) {
                             const int mid = (a + b) >> 1;
-                            const PackedPt<3, T> c = S.pts[mid];
-                            const bool before = lex_gt(c, me) || (tie_first && lex_eq(c, me));
+                            const PackedPt<D, T> c = S.pts[mid];
+                            const bool before = ord_gt<D, T>(c, me) || (tie_first && ord_eq<D, T>(c, me));
                             if (before) a = mid + 1;
                             else b = mid;
                         }
                         rank += a - lo;
                     }
-                } else {
+                } else if constexpr (D == 3) {
                     for (int j = js; j < je; ++j) {
                         const PackedPt<3, T> c = S.pts[j];
                         rank += (lex_gt(c, me) || (j < q && lex_eq(c, me))) ? 1 : 0;
                     }
+                } else {
+                    rank = q - js;  // a run from an unsorted parent: run order, swept in full below
                 }
                 S.mpts[js + rank] = me;
             }
-            // segments for the staircase warps, those of the largest destinations first (three
-            // tiers); a destination of more than kLexSeg candidates gets one slot per segment
-            // but its last for the staircases the later segments are checked against
-            for (int tier = 0; tier < 3; ++tier) {
-                const int lo_c = tier == 0 ? 512 : (tier == 1 ? 128 : pair_max);
-                const int hi_c = tier == 0 ? kTileCap : (tier == 1 ? 512 : 128);
-                for (int k = tid; k < n_it; k += kLT) {
-                    const int c = S.item_s[k + 1] - S.item_s[k];
-                    if (c > lo_c && c <= hi_c && c > pair_max) {
-                        const int nseg = lex_segments(c);
-                        const int at = atomicAdd(&S.n_big, nseg);
-                        for (int g = 0; g < nseg; ++g) S.big[at + g] = k | (g << 16);
-                        if (nseg > 1) S.item_slot0[k] = static_cast<int8_t>(atomicAdd(&S.n_slot, nseg - 1));
-                    }
-                }
-                __syncthreads();
-            }
-            clk.lap(4);
-            // --- filter, big destinations: one staircase warp per segment
-            const long long f0 = (J.phase_clk && lane == 0) ? clock64() : 0;
-            while (true) {
-                int b = 0;
-                if (lane == 0) b = atomicAdd(&S.next_big, 1);
-                b = __shfl_sync(kFull, b, 0);
-                if (b >= S.n_big) break;
-                const int k = S.big[b] & 0xffff, g = S.big[b] >> 16;
-                const int js = S.item_s[k], c = S.item_s[k + 1] - js;
-                const int nseg = lex_segments(c), len = (c + nseg - 1) / nseg;
-                if (g == 0 && lane == 0 && J.tile_surv != nullptr)
-                    atomicAdd(J.tile_surv + 1, static_cast<unsigned long long>(c));
-                const int slot = g + 1 < nseg ? S.item_slot0[k] + g : -1;
-                stair_filter<T>(S, stairs[warp], js + g * len, js + min(c, (g + 1) * len), lane,
-                                slot >= 0 ? slots + slot : nullptr, slot >= 0 ? S.slot_m + slot : nullptr);
-            }
-            const long long f1 = (J.phase_clk && lane == 0) ? clock64() : 0;
-            // --- filter, small destinations: every candidate against the points before it
-            while (true) {
-                int c0 = 0;
-                if (lane == 0) c0 = atomicAdd(&S.next_chunk, 1) * 32;
-                c0 = __shfl_sync(kFull, c0, 0);
-                if (c0 >= total) break;
-                const int q = c0 + lane;
-                int js = q, len = 0;
-                if (q < total) {
-                    const int k = S.item_of[q];
-                    const int s0 = S.item_s[k], s1 = S.item_s[k + 1];
-                    if (s1 - s0 <= pair_max) {
-                        js = s0;
-                        len = q - s0;
-                    }
-                }
-                const bool mine = q < total && (S.item_s[S.item_of[q] + 1] - S.item_s[S.item_of[q]]) <= pair_max;
-                if (!__any_sync(kFull, mine)) continue;
-                T q1 = 0, q2 = 0;
-                if (mine) {
-                    q1 = S.mpts[q].v[1];
-                    q2 = S.mpts[q].v[2];
-                }
-                bool dom = !mine;
-                const int maxlen = warp_max_i(len);
-                for (int t = 0; t < maxlen; ++t) {
-                    if (t < len) {
-                        const PackedPt<3, T> c = S.mpts[js + t];
-                        dom |= (c.v[1] >= q1) & (c.v[2] >= q2);
-                    }
-                    if ((t & 7) == 7 && __all_sync(kFull, dom)) break;
-                }
-                if (mine) S.keep[q] = dom ? 0 : 1;
-            }
-            if (J.phase_clk && lane == 0) {  // warp busy cycles: staircase loop, pairwise loop
-                const long long f2 = clock64();
-                atomicAdd(J.phase_clk + 7, static_cast<unsigned long long>(f1 - f0));
-                atomicAdd(J.phase_clk + 8, static_cast<unsigned long long>(f2 - f1));
-            }
-            __syncthreads();
-            // --- filter, segmented destinations: a survivor of its own segment is checked
-            // against the staircases of the segments before it (every point of a segment is
-            // covered by an entry of its staircase), or their points if a staircase was not kept
-            if (S.n_slot > 0) {
-                for (int q = tid; q < total; q += kLT) {
-                    if (!S.keep[q]) continue;
-                    const int k = S.item_of[q];
-                    const int js = S.item_s[k], c = S.item_s[k + 1] - js;
-                    if (c <= pair_max || c <= kLexSeg) continue;
-                    const int nseg = lex_segments(c), len = (c + nseg - 1) / nseg;
-                    const int g = (q - js) / len;
-                    const T q1 = S.mpts[q].v[1], q2 = S.mpts[q].v[2];
-                    bool dom = false;
-                    for (int t = 0; t < g && !dom; ++t) {
-                        const int slot = S.item_slot0[k] + t;
-                        const int m = S.slot_m[slot];
-                        if (m >= 0) {
-                            int a = 0, b = m;  // entries with objective 1 >= q1
-                            while (a < b) {
-                                const int mid = (a + b) >> 1;
-                                if (slots[slot].v1[mid] >= q1) a = mid + 1;
-                                else b = mid;
-                            }
-                            dom = a > 0 && slots[slot].v2[a - 1] >= q2;
-                        } else {
-                            for (int j = js + t * len; j < js + (t + 1) * len && !dom; ++j)
-                                dom = (S.mpts[j].v[1] >= q1) & (S.mpts[j].v[2] >= q2);
+            if constexpr (D == 3) {
+                // segments for the staircase warps, those of the largest destinations first (three
+                // tiers); a destination of more than kLexSeg candidates gets one slot per segment
+                // but its last for the staircases the later segments are checked against
+                for (int tier = 0; tier < 3; ++tier) {
+                    const int lo_c = tier == 0 ? 512 : (tier == 1 ? 128 : pair_max);
+                    const int hi_c = tier == 0 ? kTileCap : (tier == 1 ? 512 : 128);
+                    for (int k = tid; k < n_it; k += kLT) {
+                        const int c = S.item_s[k + 1] - S.item_s[k];
+                        if (c > lo_c && c <= hi_c && c > pair_max) {
+                            const int nseg = lex_segments(c);
+                            const int at = atomicAdd(&S.n_big, nseg);
+                            for (int g = 0; g < nseg; ++g) S.big[at + g] = k | (g << 16);
+                            if (nseg > 1) S.item_slot0[k] = static_cast<int8_t>(atomicAdd(&S.n_slot, nseg - 1));
                         }
                     }
-                    if (dom) S.keep[q] = 0;
+                    __syncthreads();
+                }
+                clk.lap(4);
+                // --- filter, big destinations: one staircase warp per segment
+                const long long f0 = (J.phase_clk && lane == 0) ? clock64() : 0;
+                while (true) {
+                    int b = 0;
+                    if (lane == 0) b = atomicAdd(&S.next_big, 1);
+                    b = __shfl_sync(kFull, b, 0);
+                    if (b >= S.n_big) break;
+                    const int k = S.big[b] & 0xffff, g = S.big[b] >> 16;
+                    const int js = S.item_s[k], c = S.item_s[k + 1] - js;
+                    const int nseg = lex_segments(c), len = (c + nseg - 1) / nseg;
+                    if (g == 0 && lane == 0 && J.tile_surv != nullptr)
+                        atomicAdd(J.tile_surv + 1, static_cast<unsigned long long>(c));
+                    const int slot = g + 1 < nseg ? S.item_slot0[k] + g : -1;
+                    stair_filter<T>(S, stairs[warp], js + g * len, js + min(c, (g + 1) * len), lane,
+                                    slot >= 0 ? slots + slot : nullptr, slot >= 0 ? S.slot_m + slot : nullptr);
+                }
+                const long long f1 = (J.phase_clk && lane == 0) ? clock64() : 0;
+                // --- filter, small destinations: every candidate against the points before it
+                while (true) {
+                    int c0 = 0;
+                    if (lane == 0) c0 = atomicAdd(&S.next_chunk, 1) * 32;
+                    c0 = __shfl_sync(kFull, c0, 0);
+                    if (c0 >= total) break;
+                    const int q = c0 + lane;
+                    int js = q, len = 0;
+                    if (q < total) {
+                        const int k = S.item_of[q];
+                        const int s0 = S.item_s[k], s1 = S.item_s[k + 1];
+                        if (s1 - s0 <= pair_max) {
+                            js = s0;
+                            len = q - s0;
+                        }
+                    }
+                    const bool mine = q < total && (S.item_s[S.item_of[q] + 1] - S.item_s[S.item_of[q]]) <= pair_max;
+                    if (!__any_sync(kFull, mine)) continue;
+                    T q1 = 0, q2 = 0;
+                    if (mine) {
+                        q1 = S.mpts[q].v[1];
+                        q2 = S.mpts[q].v[2];
+                    }
+                    bool dom = !mine;
+                    const int maxlen = warp_max_i(len);
+                    for (int t = 0; t < maxlen; ++t) {
+                        if (t < len) {
+                            const PackedPt<3, T> c = S.mpts[js + t];
+                            dom |= (c.v[1] >= q1) & (c.v[2] >= q2);
+                        }
+                        if ((t & 7) == 7 && __all_sync(kFull, dom)) break;
+                    }
+                    if (mine) S.keep[q] = dom ? 0 : 1;
+                }
+                if (J.phase_clk && lane == 0) {  // warp busy cycles: staircase loop, pairwise loop
+                    const long long f2 = clock64();
+                    atomicAdd(J.phase_clk + 7, static_cast<unsigned long long>(f1 - f0));
+                    atomicAdd(J.phase_clk + 8, static_cast<unsigned long long>(f2 - f1));
+                }
+                __syncthreads();
+                // --- filter, segmented destinations: a survivor of its own segment is checked
+                // against the staircases of the segments before it (every point of a segment is
+                // covered by an entry of its staircase), or their points if a staircase was not kept
+                if (S.n_slot > 0) {
+                    for (int q = tid; q < total; q += kLT) {
+                        if (!S.keep[q]) continue;
+                        const int k = S.item_of[q];
+                        const int js = S.item_s[k], c = S.item_s[k + 1] - js;
+                        if (c <= pair_max || c <= kLexSeg) continue;
+                        const int nseg = lex_segments(c), len = (c + nseg - 1) / nseg;
+                        const int g = (q - js) / len;
+                        const T q1 = S.mpts[q].v[1], q2 = S.mpts[q].v[2];
+                        bool dom = false;
+                        for (int t = 0; t < g && !dom; ++t) {
+                            const int slot = S.item_slot0[k] + t;
+                            const int m = S.slot_m[slot];
+                            if (m >= 0) {
+                                int a = 0, b = m;  // entries with objective 1 >= q1
+                                while (a < b) {
+                                    const int mid = (a + b) >> 1;
+                                    if (slots[slot].v1[mid] >= q1) a = mid + 1;
+                                    else b = mid;
+                                }
+                                dom = a > 0 && slots[slot].v2[a - 1] >= q2;
+                            } else {
+                                for (int j = js + t * len; j < js + (t + 1) * len && !dom; ++j)
+                                    dom = (S.mpts[j].v[1] >= q1) & (S.mpts[j].v[2] >= q2);
+                            }
+                        }
+                        if (dom) S.keep[q] = 0;
+                    }
+                    __syncthreads();
+                }
+            } else {
+                // --- filter, four objectives: a candidate is dominated only by a point before
+                // it in sum order (a dominating point has the larger sum, an equal one comes
+                // first), so each sweeps the points before it -- the likeliest dominators
+                // first -- unless its destination has a run from an unsorted parent, which it
+                // sweeps in full by the keep rule (another point >= and (different or first))
+                __syncthreads();  // the merged order is complete
+                clk.lap(4);
+                while (true) {
+                    int c0 = 0;
+                    if (lane == 0) c0 = atomicAdd(&S.next_chunk, 1) * 32;
+                    c0 = __shfl_sync(kFull, c0, 0);
+                    if (c0 >= total) break;
+                    const int q = c0 + lane;
+                    const bool valid = q < total;
+                    int js = INT_MAX, end = INT_MIN;
+                    T p[D];
+#pragma unroll
+                    for (int o = 0; o < D; ++o) p[o] = T(0);
+                    if (valid) {
+                        const int k = S.item_of[q];
+                        js = S.item_s[k];
+                        end = S.item_count[k] ? S.item_s[k + 1] : q;
+                        const PackedPt<D, T> me = S.mpts[q];
+#pragma unroll
+                        for (int o = 0; o < D; ++o) p[o] = me.v[o];
+                    }
+                    const int J0 = warp_min_i(js), J1 = warp_max_i(end);
+                    bool dom = !valid;
+                    for (int j = J0; j < J1; ++j) {
+                        const PackedPt<D, T> c = S.mpts[j];
+                        if (!dom && j >= js && j < end && j != q && ge_all<D, T>(c, p) &&
+                            (j < q || !eq_all<D, T>(c, p)))
+                            dom = true;
+                        if (((j - J0) & 31) == 31 && __all_sync(kFull, dom)) break;
+                    }
+                    if (valid) S.keep[q] = dom ? 0 : 1;
                 }
                 __syncthreads();
             }
@@ -628,10 +706,10 @@ __global__ void __launch_bounds__(kLT) expand_tile_lex_kernel(const ExpandJob *_
                 if (!S.keep[q]) continue;
                 const int k = S.item_of[q];
                 const int64_t dst = S.item_c0[k] + (S.keep_ex[q] - S.keep_ex[S.item_s[k]]);
-                T *o_ = outp + dst * 3;
-                const PackedPt<3, T> me = S.mpts[q];
+                T *o_ = outp + dst * D;
+                const PackedPt<D, T> me = S.mpts[q];
 #pragma unroll
-                for (int o = 0; o < 3; ++o) o_[o] = me.v[o];
+                for (int o = 0; o < D; ++o) o_[o] = me.v[o];
             }
             for (int k = tid; k < n_it; k += kLT) {
                 const int js = S.item_s[k], je = S.item_s[k + 1];
@@ -647,30 +725,35 @@ __global__ void __launch_bounds__(kLT) expand_tile_lex_kernel(const ExpandJob *_
 
 namespace {
 
-template <typename T>
+template <int D, typename T>
 cudaError_t launch_lex_t(const ExpandJob *jobs, const int64_t *tile_bases, int num_jobs, int64_t total_tiles, int grid,
                          unsigned long long *queue, const int64_t *tiles_dev, cudaStream_t stream) {
-    static_assert(sizeof(Stair<T>) * kLexWarps + sizeof(SegStair<T>) * kLexSlots <= sizeof(PackedPt<3, T>) * kTileCap,
-                  "staircases fit over pts");
-    const size_t smem = sizeof(LexSmem<T>);
-    const cudaError_t e = ensure_smem_limit(reinterpret_cast<const void *>(expand_tile_lex_kernel<T>), smem);
+    if constexpr (D == 3)
+        static_assert(sizeof(Stair<T>) * kLexWarps + sizeof(SegStair<T>) * kLexSlots <= sizeof(PackedPt<3, T>) * kTileCap,
+                      "staircases fit over pts");
+    const size_t smem = sizeof(LexSmem<D, T>);
+    const cudaError_t e = ensure_smem_limit(reinterpret_cast<const void *>(expand_tile_lex_kernel<D, T>), smem);
     if (e != cudaSuccess) return e;
     if (total_tiles <= 0) return cudaSuccess;
     const int64_t g = std::min<int64_t>(total_tiles, grid);
-    expand_tile_lex_kernel<T><<<static_cast<unsigned>(g), kLT, smem, stream>>>(jobs, tile_bases, num_jobs, total_tiles,
-                                                                              queue, tiles_dev);
+    expand_tile_lex_kernel<D, T><<<static_cast<unsigned>(g), kLT, smem, stream>>>(jobs, tile_bases, num_jobs,
+                                                                                 total_tiles, queue, tiles_dev);
     return cudaGetLastError();
 }
 
 }  // namespace
 
-size_t lex_tile_smem_bytes(bool wide) { return wide ? sizeof(LexSmem<int64_t>) : sizeof(LexSmem<int32_t>); }
+bool lex_tiles_cover(int d, bool wide) { return d == 3 || (d == 4 && !wide); }
 
-cudaError_t launch_expand_tiles_lex(bool wide, const ExpandJob *jobs, const int64_t *tile_bases, int num_jobs,
+cudaError_t launch_expand_tiles_lex(int d, bool wide, const ExpandJob *jobs, const int64_t *tile_bases, int num_jobs,
                                     int64_t total_tiles, int grid, unsigned long long *queue,
                                     const int64_t *tiles_dev, cudaStream_t stream) {
-    if (wide) return launch_lex_t<int64_t>(jobs, tile_bases, num_jobs, total_tiles, grid, queue, tiles_dev, stream);
-    return launch_lex_t<int32_t>(jobs, tile_bases, num_jobs, total_tiles, grid, queue, tiles_dev, stream);
+    if (d == 3 && wide)
+        return launch_lex_t<3, int64_t>(jobs, tile_bases, num_jobs, total_tiles, grid, queue, tiles_dev, stream);
+    if (d == 3) return launch_lex_t<3, int32_t>(jobs, tile_bases, num_jobs, total_tiles, grid, queue, tiles_dev, stream);
+    if (d == 4 && !wide)
+        return launch_lex_t<4, int32_t>(jobs, tile_bases, num_jobs, total_tiles, grid, queue, tiles_dev, stream);
+    return cudaErrorInvalidValue;
 }
 
 }  // namespace dev

@@ -1,4 +1,5 @@
-"""Three-objective frontiers in lexicographic order (tile_lex.cu, big_lex.cu, stair.cuh).
+"""Frontiers in lexicographic (three objectives) and objective-sum (four) order: tile_lex.cu,
+big_lex.cu, stair.cuh.
 
 * Knapsack profits with objective 1 + objective 2 the same for every item make the
   (objective 1, objective 2) projections of a frontier an antichain, so the staircase
@@ -10,8 +11,11 @@
   staged by bulk copies or loaded directly (PMDD_LEX_BULK 1 / 0), and the pairwise tile
   kernel (PMDD_LEX_TILES=0) stay exact on the golden fixtures and seeded instances, and
   so do oversized destinations of up to 4096 runs sorted by merge rounds
-  (PMDD_BIG_LEX_MAX_ARCS=4096) or none of them on the lexicographic path (0).  The
-  engine reads these settings at start-up, so each runs in a child process.
+  (PMDD_BIG_LEX_MAX_ARCS=4096) or none of them on the lexicographic path (0).  Four
+  objectives: the pairwise tile kernel (the default) and the tiles in objective-sum order
+  (PMDD_SUM_TILES=1; a candidate swept against the points before it) give the golden and
+  the oracle's frontiers.  The engine reads these settings at start-up, so each runs
+  in a child process.
 """
 import json
 import os
@@ -62,16 +66,17 @@ from pmdd_b200 import instances
 from conftest import golden_cases, golden_frontier
 n = 0
 for rec in golden_cases():
-    if rec["nobjs"] != 3:
+    if rec["nobjs"] not in (3, 4):
         continue
-    dd = P.DecisionDiagram.from_file(rec["dat"], rec["problem_type"], 3)
+    dd = P.DecisionDiagram.from_file(rec["dat"], rec["problem_type"], rec["nobjs"])
     for m in rec["methods"]:
         got = P.enumerate_dd(dd, method=int(m))
         assert np.array_equal(oracle.sorted_set(got), oracle.sorted_set(golden_frontier(rec, int(m)))), (rec["name"], m)
         n += 1
-for text, pt in ((instances.knapsack_text(46, 3, 31), 1), (instances.setpacking_text(90, 20, 3, 32), 2),
-                 (instances.tsp_text(11, 3, 33), 3)):
-    dd = P.DecisionDiagram.from_text(text, pt, 3)
+for text, pt, d in ((instances.knapsack_text(46, 3, 31), 1, 3), (instances.setpacking_text(90, 20, 3, 32), 2, 3),
+                    (instances.tsp_text(11, 3, 33), 3, 3), (instances.knapsack_text(36, 4, 34), 1, 4),
+                    (instances.setpacking_text(80, 20, 4, 35), 2, 4), (instances.tsp_text(10, 4, 36), 3, 4)):
+    dd = P.DecisionDiagram.from_text(text, pt, d)
     for m in (1, 3):
         got = P.enumerate_dd(dd, method=m)
         assert np.array_equal(oracle.sorted_set(got), oracle.sorted_set(oracle.enumerate(dd, m))), (pt, m)
@@ -82,14 +87,14 @@ print(json.dumps({{"checked": n}}))
 
 @pytest.mark.parametrize("env", [{"PMDD_LEX_PAIR_MAX": "0"}, {"PMDD_LEX_PAIR_MAX": "1024"}, {"PMDD_LEX_TILES": "0"},
                                  {"PMDD_LEX_BULK": "1"}, {"PMDD_LEX_BULK": "0"}, {"PMDD_BIG_LEX_MAX_ARCS": "4096"},
-                                 {"PMDD_BIG_LEX_MAX_ARCS": "0"}],
+                                 {"PMDD_BIG_LEX_MAX_ARCS": "0"}, {"PMDD_SUM_TILES": "1"}],
                          ids=["all-staircase", "all-pairwise", "pairwise-kernel", "bulk-staging", "direct-loads",
-                              "merge-rounds", "no-oversized-lex"])
+                              "merge-rounds", "no-oversized-lex", "four-objective-sum-order"])
 def test_filter_paths_stay_exact(env):
     from conftest import ROOT
 
     e = dict(os.environ)
-    for k in ("PMDD_LEX_PAIR_MAX", "PMDD_LEX_TILES", "PMDD_LEX_BULK", "PMDD_BIG_LEX_MAX_ARCS"):
+    for k in ("PMDD_LEX_PAIR_MAX", "PMDD_LEX_TILES", "PMDD_LEX_BULK", "PMDD_BIG_LEX_MAX_ARCS", "PMDD_SUM_TILES"):
         e.pop(k, None)
     e.update(env)
     p = subprocess.run([sys.executable, "-c", CHILD.format(root=ROOT, tests=os.path.join(ROOT, "tests"))], env=e,
