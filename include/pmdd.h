@@ -291,6 +291,9 @@ int pmdd_server_submit(pmdd_server *srv, const pmdd_dd *dd, const pmdd_options *
 /* Submits a TSP request by its cost matrices: the server uses its shared n-city MDD
  * structure (built on the device on first use) and uploads only the weight table. */
 int pmdd_server_submit_tsp(pmdd_server *srv, const pmdd_tsp *inst, const pmdd_options *opts, uint64_t req_id);
+/* Builds the shared n-city MDD structure now (in every lane) instead of at the first
+ * request of that size, and returns when it is built.  No counterpart in the reference. */
+int pmdd_server_prepare_tsp(pmdd_server *srv, int32_t n);
 /* Runs light-lane steps until at least one request completes (in either lane), max_steps
  * light-lane steps have run (0: no limit) or nothing is pending; while the light lane
  * is idle it waits up to 2 ms at a time for the heavy lane.  Returns the number of

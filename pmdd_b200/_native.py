@@ -212,6 +212,7 @@ GPU_SYMBOLS = {
                                                   ctypes.c_size_t]),
     "pmdd_server_submit_tsp": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(PmddTsp), ctypes.POINTER(PmddOptions),
                                               ctypes.c_uint64]),
+    "pmdd_server_prepare_tsp": (ctypes.c_int, [ctypes.c_void_p, c_i32]),
     "pmdd_resident_dd_shape": (ctypes.c_int, [ctypes.c_void_p, c_i32, P_i32, ctypes.POINTER(c_i64)]),
     "pmdd_resident_dd_copy": (ctypes.c_int, [ctypes.c_void_p, c_i32, P_i32, P_i32, P_i32, P_i32, P_i32, P_i32,
                                              ctypes.c_char_p, ctypes.c_size_t]),

@@ -1147,6 +1147,25 @@ int pmdd_server_submit_tsp(pmdd_server *srv, const pmdd_tsp *t, const pmdd_optio
     return PMDD_OK;
 }
 
+int pmdd_server_prepare_tsp(pmdd_server *srv, int32_t n) {
+    if (!srv || n < pmdd::dev::kTspMinCities || n > pmdd::dev::kTspMaxCities) return PMDD_ERR_INVALID;
+    std::string msg;
+    if (!srv->engine->tsp_structure(n, &msg)) return PMDD_ERR_OOM;
+    if (srv->heavy) {  // built by the worker; waited for, so that the caller's clock starts after it
+        auto rc = std::make_shared<std::atomic<int>>(-1);
+        srv->heavy->post([n, rc](pmdd::Engine &E) {
+            std::string m;
+            rc->store(E.tsp_structure(n, &m) ? PMDD_OK : PMDD_ERR_OOM);
+        }, false);
+        HeavyLane &H = *srv->heavy;
+        std::unique_lock<std::mutex> lk(H.mu);
+        H.done.wait_for(lk, std::chrono::seconds(60), [&] { return rc->load() >= 0 || H.failed; });
+        const int r = rc->load();
+        if (r != PMDD_OK) return r < 0 ? PMDD_ERR_CUDA : r;
+    }
+    return PMDD_OK;
+}
+
 namespace {
 
 // Moves the heavy lane's finished results to the caller's side (pmdd_server_run only,

@@ -60,6 +60,13 @@ class Server:
         o = _options(method, 3, 0, True, max_cand, max_prod, 0)
         return self._lib.pmdd_server_submit_tsp(self._h, ctypes.byref(spec), ctypes.byref(o), ctypes.c_uint64(req_id))
 
+    def prepare_tsp(self, n: int) -> None:
+        """Builds the shared n-city MDD structure now instead of at the first TSP request
+        of that size."""
+        rc = self._lib.pmdd_server_prepare_tsp(self._h, int(n))
+        if rc != 0:
+            raise CudaEnumerationError(rc, f"building the {n}-city structure failed")
+
     def run(self, max_steps: int = 0) -> int:
         r = self._lib.pmdd_server_run(self._h, max_steps)
         if r < 0:

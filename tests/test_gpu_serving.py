@@ -268,3 +268,21 @@ def test_small_requests_pass_a_large_one():
     assert p.returncode == 0, p.stdout + p.stderr
     one = json.loads(p.stdout.strip().splitlines()[-1])
     assert one == {str(i): frontier_digest(got[i].frontier) for i in range(len(reqs))}
+
+
+def test_prepared_tsp_structures():
+    """pmdd_server_prepare_tsp builds a size's structure in both lanes up front; requests of
+    that size then give their lone frontiers, and sizes outside 2..20 cities are refused."""
+    srv = P.Server()
+    try:
+        for n in (9, 11):
+            srv.prepare_tsp(n)
+        with pytest.raises(Exception):
+            srv.prepare_tsp(40)
+        reqs = [_request(3, instances.tsp_text(n, 3, 960 + n), m, f"tsp3_n{n}_s{960 + n}") for n in (9, 11) for m in (1, 3)]
+        got = _drive_all(srv, reqs)
+    finally:
+        srv.close()
+    for i, (kind, payload, method, dd) in enumerate(reqs):
+        assert got[i].status == OK, got[i].error
+        assert frontier_digest(got[i].frontier) == frontier_digest(P.enumerate_dd(dd, method=method)), i
