@@ -1137,16 +1137,18 @@ int Engine::step() {
         e.window = std::min<int64_t>(step_window, window_max_for(I.d, I.opts.problem_type));
         const int64_t window = e.window;
         const size_t pts_bytes = static_cast<size_t>(std::max<int64_t>(C, 1)) * I.d * I.elem();
-        e.out_pts = arena_.alloc(pts_bytes);
         // one block: slot offsets | sizes of the new frontier | the tile plan of this
-        // expansion | sorted flags (released through out_off; the arena ignores the
-        // release of out_size, which it did not hand out)
+        // expansion | sorted flags | the frontier's points (released through out_off; the
+        // arena ignores the releases of out_size and out_pts, which it did not hand out).
+        // The points come last, so that a read widened to 16 bytes past their end stays
+        // inside the block (the arena rounds blocks up to 256 bytes).
         const int64_t ntiles = std::max<int64_t>(1, (C + window - 1) / window);
         const size_t off_bytes = align256(sizeof(int64_t) * V);
-        char *ix = static_cast<char *>(
-            arena_.alloc(off_bytes + sizeof(int32_t) * (V + ntiles + 1) + static_cast<size_t>(V)));
+        const size_t size_bytes = align256(sizeof(int32_t) * (V + ntiles + 1) + static_cast<size_t>(V));
+        char *ix = static_cast<char *>(arena_.alloc(off_bytes + size_bytes + pts_bytes));
         e.out_off = reinterpret_cast<int64_t *>(ix);
         e.out_size = ix ? reinterpret_cast<int32_t *>(ix + off_bytes) : nullptr;
+        e.out_pts = ix ? ix + off_bytes + size_bytes : nullptr;
         if (e.out_size) e.out_sorted = reinterpret_cast<uint8_t *>(e.out_size + V + ntiles + 1);
         bool okay = e.out_pts && e.out_off && e.out_size;
         if (okay && s.res.num_big > 0) {
