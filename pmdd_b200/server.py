@@ -1,8 +1,12 @@
 """Served request loop over libpmdd_gpu.so's pmdd_server_* entry points.
 
 Requests are admitted as slots and HBM budget free up; every admitted request
-advances one DD layer per engine step, sharing each launch with the others
-(continuous batching).  Timestamps are host monotonic seconds.
+advances one DD layer per engine step (or several, when a small step chains layers),
+sharing each launch with the others (continuous batching).  Small requests (DDs of at
+most 2^17 arcs) run in a light lane on the device's highest-priority stream, which
+run() steps in the calling thread; larger ones in a heavy lane that a worker thread of
+the server steps, so the small ones do not wait for their steps.  A server is used from
+one thread at a time.  Timestamps are host monotonic seconds.
 """
 from __future__ import annotations
 
